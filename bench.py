@@ -1,0 +1,376 @@
+#!/usr/bin/env python3
+"""Benchmark of the DD Wilson-clover solver on B200: solves per second.
+
+One step = one complete solve D x = b to a 1e-10 relative residual with the
+FP64-outer / FP32-SAP-inner DD BiCGStab (bicgstab_dd_mix_), x = 0 start,
+on seeded synthetic fields (SU(3) links smoothed by 5 APE-style steps,
+clover-leaf clover term, Gaussian complex FP64 source).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
+    python bench.py --impl reference ...     # the reference's CPU solver
+
+Prints one JSON line (rank 0).  Multi-GPU runs (torchrun) are independent
+replicas (the single-GPU path holds the whole lattice; no data exchange):
+value = total solves of all ranks / max over ranks of the timed device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    # the plain method at GPU scale, single RHS (roofline figures):
+    # 32^3x64, 5 APE steps, csw 1.7, kappa 0.1365, outer 1e-10, inner 1e-6 / 50
+    "plain_32c64": dict(L=(32, 32, 32, 64), NB=(2, 1, 1, 1), csw=1.7, kappa=0.1365, tbc=-1,
+                        seed=11, n_smear=5, alpha=0.36, tol=1e-10, maxiter=200, tol_s=1e-6,
+                        maxiter_s=50, nsap=4, nm=2, src="gauss"),
+    # small variant of the same for quick checks
+    "plain_16c32": dict(L=(16, 16, 16, 32), NB=(2, 1, 1, 1), csw=1.7, kappa=0.1365, tbc=-1,
+                        seed=11, n_smear=5, alpha=0.36, tol=1e-10, maxiter=200, tol_s=1e-6,
+                        maxiter_s=50, nsap=4, nm=2, src="gauss"),
+}
+DEFAULT_WORKLOAD = "plain_32c64"
+# iteration counts of one full solve of each workload, measured with this
+# repository's GPU solver (same algorithm and partition as the reference);
+# used to scale the reference's bounded CPU sample to solves/s.
+REF_COUNTS = {
+    "plain_32c64": None,
+    "plain_16c32": None,
+}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        sm = []
+        reasons = set()
+        smax = None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_fields(w):
+    import qws_b200
+
+    t0 = time.time()
+    U, plaq = qws_b200.gen_gauge(w["L"], w["seed"], w["n_smear"], w["alpha"])
+    C = qws_b200.gen_clover(U, w["L"], w["csw"], w["kappa"])
+    b = qws_b200.gen_source(w["L"], w["seed"] + 1, w["src"])
+    return U, C, b, plaq, time.time() - t0
+
+
+def run_reference_sample(w, counts, threads=None):
+    """The reference's CPU solver timed on this host (subprocess)."""
+    spec = dict(w)
+    spec["counts"] = counts
+    env = dict(os.environ)
+    n = threads or len(os.sched_getaffinity(0))
+    env["OMP_NUM_THREADS"] = str(n)
+    env.setdefault("OMP_PROC_BIND", "close")
+    env["CUDA_VISIBLE_DEVICES"] = ""
+    res = subprocess.run([sys.executable, str(ROOT / "oracle" / "refbench.py"), json.dumps(spec)],
+                         capture_output=True, text=True, env=env, timeout=3600)
+    if res.returncode != 0:
+        raise RuntimeError("reference sample failed: " + res.stderr[-2000:])
+    return json.loads(res.stdout.strip().splitlines()[-1])
+
+
+def dist_setup(n_gpus):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def allreduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def bench_ours(args, w, name):
+    import torch
+
+    import qws_b200
+
+    world, rank, local = dist_setup(args.gpus)
+    U, C, b, plaq, t_gen = make_fields(w)
+    stream = torch.cuda.Stream()
+    lat = qws_b200.Lattice(w["L"], w["NB"], tbc=w["tbc"], kappa=w["kappa"], stream=stream)
+    lat.load_fields(U, C)
+    del U, C
+    with torch.cuda.stream(stream):
+        bd = lat.to_device(b)
+        xd = lat.empty("f64")
+    V = lat.V
+
+    def solve():
+        xd.zero_()
+        return lat.bicgstab_dd_mix(xd, bd, w["tol"], w["maxiter"], w["tol_s"], w["maxiter_s"],
+                                   w["nsap"], w["nm"])
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            st = solve()
+        torch.cuda.synchronize()
+        true_rel = lat.true_residual(xd, bd)
+        c0 = lat.counters()
+
+        # ---- device-resident timed region -----------------------------------
+        clocks = ClockSampler(local)
+        barrier(world)
+        torch.cuda.synchronize()
+        clocks.start()
+        lat.kernel_timing(True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        stats = []
+        for _ in range(args.steps):
+            stats.append(solve())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        barrier(world)
+        ms = e0.elapsed_time(e1)
+        kstats = lat.kernel_stats()
+        lat.kernel_timing(False)
+        c1 = lat.counters()
+        ms_max = allreduce_max(ms, world)
+
+        # ---- end to end through the public API with host buffers --------------
+        pinned = torch.from_numpy(b).pin_memory()
+        host_b = pinned.numpy()
+        host_x = torch.empty_like(pinned).pin_memory().numpy()
+        xh = lat.empty("f64")
+        bh = lat.empty("f64")
+        torch.cuda.synchronize()
+        barrier(world)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            lat.to_device(host_b, out=bh)
+            xh.zero_()
+            lat.bicgstab_dd_mix(xh, bh, w["tol"], w["maxiter"], w["tol_s"], w["maxiter_s"],
+                                w["nsap"], w["nm"])
+            lat.to_host(xh, out=host_x)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = allreduce_max(f0.elapsed_time(f1), world)
+    e2e_true = lat.true_residual(xh, bh)
+
+    per_solve = {k: (c1[k] - c0[k]) / args.steps for k in c1}
+    inner_iters = sum(s["inner_iters"] for s in stats) / len(stats)
+    outer_iters = sum(s["outer_iters"] for s in stats) / len(stats)
+    counts = {"inner_iters": int(round(inner_iters)),
+              "n_approx": int(round(per_solve["prec_s"])),
+              "n_ddd_d": int(round(per_solve["ddd_d"])) + 1}
+
+    peak, peak_kind = measured_peaks()
+    dom = max(kstats.items(), key=lambda kv: kv[1][1]) if kstats else None
+    roofline = None
+    if dom:
+        kname, (nl, kms, kbytes) = dom
+        achieved = kbytes / (kms * 1e-3) / 1e9
+        traffic = None
+        tp = ROOT / "profiles" / "traffic.json"
+        if tp.exists():
+            t = json.loads(tp.read_text())
+            ent = t.get(name, {}).get(kname)
+            if ent:
+                traffic = ent["bytes_per_launch"]
+        roofline = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1),
+                    "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                    "peak_source": peak_kind, "traffic": traffic,
+                    "bytes_per_launch": kbytes / nl, "avg_launch_us": kms / nl * 1e3,
+                    "launches": nl,
+                    "share_of_kernel_time": round(kms / sum(v[1] for v in kstats.values()), 4)}
+    kernels = {k: {"launches": v[0], "ms": round(v[1], 3),
+                   "GBps": round(v[2] / (v[1] * 1e-3) / 1e9, 1) if v[1] else None}
+               for k, v in kstats.items()}
+
+    line = {
+        "metric": "solves/s (DD BiCGStab, FP64 outer / FP32 SAP inner, 1e-10 rel. residual)",
+        "value": world * args.steps / (ms_max * 1e-3),
+        "unit": "solves/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64 outer / f32 inner",
+        "data": "synthetic: seeded SU(3) links + 5 APE steps (plaquette %.4f), clover-leaf "
+                "clover, Gaussian source" % plaq,
+        "config": {"workload": name, "lattice": "x".join(map(str, w["L"])),
+                   "block_grid": list(w["NB"]), "kappa": w["kappa"], "csw": w["csw"],
+                   "tol": w["tol"], "tol_s": w["tol_s"], "maxiter_s": w["maxiter_s"],
+                   "nsap": w["nsap"], "nm": w["nm"],
+                   "l2": "inputs larger than L2 (one FP64 spinor = %.0f MB)" % (V * 24 * 8 / 1e6),
+                   "parallelism": f"replicas x{world}"},
+        "solve": {"outer_iters": outer_iters, "inner_iters": inner_iters,
+                  "true_rel_resid": true_rel, "recursive_rel_resid": stats[-1]["rel_resid_recursive"]},
+        "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "solves/s",
+                "h2d_bytes_per_step": int(b.nbytes), "d2h_bytes_per_step": int(b.nbytes),
+                "true_rel_resid": e2e_true,
+                "path": "qws_b200.Lattice host arrays (pinned) -> qwsg_spinor_to_device_d -> "
+                        "qwsg_bicgstab_dd_mix -> qwsg_spinor_to_host_d"},
+        "gpu_launches": int(sum(v[0] for v in kstats.values())) if kstats else None,
+        "roofline": roofline,
+        "kernels": kernels,
+        "clocks": clk,
+        "counts_per_solve": counts,
+        "field_gen_s": round(t_gen, 2),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            ref = run_reference_sample(w, counts)
+            line["cpu_baseline"] = {"value": ref["solves_per_s"], "unit": "solves/s",
+                                    "cores": ref["threads"], "kind": "reference",
+                                    "sample": ref["sample"]}
+        except Exception as e:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "unit": "solves/s", "error": str(e)[-300:]}
+    lat.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def bench_reference(args, w, name):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    counts = REF_COUNTS.get(name)
+    if counts is None:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": f"no recorded iteration counts for workload {name}"}))
+        return
+    vals = []
+    ref = None
+    for i in range(args.warmup + args.steps):
+        ref = run_reference_sample(w, counts)
+        if i >= args.warmup:
+            vals.append(ref["solves_per_s"])
+    v = statistics.median(vals)
+    line = {
+        "impl": "reference",
+        "metric": "solves/s (DD BiCGStab, FP64 outer / FP32 SAP inner, 1e-10 rel. residual)",
+        "value": v, "unit": "solves/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 outer / f32 inner", "data": "synthetic (same fields as the GPU arm)",
+        "config": {"workload": name, "lattice": "x".join(map(str, w["L"])),
+                   "block_grid": list(w["NB"])},
+        "cpu_baseline": {"value": v, "unit": "solves/s", "cores": ref["threads"],
+                         "kind": "reference", "sample": ref["sample"]},
+        "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        bench_reference(args, w, args.workload)
+    else:
+        bench_ours(args, w, args.workload)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,126 @@
+/* qwsg: native C ABI of the B200 domain-decomposed Wilson-clover solver.
+ *
+ * Status-returning, handle-based interface under the reference-compatible
+ * symbols of qws_dropin.h.  Every function returns 0 on success and a
+ * non-zero code on failure (1 bad argument, 2 unsupported parameter,
+ * 3 CUDA error, 4 not initialised); qwsg_last_error() gives the message.
+ * No torch types; plain pointers and sizes.
+ *
+ * Device spinor buffers hold 24 * pad reals (pad from qwsg_geometry) in the
+ * library's structure-of-arrays "DD order" (colour-major, SAP-block-major);
+ * convert from/to host arrays with qwsg_spinor_to_device_* / _to_host_*.
+ * Host arrays in "natural" layout are indexed
+ *   spinor [site][3 colour][4 spin][2]            site = x + Lx*(y + Ly*(z + Lz*t))
+ *   gauge  [4 mu][site][3 row][3 col][2]          U_mu(x), row-major
+ *   clover [site][2][36]                          QWS's packed chiral blocks of the
+ *                                                  inverse clover term
+ *                                                  (clover_def.h:88-284)
+ *
+ * Block grid NB[4]: the lattice is cut into SAP blocks of L/NB sites.
+ * The reference's partition on an MPI rank grid npe[4] (two x-halves per
+ * rank, qws.cc:141-148) is NB = (2*npe0, npe1, npe2, npe3); NB[0] must be
+ * even and NB[1..3] 1 or even.
+ */
+#ifndef QWSG_H
+#define QWSG_H
+#include <stddef.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct qwsg_lattice qwsg_lattice;
+
+typedef struct {
+  int outer_iters;            /* the reference's conviter (bicgstab_dd_mix.cc:381) */
+  long inner_iters;           /* total inner BiCGStab iterations */
+  double rel_resid_recursive; /* sqrt(|r|^2/|b|^2) of the recursive residual at exit */
+  double rel_resid_true;      /* |b - D x| / |b| recomputed in FP64 (-1 if not requested) */
+} qwsg_solve_stats;
+
+const char* qwsg_last_error(void);
+const char* qwsg_version(void);
+
+/* lattice handle; tbc = +1 periodic / -1 antiperiodic time boundary
+ * (fbc_f[3] of qws_init_, qws.cc:298-310) */
+int qwsg_create(qwsg_lattice** out, const int L[4], const int NB[4], int tbc);
+int qwsg_destroy(qwsg_lattice* lat);
+/* run all work on this cudaStream_t (NULL = the legacy default stream);
+ * until called, the handle uses a private non-blocking stream */
+int qwsg_set_stream(qwsg_lattice* lat, void* cuda_stream);
+int qwsg_set_kappa(qwsg_lattice* lat, double kappa);
+int qwsg_geometry(const qwsg_lattice* lat, int* volume, int* pad);
+int qwsg_sync(qwsg_lattice* lat);
+
+/* resident fields, from host natural-layout FP64 arrays; the FP32 copies are
+ * casts (as qws_loadg_dd_/qws_loadc_dd_ make them, qws_bqcd.cc:125-382) */
+int qwsg_load_gauge(qwsg_lattice* lat, const double* U);
+int qwsg_load_clover(qwsg_lattice* lat, const double* C);
+/* optional explicit FP32 copies (main.cc writes glus/clvs itself) */
+int qwsg_load_gauge_s(qwsg_lattice* lat, const float* U);
+int qwsg_load_clover_s(qwsg_lattice* lat, const float* C);
+
+/* host natural <-> device DD-order planes */
+int qwsg_spinor_to_device_d(qwsg_lattice* lat, double* dev, const double* host);
+int qwsg_spinor_to_host_d(qwsg_lattice* lat, double* host, const double* dev);
+int qwsg_spinor_to_device_s(qwsg_lattice* lat, float* dev, const float* host);
+int qwsg_spinor_to_host_s(qwsg_lattice* lat, float* host, const float* dev);
+
+/* ---- operators on device buffers ---------------------------------------- */
+/* full D = 1 - kappa A^-1 H (ddd_d_ qws.cc:625-632, ddd_s_ qws.cc:641-644) */
+int qwsg_ddd_d(qwsg_lattice* lat, double* out, const double* in);
+int qwsg_ddd_s(qwsg_lattice* lat, float* out, const float* in);
+/* block-interior D on the blocks of one colour (ddd_in_{d,s}_,
+ * ddd_in_d.cc:66-196, ddd_in_s.cc:376); other sites untouched */
+int qwsg_ddd_in_d(qwsg_lattice* lat, double* out, const double* in, int colour);
+int qwsg_ddd_in_s(qwsg_lattice* lat, float* out, const float* in, int colour);
+/* out += factor A^-1 H_face in on one colour's block faces
+ * (ddd_out_pre_*+ddd_out_pos_*, ddd_out_s.cc:639,661) */
+int qwsg_ddd_out_d(qwsg_lattice* lat, double* out, const double* in, int colour, double factor);
+int qwsg_ddd_out_s(qwsg_lattice* lat, float* out, const float* in, int colour, double factor);
+/* jinv_ddd_in_s_ (static_solver.cc:141): nm Richardson steps on one colour */
+int qwsg_jinv_s(qwsg_lattice* lat, float* x, const float* b, int colour, int nm);
+/* prec_ddd_s_ (qws.cc:776) out = D M_SAP in ; prec_s_ (qws.cc:929) out = M_SAP in */
+int qwsg_prec_ddd_s(qwsg_lattice* lat, float* out, const float* in, int nsap, int nm);
+int qwsg_prec_s(qwsg_lattice* lat, float* out, const float* in, int nsap, int nm);
+
+/* ---- solvers ----------------------------------------------------------- */
+/* bicgstab_precdd_s_ (bicgstab_precdd_s.cc:85): x solves (D M) x = b from 0 */
+int qwsg_bicgstab_precdd_s(qwsg_lattice* lat, float* x, const float* b, double tol, int maxiter,
+                           int nsap, int nm, int* iters, double* final_rel);
+/* bicgstab_dd_mix_ (bicgstab_dd_mix.cc:105): FP64 outer, FP32 SAP inner;
+ * x holds the initial guess on entry.  stats may be NULL. */
+int qwsg_bicgstab_dd_mix(qwsg_lattice* lat, double* x, const double* b, double tol, int maxiter,
+                         double tol_s, int maxiter_s, int nsap, int nm, qwsg_solve_stats* stats);
+/* |b - D x| / |b| in FP64 */
+int qwsg_true_residual(qwsg_lattice* lat, const double* x, const double* b, double* rel);
+
+/* ---- synthetic fields (host, OpenMP; conventions in qws_b200/csrc/fields.cu) */
+/* seeded SU(3) links, n_smear APE-style projected averaging steps with
+ * weight alpha; writes the average plaquette (Re tr / 3) to *plaq */
+int qwsg_gen_gauge(double* U, const int L[4], unsigned long long seed, int n_smear, double alpha,
+                   double* plaq);
+int qwsg_plaquette(const double* U, const int L[4], double* plaq);
+/* clover-leaf clover term T = 1 - csw*kappa*sum_{mu<nu} sigma F, stored as QWS
+ * packed chiral blocks of T^-1; T_out (optional) receives T [V][12][12][2] */
+int qwsg_gen_clover(double* C, const double* U, const int L[4], double csw, double kappa,
+                    double* T_out);
+/* sources: kind 0 Gaussian, 1 point at the origin (arg = 4*colour + spin),
+ * 2 Z2 noise */
+int qwsg_gen_source(double* S, const int L[4], unsigned long long seed, int kind, int arg);
+
+/* per-kernel CUDA-event timing on the handle's stream: enable (clears the
+ * records) or disable; stats fills, per kernel kind k < *nkind, the number
+ * of launches, the summed device milliseconds and the summed algorithmic
+ * bytes (bytes each launch must move: spinors, links, clover) */
+int qwsg_kernel_timing(qwsg_lattice* lat, int enable);
+int qwsg_kernel_stats(qwsg_lattice* lat, int* nkind, long* launches, double* ms, double* bytes);
+const char* qwsg_kernel_name(int kind);
+
+/* per-region call counters (reference region names, timing.h) */
+int qwsg_counters(qwsg_lattice* lat, long* prec_ddd_s, long* prec_s, long* jinv,
+                  long* inner_iters, long* ddd_d);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,326 @@
+"""qws_b200: B200-native domain-decomposed Wilson-clover solver.
+
+Python mirror of the C ABI in include/qwsg.h (ctypes over the in-tree
+qws_b200/libqws_b200.so).  The compute path is the CUDA library; this module
+only moves arrays and calls it.  It raises if the library is missing: there
+is no CPU fallback.
+
+Device buffers are torch CUDA tensors used as raw memory (one spinor =
+24 * pad reals in the library's DD-order planes); host arrays are numpy in
+the natural layout documented in include/qwsg.h.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+__all__ = ["load_library", "Lattice", "QwsgError", "SolveStats", "LIB_PATH", "gen_gauge",
+           "gen_clover", "gen_source", "plaquette"]
+
+LIB_PATH = Path(__file__).resolve().parent / "libqws_b200.so"
+_lib = None
+
+
+class QwsgError(RuntimeError):
+    pass
+
+
+class SolveStats(ctypes.Structure):
+    _fields_ = [("outer_iters", ctypes.c_int), ("inner_iters", ctypes.c_long),
+                ("rel_resid_recursive", ctypes.c_double), ("rel_resid_true", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def load_library(path: str | os.PathLike | None = None):
+    """Load libqws_b200.so (build it with `python -m qws_b200.build`)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise QwsgError(f"{p} not found: build the CUDA library with `python -m qws_b200.build`")
+    lib = ctypes.CDLL(str(p), mode=os.RTLD_LOCAL)
+    vp, ip, dp, fp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_void_p, ctypes.c_void_p
+    c_int, c_double = ctypes.c_int, ctypes.c_double
+    lib.qwsg_last_error.restype = ctypes.c_char_p
+    lib.qwsg_version.restype = ctypes.c_char_p
+    sig = {
+        "qwsg_create": [ctypes.POINTER(vp), ip, ip, c_int],
+        "qwsg_destroy": [vp],
+        "qwsg_set_stream": [vp, vp],
+        "qwsg_set_kappa": [vp, c_double],
+        "qwsg_geometry": [vp, ip, ip],
+        "qwsg_sync": [vp],
+        "qwsg_load_gauge": [vp, dp],
+        "qwsg_load_clover": [vp, dp],
+        "qwsg_load_gauge_s": [vp, fp],
+        "qwsg_load_clover_s": [vp, fp],
+        "qwsg_spinor_to_device_d": [vp, vp, dp],
+        "qwsg_spinor_to_host_d": [vp, dp, vp],
+        "qwsg_spinor_to_device_s": [vp, vp, fp],
+        "qwsg_spinor_to_host_s": [vp, fp, vp],
+        "qwsg_ddd_d": [vp, vp, vp],
+        "qwsg_ddd_s": [vp, vp, vp],
+        "qwsg_ddd_in_d": [vp, vp, vp, c_int],
+        "qwsg_ddd_in_s": [vp, vp, vp, c_int],
+        "qwsg_ddd_out_d": [vp, vp, vp, c_int, c_double],
+        "qwsg_ddd_out_s": [vp, vp, vp, c_int, c_double],
+        "qwsg_jinv_s": [vp, vp, vp, c_int, c_int],
+        "qwsg_prec_ddd_s": [vp, vp, vp, c_int, c_int],
+        "qwsg_prec_s": [vp, vp, vp, c_int, c_int],
+        "qwsg_bicgstab_precdd_s": [vp, vp, vp, c_double, c_int, c_int, c_int, ip,
+                                   ctypes.POINTER(c_double)],
+        "qwsg_bicgstab_dd_mix": [vp, vp, vp, c_double, c_int, c_double, c_int, c_int, c_int,
+                                 ctypes.POINTER(SolveStats)],
+        "qwsg_true_residual": [vp, vp, vp, ctypes.POINTER(c_double)],
+        "qwsg_counters": [vp] + [ctypes.POINTER(ctypes.c_long)] * 5,
+        "qwsg_kernel_timing": [vp, c_int],
+        "qwsg_kernel_stats": [vp, ip, vp, vp, vp],
+        "qwsg_gen_gauge": [vp, ip, ctypes.c_ulonglong, c_int, c_double, ctypes.POINTER(c_double)],
+        "qwsg_plaquette": [vp, ip, ctypes.POINTER(c_double)],
+        "qwsg_gen_clover": [vp, vp, ip, c_double, c_double, vp],
+        "qwsg_gen_source": [vp, ip, ctypes.c_ulonglong, c_int, c_int],
+    }
+    for name, args in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = c_int
+    lib.qwsg_kernel_name.restype = ctypes.c_char_p
+    lib.qwsg_kernel_name.argtypes = [c_int]
+    _lib = lib
+    return lib
+
+
+def _L4(L):
+    return (ctypes.c_int * 4)(*map(int, L))
+
+
+def gen_gauge(L, seed=1, n_smear=5, alpha=0.36):
+    """Seeded SU(3) links smoothed by n_smear APE-style steps (natural layout
+    [4, V, 18] FP64).  Returns (U, plaquette)."""
+    lib = load_library()
+    V = int(np.prod(L))
+    U = np.empty((4, V, 18), np.float64)
+    p = ctypes.c_double()
+    _check(lib.qwsg_gen_gauge(U.ctypes.data_as(ctypes.c_void_p), _L4(L), int(seed), int(n_smear),
+                              float(alpha), ctypes.byref(p)))
+    return U, p.value
+
+
+def plaquette(U, L):
+    lib = load_library()
+    U = np.ascontiguousarray(U, np.float64)
+    p = ctypes.c_double()
+    _check(lib.qwsg_plaquette(U.ctypes.data_as(ctypes.c_void_p), _L4(L), ctypes.byref(p)))
+    return p.value
+
+
+def gen_clover(U, L, csw, kappa, with_T=False):
+    """Clover-leaf clover term; returns the packed inverse [V, 72] (and T)."""
+    lib = load_library()
+    V = int(np.prod(L))
+    U = np.ascontiguousarray(U, np.float64)
+    C = np.empty((V, 72), np.float64)
+    T = np.empty((V, 12, 12, 2), np.float64) if with_T else None
+    _check(lib.qwsg_gen_clover(C.ctypes.data_as(ctypes.c_void_p), U.ctypes.data_as(ctypes.c_void_p),
+                               _L4(L), float(csw), float(kappa),
+                               T.ctypes.data_as(ctypes.c_void_p) if with_T else None))
+    return (C, T) if with_T else C
+
+
+def gen_source(L, seed=2, kind="gauss", arg=0):
+    """Sources in natural layout [V, 24]: kind gauss | point (arg = 4*colour+spin) | z2."""
+    lib = load_library()
+    V = int(np.prod(L))
+    S = np.empty((V, 24), np.float64)
+    k = {"gauss": 0, "point": 1, "z2": 2}[kind]
+    _check(lib.qwsg_gen_source(S.ctypes.data_as(ctypes.c_void_p), _L4(L), int(seed), k, int(arg)))
+    return S
+
+
+def _check(rc):
+    if rc != 0:
+        raise QwsgError(f"qwsg error {rc}: {_lib.qwsg_last_error().decode()}")
+
+
+def _ptr(t):
+    """Device pointer of a torch tensor (or an int address)."""
+    if isinstance(t, int):
+        return ctypes.c_void_p(t)
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _host(a, dtype):
+    a = np.ascontiguousarray(a, dtype=dtype)
+    return a, a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Lattice:
+    """One lattice resident on the current CUDA device.
+
+    L: global extents (x, y, z, t); NB: SAP block grid (NB[0] even;
+    the reference's partition on rank grid npe is (2*npe0, npe1, npe2, npe3));
+    tbc: +1/-1 time boundary; kappa: hopping parameter.
+    """
+
+    def __init__(self, L, NB=(2, 1, 1, 1), tbc=-1, kappa=0.0, stream=None):
+        import torch
+        self.torch = torch
+        self.lib = load_library()
+        self.L, self.NB = tuple(map(int, L)), tuple(map(int, NB))
+        h = ctypes.c_void_p()
+        arr = lambda v: (ctypes.c_int * 4)(*v)
+        _check(self.lib.qwsg_create(ctypes.byref(h), arr(self.L), arr(self.NB), int(tbc)))
+        self.h = h
+        V, pad = ctypes.c_int(), ctypes.c_int()
+        _check(self.lib.qwsg_geometry(self.h, ctypes.byref(V), ctypes.byref(pad)))
+        self.V, self.pad = V.value, pad.value
+        self.set_kappa(kappa)
+        self.set_stream(stream if stream is not None else torch.cuda.current_stream())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.qwsg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- configuration -----------------------------------------------------
+    def set_stream(self, stream):
+        handle = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        _check(self.lib.qwsg_set_stream(self.h, ctypes.c_void_p(handle)))
+
+    def set_kappa(self, kappa):
+        self.kappa = float(kappa)
+        _check(self.lib.qwsg_set_kappa(self.h, self.kappa))
+
+    def load_fields(self, U, C, Us=None, Cs=None):
+        """U natural [4,V,3,3,2] FP64, C natural [V,72] FP64 (inverse clover, QWS packing)."""
+        U, pu = _host(U, np.float64)
+        C, pc = _host(C, np.float64)
+        assert U.size == 72 * self.V and C.size == 72 * self.V
+        _check(self.lib.qwsg_load_gauge(self.h, pu))
+        _check(self.lib.qwsg_load_clover(self.h, pc))
+        if Us is not None:
+            Us, p = _host(Us, np.float32)
+            _check(self.lib.qwsg_load_gauge_s(self.h, p))
+        if Cs is not None:
+            Cs, p = _host(Cs, np.float32)
+            _check(self.lib.qwsg_load_clover_s(self.h, p))
+
+    # ---- buffers -----------------------------------------------------------
+    def empty(self, dtype="f32"):
+        t = self.torch.float32 if dtype in ("f32", np.float32) else self.torch.float64
+        return self.torch.zeros(24 * self.pad, dtype=t, device="cuda")
+
+    def to_device(self, v, out=None):
+        v = np.asarray(v)
+        if v.dtype == np.float64:
+            out = self.empty("f64") if out is None else out
+            a, p = _host(v, np.float64)
+            _check(self.lib.qwsg_spinor_to_device_d(self.h, _ptr(out), p))
+        else:
+            out = self.empty("f32") if out is None else out
+            a, p = _host(v, np.float32)
+            _check(self.lib.qwsg_spinor_to_device_s(self.h, _ptr(out), p))
+        return out
+
+    def to_host(self, t, out=None):
+        """Device planes -> host natural layout (into `out` if given, e.g. pinned)."""
+        if t.dtype == self.torch.float64:
+            a = np.empty((self.V, 24), np.float64) if out is None else out
+            assert a.dtype == np.float64 and a.flags.c_contiguous and a.size == 24 * self.V
+            _check(self.lib.qwsg_spinor_to_host_d(self.h, a.ctypes.data_as(ctypes.c_void_p), _ptr(t)))
+        else:
+            a = np.empty((self.V, 24), np.float32) if out is None else out
+            assert a.dtype == np.float32 and a.flags.c_contiguous and a.size == 24 * self.V
+            _check(self.lib.qwsg_spinor_to_host_s(self.h, a.ctypes.data_as(ctypes.c_void_p), _ptr(t)))
+        return a
+
+    def sync(self):
+        _check(self.lib.qwsg_sync(self.h))
+
+    # ---- operators (device tensors in, device tensors out) -----------------
+    def _out(self, x, out):
+        return self.torch.zeros_like(x) if out is None else out
+
+    def ddd(self, x, out=None):
+        out = self._out(x, out)
+        fn = self.lib.qwsg_ddd_d if x.dtype == self.torch.float64 else self.lib.qwsg_ddd_s
+        _check(fn(self.h, _ptr(out), _ptr(x)))
+        return out
+
+    def ddd_in(self, x, colour, out=None):
+        out = self._out(x, out)
+        fn = self.lib.qwsg_ddd_in_d if x.dtype == self.torch.float64 else self.lib.qwsg_ddd_in_s
+        _check(fn(self.h, _ptr(out), _ptr(x), int(colour)))
+        return out
+
+    def ddd_out(self, x, colour, factor, out=None):
+        out = self._out(x, out)
+        fn = self.lib.qwsg_ddd_out_d if x.dtype == self.torch.float64 else self.lib.qwsg_ddd_out_s
+        _check(fn(self.h, _ptr(out), _ptr(x), int(colour), float(factor)))
+        return out
+
+    def jinv(self, b, colour, nm, out=None):
+        out = self._out(b, out)
+        _check(self.lib.qwsg_jinv_s(self.h, _ptr(out), _ptr(b), int(colour), int(nm)))
+        return out
+
+    def prec_ddd(self, x, nsap=4, nm=2, out=None):
+        out = self._out(x, out)
+        _check(self.lib.qwsg_prec_ddd_s(self.h, _ptr(out), _ptr(x), int(nsap), int(nm)))
+        return out
+
+    def prec(self, x, nsap=4, nm=2, out=None):
+        out = self._out(x, out)
+        _check(self.lib.qwsg_prec_s(self.h, _ptr(out), _ptr(x), int(nsap), int(nm)))
+        return out
+
+    def bicgstab_precdd(self, b, tol, maxiter, nsap=4, nm=2, out=None):
+        out = self._out(b, out)
+        it, rel = ctypes.c_int(), ctypes.c_double()
+        _check(self.lib.qwsg_bicgstab_precdd_s(self.h, _ptr(out), _ptr(b), float(tol), int(maxiter),
+                                               int(nsap), int(nm), ctypes.byref(it),
+                                               ctypes.byref(rel)))
+        return out, it.value, rel.value
+
+    def bicgstab_dd_mix(self, x, b, tol, maxiter, tol_s, maxiter_s, nsap=4, nm=2):
+        """Solve D x = b in place (x holds the initial guess)."""
+        st = SolveStats()
+        _check(self.lib.qwsg_bicgstab_dd_mix(self.h, _ptr(x), _ptr(b), float(tol), int(maxiter),
+                                             float(tol_s), int(maxiter_s), int(nsap), int(nm),
+                                             ctypes.byref(st)))
+        return st.as_dict()
+
+    def true_residual(self, x, b):
+        r = ctypes.c_double()
+        _check(self.lib.qwsg_true_residual(self.h, _ptr(x), _ptr(b), ctypes.byref(r)))
+        return r.value
+
+    def kernel_timing(self, enable=True):
+        _check(self.lib.qwsg_kernel_timing(self.h, 1 if enable else 0))
+
+    def kernel_stats(self):
+        """{kernel name: (launches, total device ms, algorithmic bytes)} since enabling."""
+        n = ctypes.c_int(16)
+        L = (ctypes.c_long * 16)()
+        ms = (ctypes.c_double * 16)()
+        by = (ctypes.c_double * 16)()
+        _check(self.lib.qwsg_kernel_stats(self.h, ctypes.byref(n), L, ms, by))
+        return {self.lib.qwsg_kernel_name(k).decode(): (L[k], ms[k], by[k]) for k in range(n.value)
+                if L[k] > 0}
+
+    def counters(self):
+        v = [ctypes.c_long() for _ in range(5)]
+        _check(self.lib.qwsg_counters(self.h, *[ctypes.byref(x) for x in v]))
+        return dict(zip(("prec_ddd_s", "prec_s", "jinv", "inner_iters", "ddd_d"), [x.value for x in v]))

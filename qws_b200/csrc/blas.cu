@@ -1,0 +1,370 @@
+// BLAS-1 kernels on spinor planes for the BiCGStab loops, with the dot
+// products and norms fused into the update kernels that produce their inputs
+// (bicgstab_precdd_s.cc:223-543, bicgstab_dd_mix.cc:140-368).
+//
+// Reductions: every thread accumulates in FP64, warps reduce with shuffles,
+// each block writes one partial; the last block to finish (threadfence +
+// counter) sums the partials in a fixed order with double-double (two-sum)
+// arithmetic, so results are deterministic run to run and compensated.
+#include "kernels.h"
+
+namespace qwsg {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+template <typename R>
+struct V4 {
+  R x, y, z, w;
+};
+
+template <typename R>
+__device__ __forceinline__ V4<R> ld4(const R* __restrict__ p, int pad, int g, int j);
+template <>
+__device__ __forceinline__ V4<float> ld4<float>(const float* __restrict__ p, int pad, int g, int j) {
+  float4 t = reinterpret_cast<const float4*>(p)[(size_t)j * pad + g];
+  return {t.x, t.y, t.z, t.w};
+}
+template <>
+__device__ __forceinline__ V4<double> ld4<double>(const double* __restrict__ p, int pad, int g,
+                                                  int j) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+  double2 a = q[(size_t)(2 * j) * pad + g], b = q[(size_t)(2 * j + 1) * pad + g];
+  return {a.x, a.y, b.x, b.y};
+}
+template <typename R>
+__device__ __forceinline__ void st4(R* p, int pad, int g, int j, V4<R> v);
+template <>
+__device__ __forceinline__ void st4<float>(float* p, int pad, int g, int j, V4<float> v) {
+  reinterpret_cast<float4*>(p)[(size_t)j * pad + g] = make_float4(v.x, v.y, v.z, v.w);
+}
+template <>
+__device__ __forceinline__ void st4<double>(double* p, int pad, int g, int j, V4<double> v) {
+  double2* q = reinterpret_cast<double2*>(p);
+  q[(size_t)(2 * j) * pad + g] = make_double2(v.x, v.y);
+  q[(size_t)(2 * j + 1) * pad + g] = make_double2(v.z, v.w);
+}
+
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+  s = a + b;
+  double bp = s - a;
+  e = (a - (s - bp)) + (b - bp);
+}
+
+__device__ __forceinline__ void dd_add(double& hi, double& lo, double bhi, double blo) {
+  double s, e;
+  two_sum(hi, bhi, s, e);
+  e += lo + blo;
+  hi = s + e;
+  lo = e - (hi - s);
+}
+
+template <int NR>
+__device__ void finish_reduction(const double (&v)[8], RedBuf rb, double* res) {
+  __shared__ double sh[kThreads / 32][NR > 0 ? NR : 1];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NR; k++) {
+    double x = v[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) sh[warp][k] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NR; k++) {
+      double x = 0;
+      for (int w = 0; w < kThreads / 32; w++) x += sh[w][k];
+      rb.partial[blockIdx.x * 8 + k] = x;
+    }
+    __threadfence();
+    unsigned done = atomicAdd(rb.counter, 1u);
+    last = (done == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // last block: compensated sum of the partials in block order
+#pragma unroll
+  for (int k = 0; k < NR; k++) {
+    double hi = 0, lo = 0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += kThreads) {
+      double x = *((volatile double*)&rb.partial[b * 8 + k]);
+      dd_add(hi, lo, x, 0.0);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      double h2 = __shfl_down_sync(0xffffffffu, hi, o);
+      double l2 = __shfl_down_sync(0xffffffffu, lo, o);
+      dd_add(hi, lo, h2, l2);
+    }
+    __shared__ double shh[kThreads / 32], shl[kThreads / 32];
+    if (lane == 0) {
+      shh[warp] = hi;
+      shl[warp] = lo;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double H = 0, Lo = 0;
+      for (int w = 0; w < kThreads / 32; w++) dd_add(H, Lo, shh[w], shl[w]);
+      res[k] = H + Lo;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *rb.counter = 0;
+}
+
+// ---- per-site operations ---------------------------------------------------
+template <typename R, int NR, typename Op>
+__global__ void __launch_bounds__(kThreads) k_sites(Geom G, Op op, RedBuf rb, double* res) {
+  double acc[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) acc[k] = 0;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G.V; g += gridDim.x * blockDim.x)
+    op(G, g, acc);
+  if constexpr (NR > 0) finish_reduction<NR>(acc, rb, res);
+}
+
+template <typename R>
+struct OpNorm2 {
+  const R* x;
+  __device__ void operator()(const Geom& G, int g, double* acc) const {
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+      V4<R> a = ld4(x, G.pad, g, j);
+      acc[0] += (double)a.x * a.x + (double)a.y * a.y + (double)a.z * a.z + (double)a.w * a.w;
+    }
+  }
+};
+
+template <typename R>
+struct OpCdot {
+  const R *x, *y;
+  __device__ void operator()(const Geom& G, int g, double* acc) const {
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+      V4<R> a = ld4(x, G.pad, g, j), b = ld4(y, G.pad, g, j);
+      acc[0] += (double)a.x * b.x + (double)a.y * b.y + (double)a.z * b.z + (double)a.w * b.w;
+      acc[1] += (double)a.x * b.y - (double)a.y * b.x + (double)a.z * b.w - (double)a.w * b.z;
+    }
+  }
+};
+
+template <typename R>
+struct OpNormCdot {  // |y|^2, <y, x>
+  const R *y, *x;
+  __device__ void operator()(const Geom& G, int g, double* acc) const {
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+      V4<R> a = ld4(y, G.pad, g, j), b = ld4(x, G.pad, g, j);
+      acc[0] += (double)a.x * a.x + (double)a.y * a.y + (double)a.z * a.z + (double)a.w * a.w;
+      acc[1] += (double)a.x * b.x + (double)a.y * b.y + (double)a.z * b.z + (double)a.w * b.w;
+      acc[2] += (double)a.x * b.y - (double)a.y * b.x + (double)a.z * b.w - (double)a.w * b.z;
+    }
+  }
+};
+
+// x += a p ; r -= a q ; |r|^2 (+ <r0, r> when r0 != nullptr)
+template <typename R>
+struct OpBicgUpdate {
+  R *x, *r;
+  const R *p, *q, *r0;
+  R ar, ai;
+  __device__ void operator()(const Geom& G, int g, double* acc) const {
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+      V4<R> X = ld4<R>(x, G.pad, g, j), Rr = ld4<R>(r, G.pad, g, j);
+      V4<R> P = ld4(p, G.pad, g, j), Q = ld4(q, G.pad, g, j);
+      X.x = X.x + ar * P.x - ai * P.y;
+      X.y = X.y + ar * P.y + ai * P.x;
+      X.z = X.z + ar * P.z - ai * P.w;
+      X.w = X.w + ar * P.w + ai * P.z;
+      Rr.x = Rr.x - ar * Q.x + ai * Q.y;
+      Rr.y = Rr.y - ar * Q.y - ai * Q.x;
+      Rr.z = Rr.z - ar * Q.z + ai * Q.w;
+      Rr.w = Rr.w - ar * Q.w - ai * Q.z;
+      st4<R>(x, G.pad, g, j, X);
+      st4<R>(r, G.pad, g, j, Rr);
+      acc[0] += (double)Rr.x * Rr.x + (double)Rr.y * Rr.y + (double)Rr.z * Rr.z +
+                (double)Rr.w * Rr.w;
+      if (r0) {
+        V4<R> A = ld4(r0, G.pad, g, j);
+        acc[1] += (double)A.x * Rr.x + (double)A.y * Rr.y + (double)A.z * Rr.z + (double)A.w * Rr.w;
+        acc[2] += (double)A.x * Rr.y - (double)A.y * Rr.x + (double)A.z * Rr.w - (double)A.w * Rr.z;
+      }
+    }
+  }
+};
+
+// p = r + b (p - w q)   (bicgstab_precdd_s.cc:528-543)
+template <typename R>
+struct OpBicgP {
+  R* p;
+  const R *r, *q;
+  R br, bi, wr, wi;
+  __device__ void operator()(const Geom& G, int g, double*) const {
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+      V4<R> P = ld4<R>(p, G.pad, g, j), Rr = ld4(r, G.pad, g, j), Q = ld4(q, G.pad, g, j);
+      R c0 = P.x - wr * Q.x + wi * Q.y, c1 = P.y - wr * Q.y - wi * Q.x;
+      R c2 = P.z - wr * Q.z + wi * Q.w, c3 = P.w - wr * Q.w - wi * Q.z;
+      P.x = br * c0 - bi * c1 + Rr.x;
+      P.y = br * c1 + bi * c0 + Rr.y;
+      P.z = br * c2 - bi * c3 + Rr.z;
+      P.w = br * c3 + bi * c2 + Rr.w;
+      st4<R>(p, G.pad, g, j, P);
+    }
+  }
+};
+
+// r = b - q ; p = r ; r0 = r ; |b|^2 ; |r|^2  (bicgstab_dd_mix.cc:140-152)
+template <typename R>
+struct OpBicgInit {
+  const R *b, *q;
+  R *r, *p, *r0;
+  __device__ void operator()(const Geom& G, int g, double* acc) const {
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+      V4<R> B = ld4(b, G.pad, g, j), Q;
+      if (q)
+        Q = ld4(q, G.pad, g, j);
+      else
+        Q = {0, 0, 0, 0};
+      V4<R> Rr = {B.x - Q.x, B.y - Q.y, B.z - Q.z, B.w - Q.w};
+      st4<R>(r, G.pad, g, j, Rr);
+      st4<R>(p, G.pad, g, j, Rr);
+      st4<R>(r0, G.pad, g, j, Rr);
+      acc[0] += (double)B.x * B.x + (double)B.y * B.y + (double)B.z * B.z + (double)B.w * B.w;
+      acc[1] += (double)Rr.x * Rr.x + (double)Rr.y * Rr.y + (double)Rr.z * Rr.z +
+                (double)Rr.w * Rr.w;
+    }
+  }
+};
+
+struct OpD2S {
+  float* y;
+  const double* x;
+  double s;
+  __device__ void operator()(const Geom& G, int g, double*) const {
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+      V4<double> a = ld4(x, G.pad, g, j);
+      st4<float>(y, G.pad, g, j,
+                 {(float)(a.x * s), (float)(a.y * s), (float)(a.z * s), (float)(a.w * s)});
+    }
+  }
+};
+
+struct OpS2D {
+  double* y;
+  const float* x;
+  double s;
+  __device__ void operator()(const Geom& G, int g, double*) const {
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+      V4<float> a = ld4(x, G.pad, g, j);
+      st4<double>(y, G.pad, g, j,
+                  {(double)a.x * s, (double)a.y * s, (double)a.z * s, (double)a.w * s});
+    }
+  }
+};
+
+int grid_for(const Geom& G, const RedBuf* rb) {
+  int b = (G.V + kThreads - 1) / kThreads;
+  int cap = rb ? rb->nblk : 148 * 8;
+  return b < cap ? b : cap;
+}
+
+template <typename R, int NR, typename Op>
+void run(const Geom& G, Op op, RedBuf* rb, double* res, cudaStream_t st) {
+  RedBuf dummy{nullptr, nullptr, 0};
+  k_sites<R, NR, Op><<<grid_for(G, rb), kThreads, 0, st>>>(G, op, rb ? *rb : dummy, res);
+}
+
+template <typename R>
+__global__ void k_copy(Geom G, R* y, const R* x, int site0, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int g = site0 + i;
+#pragma unroll
+  for (int j = 0; j < 6; j++) st4<R>(y, G.pad, g, j, ld4<R>(x, G.pad, g, j));
+}
+template <typename R>
+__global__ void k_zero(Geom G, R* y, int site0, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int g = site0 + i;
+#pragma unroll
+  for (int j = 0; j < 6; j++) st4<R>(y, G.pad, g, j, {0, 0, 0, 0});
+}
+
+}  // namespace
+
+template <typename R>
+void blas_copy(const Geom& G, R* y, const R* x, int site0, int n, cudaStream_t st) {
+  if (n > 0) k_copy<R><<<(n + 255) / 256, 256, 0, st>>>(G, y, x, site0, n);
+}
+template <typename R>
+void blas_zero(const Geom& G, R* y, int site0, int n, cudaStream_t st) {
+  if (n > 0) k_zero<R><<<(n + 255) / 256, 256, 0, st>>>(G, y, site0, n);
+}
+template <typename R>
+void blas_norm2(const Geom& G, const R* x, double* res, RedBuf& rb, cudaStream_t st) {
+  run<R, 1>(G, OpNorm2<R>{x}, &rb, res, st);
+}
+template <typename R>
+void blas_cdot(const Geom& G, const R* x, const R* y, double* res, RedBuf& rb, cudaStream_t st) {
+  run<R, 2>(G, OpCdot<R>{x, y}, &rb, res, st);
+}
+template <typename R>
+void blas_norm_cdot(const Geom& G, const R* y, const R* x, double* res, RedBuf& rb,
+                    cudaStream_t st) {
+  run<R, 3>(G, OpNormCdot<R>{y, x}, &rb, res, st);
+}
+template <typename R>
+void blas_bicg_update(const Geom& G, R* x, R* r, const R* p, const R* q, double ar, double ai,
+                      const R* r0, double* res, RedBuf& rb, cudaStream_t st) {
+  OpBicgUpdate<R> op{x, r, p, q, r0, (R)ar, (R)ai};
+  if (r0)
+    run<R, 3>(G, op, &rb, res, st);
+  else
+    run<R, 1>(G, op, &rb, res, st);
+}
+template <typename R>
+void blas_bicg_p(const Geom& G, R* p, const R* r, const R* q, double br, double bi, double wr,
+                 double wi, cudaStream_t st) {
+  run<R, 0>(G, OpBicgP<R>{p, r, q, (R)br, (R)bi, (R)wr, (R)wi}, nullptr, nullptr, st);
+}
+template <typename R>
+void blas_bicg_init(const Geom& G, const R* b, const R* q, R* r, R* p, R* r0, double* res,
+                    RedBuf& rb, cudaStream_t st) {
+  run<R, 2>(G, OpBicgInit<R>{b, q, r, p, r0}, &rb, res, st);
+}
+void blas_d2s(const Geom& G, float* y, const double* x, double s, cudaStream_t st) {
+  run<float, 0>(G, OpD2S{y, x, s}, nullptr, nullptr, st);
+}
+void blas_s2d(const Geom& G, double* y, const float* x, double s, cudaStream_t st) {
+  run<float, 0>(G, OpS2D{y, x, s}, nullptr, nullptr, st);
+}
+
+#define QWSG_INST(R)                                                                         \
+  template void blas_copy<R>(const Geom&, R*, const R*, int, int, cudaStream_t);             \
+  template void blas_zero<R>(const Geom&, R*, int, int, cudaStream_t);                       \
+  template void blas_norm2<R>(const Geom&, const R*, double*, RedBuf&, cudaStream_t);        \
+  template void blas_cdot<R>(const Geom&, const R*, const R*, double*, RedBuf&, cudaStream_t); \
+  template void blas_norm_cdot<R>(const Geom&, const R*, const R*, double*, RedBuf&,         \
+                                  cudaStream_t);                                             \
+  template void blas_bicg_update<R>(const Geom&, R*, R*, const R*, const R*, double, double, \
+                                    const R*, double*, RedBuf&, cudaStream_t);               \
+  template void blas_bicg_p<R>(const Geom&, R*, const R*, const R*, double, double, double,  \
+                               double, cudaStream_t);                                        \
+  template void blas_bicg_init<R>(const Geom&, const R*, const R*, R*, R*, R*, double*,      \
+                                  RedBuf&, cudaStream_t);
+QWSG_INST(float)
+QWSG_INST(double)
+#undef QWSG_INST
+
+}  // namespace qwsg

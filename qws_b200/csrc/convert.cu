@@ -1,0 +1,262 @@
+// Layout converters between host formats and the device planes.
+//
+// QWS host layout (qws.h:111-192; main.cc:426-429; reordering.cc:59-105):
+// the (single-rank) lattice is split into two x-halves ("domains") of
+// nxh = Lx/2 sites; inside a domain sites are vectors of `vlen` consecutive x
+// sites (SIMD lanes):
+//   elem  = dom*vol + xv + nxv*(y + Ly*(z + Lz*t)),  nxv = nxh/vlen
+//   spinor real r (0..23, order [colour][spin][re,im]) at (elem*24 + r)*vlen + lane
+//   link   (dom*4 + mu)*vol + ...; U[row][col] stored column-major c[col][row]:
+//          ((elem*18) + (col*3 + row)*2 + ri)*vlen + lane
+//   clover real j (0..71) at (elem*72 + j)*vlen + lane
+// Natural layout: site n = x + Lx*(y + Ly*(z + Lz*t)); spinor [n][24],
+// gauge [mu][n][row][col][2], clover [n][72].
+// Every converter runs one thread per device site and is a pure gather/scatter.
+#include "kernels.h"
+
+namespace qwsg {
+
+namespace {
+
+struct QwsIdx {
+  long elem_sp;  // spinor / clover element
+  long elem_g0;  // link element for mu = 0 (add mu*vol)
+  long vol;
+  int lane;
+};
+
+__device__ __forceinline__ void global_coords(const Geom& G, int g, int x[4]) {
+  Site s;
+  decode_site(G, g, s);
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++) x[mu] = s.bc[mu] * G.B[mu] + s.lc[mu];
+}
+
+__device__ __forceinline__ QwsIdx qws_index(const Geom& G, const int x[4], int vlen) {
+  int nxh = G.L[0] / 2, nxv = nxh / vlen;
+  int dom = x[0] / nxh, xh = x[0] - dom * nxh;
+  long vol = (long)nxv * G.L[1] * G.L[2] * G.L[3];
+  long in_dom = xh / vlen + (long)nxv * (x[1] + (long)G.L[1] * (x[2] + (long)G.L[2] * x[3]));
+  QwsIdx q;
+  q.elem_sp = dom * vol + in_dom;
+  q.elem_g0 = dom * 4 * vol + in_dom;
+  q.vol = vol;
+  q.lane = xh % vlen;
+  return q;
+}
+
+__device__ __forceinline__ long nat_index(const Geom& G, const int x[4]) {
+  return x[0] + (long)G.L[0] * (x[1] + (long)G.L[1] * (x[2] + (long)G.L[2] * x[3]));
+}
+
+template <typename R>
+__device__ __forceinline__ void store_sp(R* p, int pad, int g, const R v[24]) {
+  IO<R>::store_spinor(p, pad, g, v);
+}
+
+template <typename R>
+__global__ void k_qws2pl_sp(Geom G, R* dst, const R* __restrict__ q, int vlen, int site0, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int g = site0 + i, x[4];
+  global_coords(G, g, x);
+  QwsIdx Q = qws_index(G, x, vlen);
+  R v[24];
+#pragma unroll
+  for (int r = 0; r < 24; r++) v[r] = q[(Q.elem_sp * 24 + r) * vlen + Q.lane];
+  store_sp(dst, G.pad, g, v);
+}
+
+template <typename R>
+__global__ void k_pl2qws_sp(Geom G, R* q, const R* __restrict__ src, int vlen, int site0, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int g = site0 + i, x[4];
+  global_coords(G, g, x);
+  QwsIdx Q = qws_index(G, x, vlen);
+  R v[24];
+  IO<R>::load_spinor(src, G.pad, g, v);
+#pragma unroll
+  for (int r = 0; r < 24; r++) q[(Q.elem_sp * 24 + r) * vlen + Q.lane] = v[r];
+}
+
+template <typename R>
+__device__ __forceinline__ void store_link(R* p, int pad, int mu, int g, const R u[18]);
+template <>
+__device__ __forceinline__ void store_link<float>(float* p, int pad, int mu, int g,
+                                                  const float u[18]) {
+  float2* q = reinterpret_cast<float2*>(p);
+#pragma unroll
+  for (int e = 0; e < 9; e++) q[(size_t)(mu * 9 + e) * pad + g] = make_float2(u[2 * e], u[2 * e + 1]);
+}
+template <>
+__device__ __forceinline__ void store_link<double>(double* p, int pad, int mu, int g,
+                                                   const double u[18]) {
+  double2* q = reinterpret_cast<double2*>(p);
+#pragma unroll
+  for (int e = 0; e < 9; e++)
+    q[(size_t)(mu * 9 + e) * pad + g] = make_double2(u[2 * e], u[2 * e + 1]);
+}
+
+template <typename R>
+__device__ __forceinline__ void store_clover(R* p, int pad, int g, const R a[72]);
+template <>
+__device__ __forceinline__ void store_clover<float>(float* p, int pad, int g, const float a[72]) {
+  float4* q = reinterpret_cast<float4*>(p);
+#pragma unroll
+  for (int j = 0; j < 18; j++)
+    q[(size_t)j * pad + g] = make_float4(a[4 * j], a[4 * j + 1], a[4 * j + 2], a[4 * j + 3]);
+}
+template <>
+__device__ __forceinline__ void store_clover<double>(double* p, int pad, int g, const double a[72]) {
+  double2* q = reinterpret_cast<double2*>(p);
+#pragma unroll
+  for (int j = 0; j < 36; j++) q[(size_t)j * pad + g] = make_double2(a[2 * j], a[2 * j + 1]);
+}
+
+template <typename R>
+__global__ void k_qws2pl_gauge(Geom G, R* dst, const R* __restrict__ q, int vlen) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G.V) return;
+  int x[4];
+  global_coords(G, g, x);
+  QwsIdx Q = qws_index(G, x, vlen);
+  for (int mu = 0; mu < 4; mu++) {
+    long elem = Q.elem_g0 + mu * Q.vol;
+    R u[18];
+#pragma unroll
+    for (int row = 0; row < 3; row++)
+#pragma unroll
+      for (int col = 0; col < 3; col++)
+#pragma unroll
+        for (int ri = 0; ri < 2; ri++)
+          u[2 * (3 * row + col) + ri] = q[(elem * 18 + (col * 3 + row) * 2 + ri) * vlen + Q.lane];
+    store_link<R>(dst, G.pad, mu, g, u);
+  }
+}
+
+template <typename R>
+__global__ void k_qws2pl_clover(Geom G, R* dst, const R* __restrict__ q, int vlen) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G.V) return;
+  int x[4];
+  global_coords(G, g, x);
+  QwsIdx Q = qws_index(G, x, vlen);
+  R a[72];
+#pragma unroll
+  for (int j = 0; j < 72; j++) a[j] = q[(Q.elem_sp * 72 + j) * vlen + Q.lane];
+  store_clover<R>(dst, G.pad, g, a);
+}
+
+template <typename R>
+__global__ void k_nat2pl_sp(Geom G, R* dst, const R* __restrict__ nat) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G.V) return;
+  int x[4];
+  global_coords(G, g, x);
+  long n = nat_index(G, x);
+  R v[24];
+#pragma unroll
+  for (int r = 0; r < 24; r++) v[r] = nat[n * 24 + r];
+  store_sp(dst, G.pad, g, v);
+}
+
+template <typename R>
+__global__ void k_pl2nat_sp(Geom G, R* nat, const R* __restrict__ src) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G.V) return;
+  int x[4];
+  global_coords(G, g, x);
+  long n = nat_index(G, x);
+  R v[24];
+  IO<R>::load_spinor(src, G.pad, g, v);
+#pragma unroll
+  for (int r = 0; r < 24; r++) nat[n * 24 + r] = v[r];
+}
+
+template <typename Rin, typename R>
+__global__ void k_nat2pl_gauge(Geom G, R* dst, const Rin* __restrict__ nat) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G.V) return;
+  int x[4];
+  global_coords(G, g, x);
+  long n = nat_index(G, x);
+  for (int mu = 0; mu < 4; mu++) {
+    R u[18];
+#pragma unroll
+    for (int e = 0; e < 18; e++) u[e] = (R)nat[((long)mu * G.V + n) * 18 + e];
+    store_link<R>(dst, G.pad, mu, g, u);
+  }
+}
+
+template <typename Rin, typename R>
+__global__ void k_nat2pl_clover(Geom G, R* dst, const Rin* __restrict__ nat) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G.V) return;
+  int x[4];
+  global_coords(G, g, x);
+  long n = nat_index(G, x);
+  R a[72];
+#pragma unroll
+  for (int j = 0; j < 72; j++) a[j] = (R)nat[n * 72 + j];
+  store_clover<R>(dst, G.pad, g, a);
+}
+
+inline int nb(long n) { return (int)((n + 127) / 128); }
+
+}  // namespace
+
+template <typename R>
+void qws_to_planes_spinor(const Geom& G, R* dst, const R* qws, int vlen, int site0, int n,
+                          cudaStream_t st) {
+  if (n > 0) k_qws2pl_sp<R><<<nb(n), 128, 0, st>>>(G, dst, qws, vlen, site0, n);
+}
+template <typename R>
+void planes_to_qws_spinor(const Geom& G, R* qws, const R* src, int vlen, int site0, int n,
+                          cudaStream_t st) {
+  if (n > 0) k_pl2qws_sp<R><<<nb(n), 128, 0, st>>>(G, qws, src, vlen, site0, n);
+}
+template <typename R>
+void qws_to_planes_gauge(const Geom& G, R* dst, const R* qws, int vlen, cudaStream_t st) {
+  k_qws2pl_gauge<R><<<nb(G.V), 128, 0, st>>>(G, dst, qws, vlen);
+}
+template <typename R>
+void qws_to_planes_clover(const Geom& G, R* dst, const R* qws, int vlen, cudaStream_t st) {
+  k_qws2pl_clover<R><<<nb(G.V), 128, 0, st>>>(G, dst, qws, vlen);
+}
+template <typename R>
+void nat_to_planes_spinor(const Geom& G, R* dst, const R* nat, cudaStream_t st) {
+  k_nat2pl_sp<R><<<nb(G.V), 128, 0, st>>>(G, dst, nat);
+}
+template <typename R>
+void planes_to_nat_spinor(const Geom& G, R* nat, const R* src, cudaStream_t st) {
+  k_pl2nat_sp<R><<<nb(G.V), 128, 0, st>>>(G, nat, src);
+}
+template <typename Rin, typename R>
+void nat_to_planes_gauge(const Geom& G, R* dst, const Rin* nat, cudaStream_t st) {
+  k_nat2pl_gauge<Rin, R><<<nb(G.V), 128, 0, st>>>(G, dst, nat);
+}
+template <typename Rin, typename R>
+void nat_to_planes_clover(const Geom& G, R* dst, const Rin* nat, cudaStream_t st) {
+  k_nat2pl_clover<Rin, R><<<nb(G.V), 128, 0, st>>>(G, dst, nat);
+}
+
+#define QWSG_INST(R)                                                                             \
+  template void qws_to_planes_spinor<R>(const Geom&, R*, const R*, int, int, int, cudaStream_t); \
+  template void planes_to_qws_spinor<R>(const Geom&, R*, const R*, int, int, int, cudaStream_t); \
+  template void qws_to_planes_gauge<R>(const Geom&, R*, const R*, int, cudaStream_t);            \
+  template void qws_to_planes_clover<R>(const Geom&, R*, const R*, int, cudaStream_t);           \
+  template void nat_to_planes_spinor<R>(const Geom&, R*, const R*, cudaStream_t);                \
+  template void planes_to_nat_spinor<R>(const Geom&, R*, const R*, cudaStream_t);
+QWSG_INST(float)
+QWSG_INST(double)
+#undef QWSG_INST
+template void nat_to_planes_gauge<double, double>(const Geom&, double*, const double*, cudaStream_t);
+template void nat_to_planes_gauge<double, float>(const Geom&, float*, const double*, cudaStream_t);
+template void nat_to_planes_gauge<float, float>(const Geom&, float*, const float*, cudaStream_t);
+template void nat_to_planes_clover<double, double>(const Geom&, double*, const double*,
+                                                   cudaStream_t);
+template void nat_to_planes_clover<double, float>(const Geom&, float*, const double*, cudaStream_t);
+template void nat_to_planes_clover<float, float>(const Geom&, float*, const float*, cudaStream_t);
+
+}  // namespace qwsg

@@ -1,0 +1,146 @@
+// Solver context: geometry, resident fields and work buffers on one GPU.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <complex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+
+namespace qwsg {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define QWSG_CUDA(call)                                                                     \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      throw ::qwsg::Error(3, std::string(#call) + ": " + cudaGetErrorString(e_));           \
+  } while (0)
+
+struct SolveStats {
+  int outer_iters = 0;
+  long inner_iters = 0;
+  double rel_resid_recursive = 0;  // sqrt(|r|^2/|b|^2) at exit
+  double rel_resid_true = -1;      // |b - D x| / |b| (when requested)
+};
+
+struct Ctx {
+  Geom G{};
+  double kappa = 0;
+  cudaStream_t st = nullptr;
+  bool own_stream = false;
+  int device = 0;
+
+  // resident fields (device planes)
+  double* Ud = nullptr;
+  double* Cd = nullptr;
+  float* Us = nullptr;
+  float* Cs = nullptr;
+
+  // reductions
+  RedBuf rb{};
+  double* d_res = nullptr;
+  double* h_res = nullptr;  // pinned
+
+  // work buffers, allocated on first use
+  float* sap_s = nullptr;
+  float* sap_a = nullptr;
+  float* sap_t = nullptr;
+  float* in_q = nullptr;
+  float* in_r = nullptr;
+  float* in_p = nullptr;
+  float* in_t = nullptr;
+  float* in_r0 = nullptr;
+  float* ai_b = nullptr;
+  float* ai_t = nullptr;
+  float* ai_x = nullptr;
+  double* out_q = nullptr;
+  double* out_r = nullptr;
+  double* out_p = nullptr;
+  double* out_t = nullptr;
+  double* out_u = nullptr;
+  double* out_r0 = nullptr;
+  std::vector<void*> owned;
+  void* stage = nullptr;  // host<->device conversion staging
+  size_t stage_bytes = 0;
+
+  // per-kernel CUDA-event timing (kind = kernel_kind(), see solver.cu)
+  struct KRec {
+    int kind;
+    cudaEvent_t a, b;
+    double bytes;
+  };
+  bool timing = false;
+  std::vector<KRec> recs;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_next = 0;
+  cudaEvent_t next_event();
+
+  // counters (calls of each reference-named region)
+  long n_prec_ddd = 0, n_prec_s = 0, n_jinv = 0, n_dslash_d = 0, n_inner_iter = 0;
+
+  Ctx(const int L[4], const int NB[4], int tbc);
+  ~Ctx();
+
+  size_t spinor_elems() const { return (size_t)24 * G.pad; }
+  template <typename R>
+  R* alloc_spinor();
+  void ensure_sap();
+  void ensure_inner();
+  void ensure_outer();
+  void ensure_fields_d();
+  void ensure_fields_s();
+  // synchronous read of n reduction results
+  const double* fetch(int n);
+  void check_launch(const char* what);
+};
+
+// kernel kinds for timing
+enum {
+  K_D_F64 = 0,      // full D, FP64 (outer residual)
+  K_D_F32 = 1,      // full D, FP32
+  K_DIN_F64 = 2,    // block-interior D, FP64
+  K_DIN_F32 = 3,    // block-interior D, FP32
+  K_JINV_F32 = 4,   // Richardson step on D_block
+  K_SAPE_F32 = 5,   // SAP update s_e += in_e - D_blk a_e
+  K_OUT_F64 = 6,    // face hops, FP64
+  K_OUT_F32 = 7,    // face hops, FP32
+  K_NKIND = 8
+};
+const char* kernel_kind_name(int k);
+// drain event records into per-kind totals (launches, ms, algorithmic bytes)
+void kernel_stats(Ctx& c, long* launches, double* ms, double* bytes);
+
+// operators on device planes -----------------------------------------------
+void dslash_full_d(Ctx& c, double* out, const double* in);
+void dslash_full_s(Ctx& c, float* out, const float* in);
+// D_block on one colour (col >= 0) or one domain (dom >= 0)
+template <typename R>
+void dslash_inner(Ctx& c, R* out, const R* in, int col, int dom);
+// out += factor A^-1 H_face in, on one colour or domain
+template <typename R>
+void dslash_outer(Ctx& c, R* out, const R* in, int col, int dom, double factor, int zero_col);
+void jinv_s(Ctx& c, float* x, const float* b, int col, int nm);
+void prec_ddd_s(Ctx& c, float* out, const float* in, int nsap, int nm);
+void prec_s(Ctx& c, float* out, const float* in, int nsap, int nm);
+int bicgstab_precdd_s(Ctx& c, float* x, const float* b, double tol, int maxiter, int nsap, int nm,
+                      double* final_rel);
+void bicgstab_dd_mix(Ctx& c, double* x, const double* b, double tol, int maxiter, double tol_s,
+                     int maxiter_s, int nsap, int nm, SolveStats* stats, double* hist,
+                     int hist_len);
+double true_residual(Ctx& c, const double* x, const double* b);
+
+void set_error(const std::string& m);
+
+}  // namespace qwsg
+
+// the opaque handle of the C ABI (include/qwsg.h)
+struct qwsg_lattice {
+  qwsg::Ctx* c;
+};

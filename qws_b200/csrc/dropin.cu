@@ -1,0 +1,608 @@
+// Drop-in implementation of the reference's C entry points (include/qws_dropin.h).
+//
+// Host arrays keep QWS's layout; every call stages them through the handle's
+// device buffer, converts to planes on the GPU, runs the CUDA path and
+// converts back.  Fields are uploaded lazily (dirty flag).
+#include <omp.h>
+#include <sys/time.h>
+
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "../../include/qws_dropin.h"
+#include "../../include/qwsg.h"
+#include "ctx.h"
+
+// reference-compatible globals (qws.cc:74-127)
+extern "C" {
+pglud_t glud = nullptr;
+pglus_t glus = nullptr;
+pclvd_t clvd = nullptr;
+pclvs_t clvs = nullptr;
+double kappa = 0, kappa2 = 0, mkappa = 0;
+int nx = 0, ny = 0, nz = 0, nt = 0, nxh = 0, nxd = 0, nxs = 0, vold = 0, vols = 0;
+int rank = 0, npe[4] = {1, 1, 1, 1}, domain_e = 0, domain_o = 1;
+double fbc[4][2];
+FILE* para_outputfile = nullptr;
+// supplied by the host program in BQCD (qws_bqcd.cc:56-57); optional here
+int std_xyzt2i_(int*) __attribute__((weak));
+int e_o_(int*) __attribute__((weak));
+}
+
+namespace {
+
+using namespace qwsg;
+
+struct Dropin {
+  qwsg_lattice* lat = nullptr;
+  int vlend = 8, vlens = 16;
+  bool fields_dirty = true;
+  bool always_upload = false;
+  double* pd[3] = {nullptr, nullptr, nullptr};  // FP64 planes: 0,1 work, 2 face snapshot
+  float* ps[3] = {nullptr, nullptr, nullptr};   // FP32 planes
+  double t_solver = 0;
+  long n_calls_dd_mix = 0;
+};
+Dropin g;
+int g_vlend_req = 0, g_vlens_req = 0;
+
+Ctx& ctx() {
+  if (!g.lat) {
+    fprintf(stderr, "qws_b200: called before qws_init_\n");
+    std::exit(1);
+  }
+  return *g.lat->c;
+}
+
+[[noreturn]] void die(const std::string& m) {
+  fprintf(stderr, "qws_b200: %s\n", m.c_str());
+  std::exit(1);
+}
+
+template <typename F>
+void guard(const char* name, F&& f) {
+  try {
+    f();
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    die(std::string(name) + ": " + e.what());
+  }
+}
+
+void* stage(Ctx& c, size_t n) {
+  if (n > c.stage_bytes) {
+    QWSG_CUDA(cudaStreamSynchronize(c.st));
+    if (c.stage) cudaFree(c.stage);
+    c.stage = nullptr;
+    c.stage_bytes = 0;
+    QWSG_CUDA(cudaMalloc(&c.stage, n));
+    c.stage_bytes = n;
+  }
+  return c.stage;
+}
+
+void ensure_planes(Ctx& c) {
+  for (int i = 0; i < 3; i++) {
+    if (!g.pd[i]) g.pd[i] = c.alloc_spinor<double>();
+    if (!g.ps[i]) g.ps[i] = c.alloc_spinor<float>();
+  }
+}
+
+// upload the resident fields from the host globals when dirty
+void sync_fields(Ctx& c) {
+  c.kappa = kappa;
+  if (!g.fields_dirty && !g.always_upload) return;
+  c.ensure_fields_d();
+  c.ensure_fields_s();
+  const size_t V = (size_t)c.G.V;
+  void* d = stage(c, sizeof(double) * 72 * V);
+  QWSG_CUDA(cudaMemcpyAsync(d, glud, sizeof(double) * 72 * V, cudaMemcpyHostToDevice, c.st));
+  qws_to_planes_gauge<double>(c.G, c.Ud, (const double*)d, g.vlend, c.st);
+  QWSG_CUDA(cudaMemcpyAsync(d, clvd, sizeof(double) * 72 * V, cudaMemcpyHostToDevice, c.st));
+  qws_to_planes_clover<double>(c.G, c.Cd, (const double*)d, g.vlend, c.st);
+  QWSG_CUDA(cudaMemcpyAsync(d, glus, sizeof(float) * 72 * V, cudaMemcpyHostToDevice, c.st));
+  qws_to_planes_gauge<float>(c.G, c.Us, (const float*)d, g.vlens, c.st);
+  QWSG_CUDA(cudaMemcpyAsync(d, clvs, sizeof(float) * 72 * V, cudaMemcpyHostToDevice, c.st));
+  qws_to_planes_clover<float>(c.G, c.Cs, (const float*)d, g.vlens, c.st);
+  c.check_launch("field upload");
+  QWSG_CUDA(cudaStreamSynchronize(c.st));
+  g.fields_dirty = false;
+}
+
+// host QWS spinor array (whole lattice when dom < 0, else the half array of
+// domain dom) -> device planes
+template <typename R>
+void up(Ctx& c, R* planes, const void* host, int dom, int vlen) {
+  const size_t Vh = (size_t)c.G.Vh;
+  size_t off = dom < 0 ? 0 : (size_t)dom * Vh * 24;
+  size_t n = dom < 0 ? 2 * Vh * 24 : Vh * 24;
+  R* d = (R*)stage(c, sizeof(R) * 2 * Vh * 24);
+  QWSG_CUDA(cudaMemcpyAsync(d + off, host, sizeof(R) * n, cudaMemcpyHostToDevice, c.st));
+  qws_to_planes_spinor<R>(c.G, planes, d, vlen, dom < 0 ? 0 : dom * c.G.Vh,
+                          dom < 0 ? c.G.V : c.G.Vh, c.st);
+  c.check_launch("spinor upload");
+}
+
+template <typename R>
+void down(Ctx& c, void* host, const R* planes, int dom, int vlen) {
+  const size_t Vh = (size_t)c.G.Vh;
+  size_t off = dom < 0 ? 0 : (size_t)dom * Vh * 24;
+  size_t n = dom < 0 ? 2 * Vh * 24 : Vh * 24;
+  R* d = (R*)stage(c, sizeof(R) * 2 * Vh * 24);
+  planes_to_qws_spinor<R>(c.G, d, planes, vlen, dom < 0 ? 0 : dom * c.G.Vh,
+                          dom < 0 ? c.G.V : c.G.Vh, c.st);
+  c.check_launch("spinor download");
+  QWSG_CUDA(cudaMemcpyAsync(host, d + off, sizeof(R) * n, cudaMemcpyDeviceToHost, c.st));
+  QWSG_CUDA(cudaStreamSynchronize(c.st));
+}
+
+int xyzt2i(int* j) {
+  if (std_xyzt2i_) return std_xyzt2i_(j);
+  int lex = j[0] + nx * (j[1] + ny * (j[2] + nz * j[3]));
+  return lex / 2 + 1;
+}
+int eo_of(int* j) {
+  if (e_o_) return e_o_(j);
+  return (j[0] + j[1] + j[2] + j[3]) % 2;
+}
+
+// QWS host-layout element / lane of site (x,y,z,t) for lane width vlen
+inline size_t qws_elem(int x, int y, int z, int t, int vlen, size_t* lane) {
+  int nxv = nxh / vlen;
+  size_t vol = (size_t)nxv * ny * nz * nt;
+  int dom = x / nxh, xh = x % nxh;
+  *lane = xh % vlen;
+  return dom * vol + xh / vlen + (size_t)nxv * (y + (size_t)ny * (z + (size_t)nz * t));
+}
+
+double wall() {
+  struct timeval tv;
+  gettimeofday(&tv, nullptr);
+  return tv.tv_sec + 1e-6 * tv.tv_usec;
+}
+
+}  // namespace
+
+extern "C" {
+
+int qwsg_set_host_vlen(int vlend, int vlens) {
+  if (vlend <= 0 || vlens <= 0) return 1;
+  g_vlend_req = vlend;
+  g_vlens_req = vlens;
+  return 0;
+}
+
+int qwsg_mark_fields_dirty(void) {
+  g.fields_dirty = true;
+  return 0;
+}
+
+qwsg_lattice* qwsg_dropin_lattice(void) { return g.lat; }
+
+// qws.cc:130-316 for one process holding the whole lattice
+void qws_init_(int* lx, int* ly, int* lz, int* lt, int* npe_f, int* fbc_f, int* pce_f,
+               int* pco_f, int* block_size) {
+  (void)pce_f;
+  (void)pco_f;
+  (void)block_size;  // unused by the reference as well (qws.cc:121-122)
+  const char* e;
+  g.vlend = g_vlend_req ? g_vlend_req : ((e = getenv("QWSG_VLEND")) ? atoi(e) : 8);
+  g.vlens = g_vlens_req ? g_vlens_req : ((e = getenv("QWSG_VLENS")) ? atoi(e) : 16);
+  g.always_upload = (e = getenv("QWSG_ALWAYS_UPLOAD")) && atoi(e) != 0;
+  for (int i = 0; i < 4; i++) {
+    npe[i] = npe_f[i];
+    if (npe[i] != 1)
+      die("qws_init_: the drop-in runs one GPU holding the whole lattice; npe must be 1 1 1 1 "
+          "(use qwsg_create with NB = (2*npe0, npe1, npe2, npe3) for the reference's partition "
+          "of a rank grid)");
+  }
+  nx = *lx;
+  ny = *ly;
+  nz = *lz;
+  nt = *lt;
+  nxh = nx / 2;
+  nxd = nxh / g.vlend;
+  nxs = nxh / g.vlens;
+  if (nxd == 0 || nxh % g.vlend) die("qws_init_: nx/2 must be a positive multiple of VLEND");
+  if (nxs == 0 || nxh % g.vlens) die("qws_init_: nx/2 must be a positive multiple of VLENS");
+  vold = nxd * ny * nz * nt;
+  vols = nxs * ny * nz * nt;
+  rank = 0;
+  domain_e = 0;
+  domain_o = 1;
+  // fbc (qws.cc:298-310) for a single rank: the t phase is applied on both faces
+  for (int mu = 0; mu < 4; mu++) fbc[mu][0] = fbc[mu][1] = 2;
+  if (fbc_f[3] != 1) fbc[3][0] = fbc[3][1] = 2.0 * fbc_f[3];
+  const size_t V = (size_t)nx * ny * nz * nt;
+  void* p;
+  if (posix_memalign(&p, CLS, sizeof(double) * 72 * V)) die("qws_init_: out of host memory");
+  glud = (pglud_t)p;
+  if (posix_memalign(&p, CLS, sizeof(float) * 72 * V)) die("qws_init_: out of host memory");
+  glus = (pglus_t)p;
+  if (posix_memalign(&p, CLS, sizeof(double) * 72 * V)) die("qws_init_: out of host memory");
+  clvd = (pclvd_t)p;
+  if (posix_memalign(&p, CLS, sizeof(float) * 72 * V)) die("qws_init_: out of host memory");
+  clvs = (pclvs_t)p;
+  memset(glud, 0, sizeof(double) * 72 * V);
+  memset(glus, 0, sizeof(float) * 72 * V);
+  memset(clvd, 0, sizeof(double) * 72 * V);
+  memset(clvs, 0, sizeof(float) * 72 * V);
+  int L[4] = {nx, ny, nz, nt}, NB[4] = {2, 1, 1, 1};
+  if (qwsg_create(&g.lat, L, NB, fbc_f[3] == -1 ? -1 : 1) != 0)
+    die(std::string("qws_init_: ") + qwsg_last_error());
+  g.fields_dirty = true;
+  guard("qws_init_", [&] { ensure_planes(ctx()); });
+}
+
+void qws_finalize_(void) {
+  if (g.lat) qwsg_destroy(g.lat);
+  g.lat = nullptr;
+  for (int i = 0; i < 3; i++) g.pd[i] = nullptr, g.ps[i] = nullptr;  // freed with the handle
+  free(glud);
+  free(glus);
+  free(clvd);
+  free(clvs);
+  glud = nullptr;
+  glus = nullptr;
+  clvd = nullptr;
+  clvs = nullptr;
+}
+
+// ---- loaders (qws_bqcd.cc) --------------------------------------------------
+void qws_loadg_dd_(double* u, int* volh_tot, double* in_kappa) {
+  kappa = *in_kappa;
+  mkappa = -kappa;
+  kappa2 = kappa * kappa;
+  double* gd = (double*)glud;
+  float* gs = (float*)glus;
+#pragma omp parallel for collapse(2)
+  for (int t = 0; t < nt; t++)
+    for (int z = 0; z < nz; z++)
+      for (int y = 0; y < ny; y++)
+        for (int x = 0; x < nx; x++) {
+          int j[4] = {x, y, z, t};
+          int i = xyzt2i(j), eo = eo_of(j);
+          size_t ihh = (size_t)(i - 1) * 18 + (size_t)eo * (*volh_tot) * 18;
+          size_t lane_d, lane_s;
+          size_t ed = qws_elem(x, y, z, t, g.vlend, &lane_d);
+          size_t es = qws_elem(x, y, z, t, g.vlens, &lane_s);
+          int dom = x / nxh;
+          size_t vold_ = (size_t)vold, vols_ = (size_t)vols;
+          for (int mu = 0; mu < 4; mu++) {
+            // link element: dom*4*vol + mu*vol + in-domain index
+            size_t gd_e = ed + (size_t)dom * 3 * vold_ + mu * vold_;
+            size_t gs_e = es + (size_t)dom * 3 * vols_ + mu * vols_;
+            for (int c1 = 0; c1 < 3; c1++)
+              for (int c2 = 0; c2 < 3; c2++)
+                for (int ri = 0; ri < 2; ri++) {
+                  double v = u[ri + 2 * c1 + 6 * c2 + ihh + (size_t)mu * (*volh_tot) * 36];
+                  gd[(gd_e * 18 + (c2 * 3 + c1) * 2 + ri) * g.vlend + lane_d] = v;
+                  gs[(gs_e * 18 + (c2 * 3 + c1) * 2 + ri) * g.vlens + lane_s] = (float)v;
+                }
+          }
+        }
+  g.fields_dirty = true;
+}
+
+// BQCD's 36 reals per chiral block -> QWS packing (qws_bqcd.cc:301-377)
+static const int kClvPerm[36] = {0,  1,  20, 21, 32, 33, 2,  3,  4,  5,  6,  7,
+                                 8,  9,  10, 11, 12, 13, 14, 15, 16, 17, 18, 19,
+                                 22, 23, 24, 25, 26, 27, 28, 29, 30, 31, 34, 35};
+
+void qws_loadc_dd_(double* c, int* volh) {
+  double* cd = (double*)clvd;
+  float* cs = (float*)clvs;
+#pragma omp parallel for collapse(2)
+  for (int t = 0; t < nt; t++)
+    for (int z = 0; z < nz; z++)
+      for (int y = 0; y < ny; y++)
+        for (int x = 0; x < nx; x++) {
+          int j[4] = {x, y, z, t};
+          int i = xyzt2i(j), eo = eo_of(j);
+          size_t ihh = (size_t)(i - 1) * 72 + (size_t)eo * (*volh) * 72;
+          size_t lane_d, lane_s;
+          size_t ed = qws_elem(x, y, z, t, g.vlend, &lane_d);
+          size_t es = qws_elem(x, y, z, t, g.vlens, &lane_s);
+          for (int ud = 0; ud < 2; ud++)
+            for (int k = 0; k < 36; k++) {
+              double v = c[kClvPerm[k] + ud * 36 + ihh];
+              cd[(ed * 72 + ud * 36 + k) * g.vlend + lane_d] = v;
+              cs[(es * 72 + ud * 36 + k) * g.vlens + lane_s] = (float)v;
+            }
+        }
+  g.fields_dirty = true;
+}
+
+}  // extern "C"
+
+template <typename R>
+static void loadf(R* out, const double* ine, const double* ino, int vlen) {
+#pragma omp parallel for collapse(2)
+  for (int t = 0; t < nt; t++)
+    for (int z = 0; z < nz; z++)
+      for (int y = 0; y < ny; y++)
+        for (int x = 0; x < nx; x++) {
+          int j[4] = {x, y, z, t};
+          int i = xyzt2i(j), eo = eo_of(j);
+          size_t ihh = (size_t)(i - 1) * 24;
+          size_t lane;
+          size_t e = qws_elem(x, y, z, t, vlen, &lane);
+          const double* src = eo == 0 ? ine : ino;
+          for (int c = 0; c < 3; c++)
+            for (int s = 0; s < 4; s++)
+              for (int ri = 0; ri < 2; ri++)
+                out[(e * 24 + c * 8 + s * 2 + ri) * vlen + lane] = (R)src[ri + 2 * s + 8 * c + ihh];
+        }
+}
+
+template <typename R>
+static void storef(double* oute, double* outo, const R* in, int vlen) {
+#pragma omp parallel for collapse(2)
+  for (int t = 0; t < nt; t++)
+    for (int z = 0; z < nz; z++)
+      for (int y = 0; y < ny; y++)
+        for (int x = 0; x < nx; x++) {
+          int j[4] = {x, y, z, t};
+          int i = xyzt2i(j), eo = eo_of(j);
+          size_t ihh = (size_t)(i - 1) * 24;
+          size_t lane;
+          size_t e = qws_elem(x, y, z, t, vlen, &lane);
+          double* dst = eo == 0 ? oute : outo;
+          for (int c = 0; c < 3; c++)
+            for (int s = 0; s < 4; s++)
+              for (int ri = 0; ri < 2; ri++)
+                dst[ri + 2 * s + 8 * c + ihh] = (double)in[(e * 24 + c * 8 + s * 2 + ri) * vlen + lane];
+        }
+}
+
+extern "C" {
+
+void qws_loadfd_dd_(scd_t* out, double* ine, double* ino) { loadf<double>((double*)out, ine, ino, g.vlend); }
+void qws_storefd_dd_(double* oute, double* outo, scd_t* in) { storef<double>(oute, outo, (const double*)in, g.vlend); }
+void qws_loadfs_dd_(scs_t* out, double* ine, double* ino) { loadf<float>((float*)out, ine, ino, g.vlens); }
+void qws_storefs_dd_(double* oute, double* outo, scs_t* in) { storef<float>(oute, outo, (const float*)in, g.vlens); }
+
+// ---- solvers ----------------------------------------------------------------
+void bicgstab_dd_mix_(scd_t* x, scd_t* b, double* tol, int* conviter, int* maxiter, double* tol_s,
+                      int* maxiter_s, int* nsap, int* nm) {
+  guard("bicgstab_dd_mix_", [&] {
+    Ctx& c = ctx();
+    double t0 = wall();
+    sync_fields(c);
+    up<double>(c, g.pd[1], b, -1, g.vlend);
+    up<double>(c, g.pd[0], x, -1, g.vlend);
+    SolveStats st;
+    bicgstab_dd_mix(c, g.pd[0], g.pd[1], *tol, *maxiter, *tol_s, *maxiter_s, *nsap, *nm, &st,
+                    nullptr, 0);
+    down<double>(c, x, g.pd[0], -1, g.vlend);
+    *conviter = st.outer_iters;
+    g.t_solver += wall() - t0;
+    g.n_calls_dd_mix++;
+  });
+}
+
+void bicgstab_precdd_s_(scs_t* x, scs_t* b, double* tol, int* conviter, int* maxiter, int* nsap,
+                        int* nm) {
+  guard("bicgstab_precdd_s_", [&] {
+    Ctx& c = ctx();
+    sync_fields(c);
+    up<float>(c, g.ps[1], b, -1, g.vlens);
+    int it = bicgstab_precdd_s(c, g.ps[0], g.ps[1], *tol, *maxiter, *nsap, *nm, nullptr);
+    down<float>(c, x, g.ps[0], -1, g.vlens);
+    *conviter = it;
+  });
+}
+
+void prec_ddd_s_(scs_t* out, scs_t* in, int* nsap, int* nm) {
+  guard("prec_ddd_s_", [&] {
+    Ctx& c = ctx();
+    sync_fields(c);
+    up<float>(c, g.ps[1], in, -1, g.vlens);
+    prec_ddd_s(c, g.ps[0], g.ps[1], *nsap, *nm);
+    down<float>(c, out, g.ps[0], -1, g.vlens);
+  });
+}
+
+void prec_s_(scs_t* out, scs_t* in, int* nsap, int* nm) {
+  guard("prec_s_", [&] {
+    Ctx& c = ctx();
+    sync_fields(c);
+    up<float>(c, g.ps[1], in, -1, g.vlens);
+    prec_s(c, g.ps[0], g.ps[1], *nsap, *nm);
+    down<float>(c, out, g.ps[0], -1, g.vlens);
+  });
+}
+
+void jinv_ddd_in_s_(scs_t* x, scs_t* b, int* DEO, int* maxiter) {
+  guard("jinv_ddd_in_s_", [&] {
+    Ctx& c = ctx();
+    sync_fields(c);
+    up<float>(c, g.ps[1], b, *DEO, g.vlens);
+    jinv_s(c, g.ps[0], g.ps[1], *DEO, *maxiter);
+    down<float>(c, x, g.ps[0], *DEO, g.vlens);
+  });
+}
+
+// ---- DD operator ------------------------------------------------------------
+void ddd_d_(scd_t* out, scd_t* in) {
+  guard("ddd_d_", [&] {
+    Ctx& c = ctx();
+    sync_fields(c);
+    up<double>(c, g.pd[1], in, -1, g.vlend);
+    dslash_full_d(c, g.pd[0], g.pd[1]);
+    down<double>(c, out, g.pd[0], -1, g.vlend);
+  });
+}
+
+void ddd_s_(scs_t* out, scs_t* in) {
+  guard("ddd_s_", [&] {
+    Ctx& c = ctx();
+    sync_fields(c);
+    up<float>(c, g.ps[1], in, -1, g.vlens);
+    dslash_full_s(c, g.ps[0], g.ps[1]);
+    down<float>(c, out, g.ps[0], -1, g.vlens);
+  });
+}
+
+// ddd_eo_s_ (qws.cc:634-639): D on the half of the full arrays of one domain
+void ddd_eo_s_(scs_t* out, scs_t* in, int* domain) {
+  guard("ddd_eo_s_", [&] {
+    Ctx& c = ctx();
+    sync_fields(c);
+    const int d = *domain;
+    up<float>(c, g.ps[1], in, -1, g.vlens);
+    dslash_inner<float>(c, g.ps[0], g.ps[1], d, -1);
+    dslash_outer<float>(c, g.ps[0], g.ps[1], d, -1, -c.kappa, -1);
+    // the other half of `out` is left as the caller had it
+    float* half = (float*)out + (size_t)d * c.G.Vh * 24;
+    down<float>(c, half, g.ps[0], d, g.vlens);
+  });
+}
+
+void ddd_in_d_(scd_t* out, scd_t* in, int* DEO) {
+  guard("ddd_in_d_", [&] {
+    Ctx& c = ctx();
+    sync_fields(c);
+    up<double>(c, g.pd[1], in, *DEO, g.vlend);
+    dslash_inner<double>(c, g.pd[0], g.pd[1], *DEO, -1);
+    down<double>(c, out, g.pd[0], *DEO, g.vlend);
+  });
+}
+
+void ddd_in_s_(scs_t* out, scs_t* in, int* DEO) {
+  guard("ddd_in_s_", [&] {
+    Ctx& c = ctx();
+    sync_fields(c);
+    up<float>(c, g.ps[1], in, *DEO, g.vlens);
+    dslash_inner<float>(c, g.ps[0], g.ps[1], *DEO, -1);
+    down<float>(c, out, g.ps[0], *DEO, g.vlens);
+  });
+}
+
+// pre: capture the faces = keep a device copy of the whole field
+void ddd_out_pre_d_(scd_t* in, int* DEO) {
+  (void)DEO;
+  guard("ddd_out_pre_d_", [&] {
+    Ctx& c = ctx();
+    sync_fields(c);
+    up<double>(c, g.pd[2], in, -1, g.vlend);
+  });
+}
+
+void ddd_out_pos_d_(scd_t* out, scd_t* in, int* DEO) {
+  (void)in;
+  guard("ddd_out_pos_d_", [&] {
+    Ctx& c = ctx();
+    up<double>(c, g.pd[0], out, *DEO, g.vlend);
+    dslash_outer<double>(c, g.pd[0], g.pd[2], *DEO, -1, -c.kappa, -1);
+    down<double>(c, out, g.pd[0], *DEO, g.vlend);
+  });
+}
+
+void ddd_out_pre_s_(scs_t* in, int* DEO) {
+  (void)DEO;
+  guard("ddd_out_pre_s_", [&] {
+    Ctx& c = ctx();
+    sync_fields(c);
+    up<float>(c, g.ps[2], in, -1, g.vlens);
+  });
+}
+
+void ddd_out_pos_s_(scs_t* out, scs_t* in, int* DEO, float factor) {
+  (void)in;
+  guard("ddd_out_pos_s_", [&] {
+    Ctx& c = ctx();
+    up<float>(c, g.ps[0], out, *DEO, g.vlens);
+    dslash_outer<float>(c, g.ps[0], g.ps[2], *DEO, -1, factor, -1);
+    down<float>(c, out, g.ps[0], *DEO, g.vlens);
+  });
+}
+
+void ddd_out_pre_s_no_timer_(scs_t* in, int* DEO) { ddd_out_pre_s_(in, DEO); }
+void ddd_out_pos_s_no_timer_(scs_t* out, scs_t* in, int* DEO, float factor) {
+  ddd_out_pos_s_(out, in, DEO, factor);
+}
+
+// ---- converters (reordering.cc) ---------------------------------------------
+void fermi_reorder_s2d_dd_(scd_t* out, const scs_t* in) {
+  guard("fermi_reorder_s2d_dd_", [&] {
+    Ctx& c = ctx();
+    up<float>(c, g.ps[0], in, -1, g.vlens);
+    blas_s2d(c.G, g.pd[0], g.ps[0], 1.0, c.st);
+    down<double>(c, out, g.pd[0], -1, g.vlend);
+  });
+}
+
+void fermi_reorder_d2s_dd_(scs_t* out, const scd_t* in) {
+  guard("fermi_reorder_d2s_dd_", [&] {
+    Ctx& c = ctx();
+    up<double>(c, g.pd[0], in, -1, g.vlend);
+    blas_d2s(c.G, g.ps[0], g.pd[0], 1.0, c.st);
+    down<float>(c, out, g.ps[0], -1, g.vlens);
+  });
+}
+
+void fermi_reorder_s2d_dd_renorm_(scd_t* out, const scs_t* in, const double* dnorm) {
+  guard("fermi_reorder_s2d_dd_renorm_", [&] {
+    Ctx& c = ctx();
+    up<float>(c, g.ps[0], in, -1, g.vlens);
+    blas_s2d(c.G, g.pd[0], g.ps[0], *dnorm, c.st);
+    down<double>(c, out, g.pd[0], -1, g.vlend);
+  });
+}
+
+void fermi_reorder_d2s_dd_renorm_(scs_t* out, const scd_t* in, double* dnorm) {
+  guard("fermi_reorder_d2s_dd_renorm_", [&] {
+    Ctx& c = ctx();
+    up<double>(c, g.pd[0], in, -1, g.vlend);
+    blas_norm2<double>(c.G, g.pd[0], c.d_res, c.rb, c.st);
+    const double n = std::sqrt(c.fetch(1)[0]);
+    *dnorm = n;
+    blas_d2s(c.G, g.ps[0], g.pd[0], 1.0 / n, c.st);
+    down<float>(c, out, g.ps[0], -1, g.vlens);
+  });
+}
+
+// ---- helpers ----------------------------------------------------------------
+void print_scdnorm2(const char* a, scd_t* in, int size) {
+  const double* p = (const double*)in;
+  const size_t n = (size_t)size * 24 * g.vlend;
+  double r = 0;
+#pragma omp parallel for reduction(+ : r)
+  for (size_t i = 0; i < n; i++) r += p[i] * p[i];
+  printf("%30s : %24.14e\n", a, r);
+  fflush(stdout);
+}
+
+void print_scsnorm2(const char* a, scs_t* in, int size) {
+  const float* p = (const float*)in;
+  const size_t n = (size_t)size * 24 * g.vlens;
+  double r = 0;
+#pragma omp parallel for reduction(+ : r)
+  for (size_t i = 0; i < n; i++) r += (double)p[i] * p[i];
+  printf("%30s : %24.14e\n", a, (double)(float)r);
+  fflush(stdout);
+}
+
+void zero_scd_field(scd_t* inout, int size) { memset(inout, 0, sizeof(double) * 24 * g.vlend * (size_t)size); }
+void zero_scs_field(scs_t* inout, int size) { memset(inout, 0, sizeof(float) * 24 * g.vlens * (size_t)size); }
+
+double get_clock(void) { return wall(); }
+
+// region table in the spirit of timing.c:81-185 (call counts of this library)
+void print_timing_(void) {
+  if (!g.lat) return;
+  Ctx& c = *g.lat->c;
+  printf("    rank\tfunc_id                         \t   calls\n");
+  printf("       0\t%-32s\t%8ld\n", "bicgstab_dd_mix_", g.n_calls_dd_mix);
+  printf("       0\t%-32s\t%8ld\n", "bicgstab_precdd_s_iter_", c.n_inner_iter);
+  printf("       0\t%-32s\t%8ld\n", "prec_ddd_s_", c.n_prec_ddd);
+  printf("       0\t%-32s\t%8ld\n", "prec_s_", c.n_prec_s);
+  printf("       0\t%-32s\t%8ld\n", "jinv_ddd_in_s_", c.n_jinv);
+  printf("       0\t%-32s\t%8ld\n", "ddd_d_", c.n_dslash_d);
+  fflush(stdout);
+}
+
+}  // extern "C"

@@ -1,0 +1,135 @@
+// Wilson-clover hopping kernels for the DD solver (FP64 and FP32).
+//
+// One templated kernel covers every operator the reference spreads over
+// ddd_in_*, ddd_out_pre/pos_*, jinv_ddd_in_s_ and the SAP update loops:
+//   SEL  which hops:  inner (stay inside the SAP block; ddd_in, open block
+//        faces, ddd_in_d.cc:91-190), outer (cross a block face; the
+//        reference's halo path ddd_out_*), or all (ddd_d_/ddd_s_).
+//   EPI  what is done with acc = A^-1 * (sum of selected hops):
+//        EPI_D    out = src - kappa*acc                (ddd_in / D)
+//        EPI_ADD  out += coef*acc                      (ddd_out_pos, factor coef)
+//        EPI_JINV out = aux + kappa*acc                (one Richardson step
+//                 x <- b + kappa A^-1 H_blk x, algebraically the reference's
+//                 x + (b - D_blk x), static_solver.cc:77-139)
+//        EPI_SAPE out = out + (aux - (src - kappa*acc)) (s_e += in_e - D_blk a_e,
+//                 qws.cc:815-818 with the ddd_in result kept in registers)
+// Faces are not packed: a face hop reads the neighbouring block's site of
+// the source field directly from HBM (the whole lattice is resident).
+#include "kernels.h"
+#include "lattice.cuh"
+
+namespace qwsg {
+
+template <typename R, int SEL, int MU, int DIR>
+__device__ __forceinline__ void do_hop(const HopArgs<R>& a, const Site& s, int g, R acc[24]) {
+  const bool face = DIR > 0 ? (s.lc[MU] == a.G.B[MU] - 1) : (s.lc[MU] == 0);
+  if (face) {
+    if (!(SEL & HOP_OUTER)) return;
+  } else {
+    if (!(SEL & HOP_INNER)) return;
+  }
+  int gn;
+  if (!face) {
+    gn = g + DIR * a.G.str[MU];
+  } else {
+    int ncol;
+    gn = nbr_across(a.G, s, MU, DIR, &ncol);
+    if (ncol == a.zero_col) return;  // that colour's source is defined as zero
+  }
+  R v[24];
+  if (MU == 3)
+    IO<R>::load_half(a.src, a.G.pad, gn, DIR > 0, v);
+  else
+    IO<R>::load_spinor(a.src, a.G.pad, gn, v);
+  R h[12], r[12], u[18];
+  project<R, MU, DIR>(v, h);
+  IO<R>::load_link(a.U, a.G.pad, MU, DIR > 0 ? g : gn, u);
+  if (DIR > 0)
+    link_mul<R, false>(u, h, r);
+  else
+    link_mul<R, true>(u, h, r);
+  R f = 1;
+  if (MU == 3) {
+    f = 2;
+    if (face && (DIR > 0 ? s.bc[3] == a.G.NB[3] - 1 : s.bc[3] == 0)) f = (R)(2 * a.G.tbc);
+  }
+  reconstruct<R, MU, DIR>(r, acc, f);
+}
+
+template <typename R, int SEL, int EPI>
+__global__ void __launch_bounds__(128) k_hop(const HopArgs<R> a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nsites) return;
+  const int g = a.site0 + i;
+  Site s;
+  decode_site(a.G, g, s);
+  if (a.dom >= 0 && (s.bc[0] & 1) != a.dom) return;
+  if (SEL == HOP_OUTER) {
+    bool face = false;
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) face |= (s.lc[mu] == 0) | (s.lc[mu] == a.G.B[mu] - 1);
+    if (!face) return;
+  }
+  R acc[24];
+#pragma unroll
+  for (int j = 0; j < 24; j++) acc[j] = 0;
+  do_hop<R, SEL, 0, +1>(a, s, g, acc);
+  do_hop<R, SEL, 0, -1>(a, s, g, acc);
+  do_hop<R, SEL, 1, +1>(a, s, g, acc);
+  do_hop<R, SEL, 1, -1>(a, s, g, acc);
+  do_hop<R, SEL, 2, +1>(a, s, g, acc);
+  do_hop<R, SEL, 2, -1>(a, s, g, acc);
+  do_hop<R, SEL, 3, +1>(a, s, g, acc);
+  do_hop<R, SEL, 3, -1>(a, s, g, acc);
+  clover_apply<R>(a.C, a.G.pad, g, acc);
+  R o[24];
+  if (EPI == EPI_D) {
+    IO<R>::load_spinor(a.src, a.G.pad, g, o);
+#pragma unroll
+    for (int j = 0; j < 24; j++) o[j] = o[j] + a.coef * acc[j];
+  } else if (EPI == EPI_ADD) {
+    IO<R>::load_spinor(a.out, a.G.pad, g, o);
+#pragma unroll
+    for (int j = 0; j < 24; j++) o[j] = o[j] + a.coef * acc[j];
+  } else if (EPI == EPI_JINV) {
+    IO<R>::load_spinor(a.aux, a.G.pad, g, o);
+#pragma unroll
+    for (int j = 0; j < 24; j++) o[j] = o[j] + a.coef * acc[j];
+  } else {  // EPI_SAPE: coef = -kappa
+    R in[24], av[24];
+    IO<R>::load_spinor(a.out, a.G.pad, g, o);
+    IO<R>::load_spinor(a.aux, a.G.pad, g, in);
+    IO<R>::load_spinor(a.src, a.G.pad, g, av);
+#pragma unroll
+    for (int j = 0; j < 24; j++) o[j] = o[j] + (in[j] - (av[j] + a.coef * acc[j]));
+  }
+  IO<R>::store_spinor(a.out, a.G.pad, g, o);
+}
+
+template <typename R, int SEL, int EPI>
+static void launch(const HopArgs<R>& a, cudaStream_t st) {
+  if (a.nsites <= 0) return;
+  const int threads = 128;
+  const int blocks = (a.nsites + threads - 1) / threads;
+  k_hop<R, SEL, EPI><<<blocks, threads, 0, st>>>(a);
+}
+
+template <typename R>
+void launch_hop(int sel, int epi, const HopArgs<R>& a, cudaStream_t st) {
+#define QWSG_CASE(S, E)              \
+  if (sel == S && epi == E) {        \
+    launch<R, S, E>(a, st);          \
+    return;                          \
+  }
+  QWSG_CASE(HOP_ALL, EPI_D)
+  QWSG_CASE(HOP_INNER, EPI_D)
+  QWSG_CASE(HOP_OUTER, EPI_ADD)
+  QWSG_CASE(HOP_INNER, EPI_JINV)
+  QWSG_CASE(HOP_INNER, EPI_SAPE)
+#undef QWSG_CASE
+}
+
+template void launch_hop<float>(int, int, const HopArgs<float>&, cudaStream_t);
+template void launch_hop<double>(int, int, const HopArgs<double>&, cudaStream_t);
+
+}  // namespace qwsg

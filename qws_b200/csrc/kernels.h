@@ -1,0 +1,94 @@
+// Kernel launch interface shared by the host-side solver code.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "lattice.cuh"
+
+namespace qwsg {
+
+enum { HOP_INNER = 1, HOP_OUTER = 2, HOP_ALL = 3 };
+enum { EPI_D = 0, EPI_ADD = 1, EPI_JINV = 2, EPI_SAPE = 3 };
+
+template <typename R>
+struct HopArgs {
+  Geom G;
+  const R* src;   // field the hops read
+  const R* aux;   // b (EPI_JINV) or the SAP right-hand side `in` (EPI_SAPE)
+  R* out;
+  const R* U;     // gauge planes
+  const R* C;     // clover planes
+  R coef;
+  int site0;      // first site (DD order) handled
+  int nsites;     // number of consecutive sites handled
+  int dom;        // >= 0: only sites whose block has ibx % 2 == dom
+  int zero_col;   // >= 0: face hops landing on this colour contribute zero
+};
+
+template <typename R>
+void launch_hop(int sel, int epi, const HopArgs<R>& a, cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// BLAS-1 on spinor planes (complex per-site vectors of 12 components).
+// Reductions are written to `res` (device, double) deterministically.
+// ---------------------------------------------------------------------------
+struct RedBuf {
+  double* partial;    // [nblk_max * 8]
+  unsigned* counter;  // one per concurrent reduction slot
+  int nblk;
+};
+
+template <typename R>
+void blas_copy(const Geom& G, R* y, const R* x, int site0, int n, cudaStream_t st);
+template <typename R>
+void blas_zero(const Geom& G, R* y, int site0, int n, cudaStream_t st);
+// res[0] = |x|^2
+template <typename R>
+void blas_norm2(const Geom& G, const R* x, double* res, RedBuf& rb, cudaStream_t st);
+// res[0..1] = <x,y> = sum conj(x) y
+template <typename R>
+void blas_cdot(const Geom& G, const R* x, const R* y, double* res, RedBuf& rb, cudaStream_t st);
+// res[0] = |y|^2, res[1..2] = <y,x>  (omega step: |t|^2, <t,r>)
+template <typename R>
+void blas_norm_cdot(const Geom& G, const R* y, const R* x, double* res, RedBuf& rb,
+                    cudaStream_t st);
+// x += a p ; r -= a q ; res[0] = |r|^2 ; optionally res[1..2] = <r0, r>
+template <typename R>
+void blas_bicg_update(const Geom& G, R* x, R* r, const R* p, const R* q, double ar, double ai,
+                      const R* r0, double* res, RedBuf& rb, cudaStream_t st);
+// p = r + b (p - w q)
+template <typename R>
+void blas_bicg_p(const Geom& G, R* p, const R* r, const R* q, double br, double bi, double wr,
+                 double wi, cudaStream_t st);
+// r = b - q ; p = r ; r0 = r ; res[0] = |b|^2 ; res[1] = |r|^2
+template <typename R>
+void blas_bicg_init(const Geom& G, const R* b, const R* q, R* r, R* p, R* r0, double* res,
+                    RedBuf& rb, cudaStream_t st);
+// y = (float)(x * s)   /   y = (double)x * s
+void blas_d2s(const Geom& G, float* y, const double* x, double s, cudaStream_t st);
+void blas_s2d(const Geom& G, double* y, const float* x, double s, cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// layout conversion: QWS host layout (lane width vlen) <-> device planes.
+// The QWS array covers the whole (single-rank) lattice: two x-half domains.
+// ---------------------------------------------------------------------------
+template <typename R>
+void qws_to_planes_spinor(const Geom& G, R* dst, const R* qws, int vlen, int site0, int n,
+                          cudaStream_t st);
+template <typename R>
+void planes_to_qws_spinor(const Geom& G, R* qws, const R* src, int vlen, int site0, int n,
+                          cudaStream_t st);
+template <typename R>
+void qws_to_planes_gauge(const Geom& G, R* dst, const R* qws, int vlen, cudaStream_t st);
+template <typename R>
+void qws_to_planes_clover(const Geom& G, R* dst, const R* qws, int vlen, cudaStream_t st);
+// natural layout (site = x + Lx*(y + Ly*(z + Lz*t))) <-> device planes
+template <typename R>
+void nat_to_planes_spinor(const Geom& G, R* dst, const R* nat, cudaStream_t st);
+template <typename R>
+void planes_to_nat_spinor(const Geom& G, R* nat, const R* src, cudaStream_t st);
+template <typename Rin, typename R>
+void nat_to_planes_gauge(const Geom& G, R* dst, const Rin* nat, cudaStream_t st);
+template <typename Rin, typename R>
+void nat_to_planes_clover(const Geom& G, R* dst, const Rin* nat, cudaStream_t st);
+
+}  // namespace qwsg

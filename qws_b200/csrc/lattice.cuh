@@ -1,0 +1,369 @@
+// Device-side lattice geometry and field storage for the B200 DD solver.
+//
+// Site order in HBM ("DD order"): the lattice is cut into SAP blocks of
+// B[0]xB[1]xB[2]xB[3] sites on a block grid NB[4] (NB[0] even).  Blocks are
+// coloured (ibx+iby+ibz+ibt) % 2 -- the reference's domain_e/domain_o
+// assignment (qws.cc:224-225, 275-276) when NB = (2*npe0, npe1, npe2, npe3).
+// Sites are stored colour-major, then block-major, then lexicographic inside
+// the block:
+//     g = colour*Vh + (block_linear >> 1)*Vb + local
+// so every SAP half-sweep (one colour) touches one contiguous half of every
+// field, and a block's sites are contiguous.
+//
+// Fields are structure-of-arrays "planes" of 16-byte (FP32 float4 / FP64
+// double2) or 8-byte (FP32 float2 links) vectors with plane stride `pad`
+// (>= V, multiple of 128), so a warp's load of one plane is one contiguous,
+// fully coalesced 512-byte (or 256-byte) transaction:
+//   spinor  : 24 reals/site, per-site order [colour][spin][re,im] (QWS's own,
+//             qws.h:134-139); FP32 6 float4 planes, FP64 12 double2 planes.
+//   gauge   : per direction mu, U_mu(x)[row][col] complex; 9 complex planes
+//             per mu (float2 / double2), plane index mu*9 + 3*row + col.
+//   clover  : the reference's packed 2x36 chiral blocks (clover_def.h:88-284);
+//             FP32 18 float4 planes, FP64 36 double2 planes.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace qwsg {
+
+struct Geom {
+  int L[4];    // global extents
+  int B[4];    // block extents
+  int NB[4];   // block grid
+  int Vb;      // sites per block
+  int V;       // sites
+  int Vh;      // sites per colour
+  int nbh0;    // NB[0] / 2
+  int tbc;     // +1 periodic / -1 antiperiodic in t (fbc_f[3], qws.cc:298-310)
+  int pad;     // plane stride in elements
+  int str[4];  // in-block strides: 1, B0, B0*B1, B0*B1*B2
+};
+
+struct Site {
+  int col;     // block colour
+  int lc[4];   // coordinates inside the block
+  int bc[4];   // block coordinates
+};
+
+__device__ __forceinline__ void decode_site(const Geom& G, int g, Site& s) {
+  s.col = g >= G.Vh;
+  int rem = g - s.col * G.Vh;
+  int k = rem / G.Vb;
+  int t = rem - k * G.Vb;
+  s.lc[0] = t % G.B[0];
+  t /= G.B[0];
+  s.lc[1] = t % G.B[1];
+  t /= G.B[1];
+  s.lc[2] = t % G.B[2];
+  s.lc[3] = t / G.B[2];
+  int q = k / G.nbh0;
+  int r = k - q * G.nbh0;
+  s.bc[1] = q % G.NB[1];
+  q /= G.NB[1];
+  s.bc[2] = q % G.NB[2];
+  s.bc[3] = q / G.NB[2];
+  s.bc[0] = 2 * r + ((s.col + s.bc[1] + s.bc[2] + s.bc[3]) & 1);
+}
+
+// index of the neighbour across the block face in direction mu (dir = +1/-1)
+__device__ __forceinline__ int nbr_across(const Geom& G, const Site& s, int mu, int dir,
+                                          int* ncol) {
+  int bc0 = s.bc[0], bc1 = s.bc[1], bc2 = s.bc[2], bc3 = s.bc[3];
+  int l0 = s.lc[0], l1 = s.lc[1], l2 = s.lc[2], l3 = s.lc[3];
+  int* bcp = mu == 0 ? &bc0 : mu == 1 ? &bc1 : mu == 2 ? &bc2 : &bc3;
+  int* lcp = mu == 0 ? &l0 : mu == 1 ? &l1 : mu == 2 ? &l2 : &l3;
+  if (dir > 0) {
+    *lcp = 0;
+    *bcp = (*bcp + 1 == G.NB[mu]) ? 0 : *bcp + 1;
+  } else {
+    *lcp = G.B[mu] - 1;
+    *bcp = (*bcp == 0) ? G.NB[mu] - 1 : *bcp - 1;
+  }
+  int col = (bc0 + bc1 + bc2 + bc3) & 1;
+  int blin = bc0 + G.NB[0] * (bc1 + G.NB[1] * (bc2 + G.NB[2] * bc3));
+  int local = l0 + G.B[0] * (l1 + G.B[1] * (l2 + G.B[2] * l3));
+  *ncol = col;
+  return col * G.Vh + (blin >> 1) * G.Vb + local;
+}
+
+// ---------------------------------------------------------------------------
+// plane I/O
+// ---------------------------------------------------------------------------
+template <typename R>
+struct IO;
+
+template <>
+struct IO<float> {
+  __device__ __forceinline__ static void load_spinor(const float* __restrict__ p, int pad, int g,
+                                                     float v[24]) {
+    const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+      float4 t = __ldg(q + (size_t)j * pad + g);
+      v[4 * j + 0] = t.x;
+      v[4 * j + 1] = t.y;
+      v[4 * j + 2] = t.z;
+      v[4 * j + 3] = t.w;
+    }
+  }
+  // spins {s0, s0+1} only (t-direction projections need half the spinor)
+  __device__ __forceinline__ static void load_half(const float* __restrict__ p, int pad, int g,
+                                                   int upper, float v[24]) {
+    const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      int j = 2 * c + (upper ? 1 : 0);
+      float4 t = __ldg(q + (size_t)j * pad + g);
+      v[4 * j + 0] = t.x;
+      v[4 * j + 1] = t.y;
+      v[4 * j + 2] = t.z;
+      v[4 * j + 3] = t.w;
+    }
+  }
+  __device__ __forceinline__ static void store_spinor(float* __restrict__ p, int pad, int g,
+                                                      const float v[24]) {
+    float4* q = reinterpret_cast<float4*>(p);
+#pragma unroll
+    for (int j = 0; j < 6; j++)
+      q[(size_t)j * pad + g] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+  }
+  __device__ __forceinline__ static void load_link(const float* __restrict__ U, int pad, int mu,
+                                                   int g, float u[18]) {
+    const float2* q = reinterpret_cast<const float2*>(U);
+#pragma unroll
+    for (int e = 0; e < 9; e++) {
+      float2 t = __ldg(q + (size_t)(mu * 9 + e) * pad + g);
+      u[2 * e] = t.x;
+      u[2 * e + 1] = t.y;
+    }
+  }
+  __device__ __forceinline__ static void load_clover_block(const float* __restrict__ C, int pad,
+                                                           int g, int blk, float a[36]) {
+    const float4* q = reinterpret_cast<const float4*>(C);
+#pragma unroll
+    for (int j = 0; j < 9; j++) {
+      float4 t = __ldg(q + (size_t)(9 * blk + j) * pad + g);
+      a[4 * j + 0] = t.x;
+      a[4 * j + 1] = t.y;
+      a[4 * j + 2] = t.z;
+      a[4 * j + 3] = t.w;
+    }
+  }
+};
+
+template <>
+struct IO<double> {
+  __device__ __forceinline__ static void load_spinor(const double* __restrict__ p, int pad, int g,
+                                                     double v[24]) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+    for (int j = 0; j < 12; j++) {
+      double2 t = __ldg(q + (size_t)j * pad + g);
+      v[2 * j] = t.x;
+      v[2 * j + 1] = t.y;
+    }
+  }
+  __device__ __forceinline__ static void load_half(const double* __restrict__ p, int pad, int g,
+                                                   int upper, double v[24]) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        int j = 4 * c + 2 * (upper ? 1 : 0) + s;
+        double2 t = __ldg(q + (size_t)j * pad + g);
+        v[2 * j] = t.x;
+        v[2 * j + 1] = t.y;
+      }
+  }
+  __device__ __forceinline__ static void store_spinor(double* __restrict__ p, int pad, int g,
+                                                      const double v[24]) {
+    double2* q = reinterpret_cast<double2*>(p);
+#pragma unroll
+    for (int j = 0; j < 12; j++) q[(size_t)j * pad + g] = make_double2(v[2 * j], v[2 * j + 1]);
+  }
+  __device__ __forceinline__ static void load_link(const double* __restrict__ U, int pad, int mu,
+                                                   int g, double u[18]) {
+    const double2* q = reinterpret_cast<const double2*>(U);
+#pragma unroll
+    for (int e = 0; e < 9; e++) {
+      double2 t = __ldg(q + (size_t)(mu * 9 + e) * pad + g);
+      u[2 * e] = t.x;
+      u[2 * e + 1] = t.y;
+    }
+  }
+  __device__ __forceinline__ static void load_clover_block(const double* __restrict__ C, int pad,
+                                                           int g, int blk, double a[36]) {
+    const double2* q = reinterpret_cast<const double2*>(C);
+#pragma unroll
+    for (int j = 0; j < 18; j++) {
+      double2 t = __ldg(q + (size_t)(18 * blk + j) * pad + g);
+      a[2 * j] = t.x;
+      a[2 * j + 1] = t.y;
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Wilson hop pieces.  v[24] = spinor [c][s][ri]; h = 2-spinor per colour.
+// Spin projections and reconstructions follow the reference's Dirac-basis
+// conventions (wilson_d.h: __s_xf/__s_xb/__s_yf/..., ddd_in_d.cc:97-178):
+//   x+  h = (v0 - i v3, v1 - i v2)   recon (h0, h1,  i h1,  i h0)
+//   x-  h = (v0 + i v3, v1 + i v2)   recon (h0, h1, -i h1, -i h0)
+//   y+  h = (v0 - v3,   v1 + v2)     recon (h0, h1,  h1,   -h0)
+//   y-  h = (v0 + v3,   v1 - v2)     recon (h0, h1, -h1,    h0)
+//   z+  h = (v0 - i v2, v1 + i v3)   recon (h0, h1,  i h0, -i h1)
+//   z-  h = (v0 + i v2, v1 - i v3)   recon (h0, h1, -i h0,  i h1)
+//   t+  h = (v2, v3) * 2             recon (0, 0, h0, h1)
+//   t-  h = (v0, v1) * 2             recon (h0, h1, 0, 0)
+// ---------------------------------------------------------------------------
+#define RE(c, s) v[8 * (c) + 2 * (s)]
+#define IM(c, s) v[8 * (c) + 2 * (s) + 1]
+
+template <typename R, int MU, int DIR>
+__device__ __forceinline__ void project(const R v[24], R h[12]) {
+  // h[4*c + 2*k + ri]
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    R* o = h + 4 * c;
+    if (MU == 0 && DIR > 0) {
+      o[0] = RE(c, 0) + IM(c, 3); o[1] = IM(c, 0) - RE(c, 3);
+      o[2] = RE(c, 1) + IM(c, 2); o[3] = IM(c, 1) - RE(c, 2);
+    } else if (MU == 0) {
+      o[0] = RE(c, 0) - IM(c, 3); o[1] = IM(c, 0) + RE(c, 3);
+      o[2] = RE(c, 1) - IM(c, 2); o[3] = IM(c, 1) + RE(c, 2);
+    } else if (MU == 1 && DIR > 0) {
+      o[0] = RE(c, 0) - RE(c, 3); o[1] = IM(c, 0) - IM(c, 3);
+      o[2] = RE(c, 1) + RE(c, 2); o[3] = IM(c, 1) + IM(c, 2);
+    } else if (MU == 1) {
+      o[0] = RE(c, 0) + RE(c, 3); o[1] = IM(c, 0) + IM(c, 3);
+      o[2] = RE(c, 1) - RE(c, 2); o[3] = IM(c, 1) - IM(c, 2);
+    } else if (MU == 2 && DIR > 0) {
+      o[0] = RE(c, 0) + IM(c, 2); o[1] = IM(c, 0) - RE(c, 2);
+      o[2] = RE(c, 1) - IM(c, 3); o[3] = IM(c, 1) + RE(c, 3);
+    } else if (MU == 2) {
+      o[0] = RE(c, 0) - IM(c, 2); o[1] = IM(c, 0) + RE(c, 2);
+      o[2] = RE(c, 1) + IM(c, 3); o[3] = IM(c, 1) - RE(c, 3);
+    } else if (MU == 3 && DIR > 0) {
+      o[0] = RE(c, 2); o[1] = IM(c, 2); o[2] = RE(c, 3); o[3] = IM(c, 3);
+    } else {
+      o[0] = RE(c, 0); o[1] = IM(c, 0); o[2] = RE(c, 1); o[3] = IM(c, 1);
+    }
+  }
+}
+#undef RE
+#undef IM
+
+// r = U h (forward) or U^dagger h (backward); U row-major complex [3][3]
+template <typename R, bool DAG>
+__device__ __forceinline__ void link_mul(const R u[18], const R h[12], R r[12]) {
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      R re = 0, im = 0;
+#pragma unroll
+      for (int b = 0; b < 3; b++) {
+        R ur, ui;
+        if (DAG) {
+          ur = u[2 * (3 * b + a)];
+          ui = -u[2 * (3 * b + a) + 1];
+        } else {
+          ur = u[2 * (3 * a + b)];
+          ui = u[2 * (3 * a + b) + 1];
+        }
+        R hr = h[4 * b + 2 * k], hi = h[4 * b + 2 * k + 1];
+        re += ur * hr - ui * hi;
+        im += ur * hi + ui * hr;
+      }
+      r[4 * a + 2 * k] = re;
+      r[4 * a + 2 * k + 1] = im;
+    }
+}
+
+#define AR(c, s) acc[8 * (c) + 2 * (s)]
+#define AI(c, s) acc[8 * (c) + 2 * (s) + 1]
+template <typename R, int MU, int DIR>
+__device__ __forceinline__ void reconstruct(const R r[12], R acc[24], R f) {
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    R r0 = r[4 * c], i0 = r[4 * c + 1], r1 = r[4 * c + 2], i1 = r[4 * c + 3];
+    if (MU == 3) {
+      if (DIR > 0) {
+        AR(c, 2) += f * r0; AI(c, 2) += f * i0; AR(c, 3) += f * r1; AI(c, 3) += f * i1;
+      } else {
+        AR(c, 0) += f * r0; AI(c, 0) += f * i0; AR(c, 1) += f * r1; AI(c, 1) += f * i1;
+      }
+      continue;
+    }
+    AR(c, 0) += r0; AI(c, 0) += i0; AR(c, 1) += r1; AI(c, 1) += i1;
+    if (MU == 0 && DIR > 0) {
+      AR(c, 2) -= i1; AI(c, 2) += r1; AR(c, 3) -= i0; AI(c, 3) += r0;
+    } else if (MU == 0) {
+      AR(c, 2) += i1; AI(c, 2) -= r1; AR(c, 3) += i0; AI(c, 3) -= r0;
+    } else if (MU == 1 && DIR > 0) {
+      AR(c, 2) += r1; AI(c, 2) += i1; AR(c, 3) -= r0; AI(c, 3) -= i0;
+    } else if (MU == 1) {
+      AR(c, 2) -= r1; AI(c, 2) -= i1; AR(c, 3) += r0; AI(c, 3) += i0;
+    } else if (MU == 2 && DIR > 0) {
+      AR(c, 2) -= i0; AI(c, 2) += r0; AR(c, 3) += i1; AI(c, 3) -= r1;
+    } else {
+      AR(c, 2) += i0; AI(c, 2) -= r0; AR(c, 3) -= i1; AI(c, 3) += r1;
+    }
+  }
+}
+#undef AR
+#undef AI
+
+// v <- A^-1 v with the packed chiral clover (clover_def.h:88-284):
+// x0 = (s0+s2, s1+s3), x1 = (s0-s2, s1-s3) per colour (no 1/2), y_i = A_i x_i,
+// s0 = y0+y1, s2 = y0-y1 (colours 0..2), s1/s3 likewise from entries 3..5.
+template <typename R>
+__device__ __forceinline__ void clover_apply(const R* __restrict__ C, int pad, int g, R v[24]) {
+  R xr[2][6], xi[2][6];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    R s0r = v[8 * c], s0i = v[8 * c + 1], s1r = v[8 * c + 2], s1i = v[8 * c + 3];
+    R s2r = v[8 * c + 4], s2i = v[8 * c + 5], s3r = v[8 * c + 6], s3i = v[8 * c + 7];
+    xr[0][c] = s0r + s2r; xi[0][c] = s0i + s2i;
+    xr[0][3 + c] = s1r + s3r; xi[0][3 + c] = s1i + s3i;
+    xr[1][c] = s0r - s2r; xi[1][c] = s0i - s2i;
+    xr[1][3 + c] = s1r - s3r; xi[1][3 + c] = s1i - s3i;
+  }
+  R yr[2][6], yi[2][6];
+#pragma unroll
+  for (int i = 0; i < 2; i++) {
+    R a[36];
+    IO<R>::load_clover_block(C, pad, g, i, a);
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+      yr[i][j] = a[j] * xr[i][j];
+      yi[i][j] = a[j] * xi[i][j];
+    }
+    int n = 0;
+#pragma unroll
+    for (int j = 0; j < 6; j++)
+#pragma unroll
+      for (int k = j + 1; k < 6; k++, n++) {
+        R mr = a[6 + 2 * n], mi = a[7 + 2 * n];
+        // y_j += M_jk x_k ; y_k += conj(M_jk) x_j
+        yr[i][j] += mr * xr[i][k] - mi * xi[i][k];
+        yi[i][j] += mr * xi[i][k] + mi * xr[i][k];
+        yr[i][k] += mr * xr[i][j] + mi * xi[i][j];
+        yi[i][k] += mr * xi[i][j] - mi * xr[i][j];
+      }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    v[8 * c + 0] = yr[0][c] + yr[1][c];
+    v[8 * c + 1] = yi[0][c] + yi[1][c];
+    v[8 * c + 4] = yr[0][c] - yr[1][c];
+    v[8 * c + 5] = yi[0][c] - yi[1][c];
+    v[8 * c + 2] = yr[0][3 + c] + yr[1][3 + c];
+    v[8 * c + 3] = yi[0][3 + c] + yi[1][3 + c];
+    v[8 * c + 6] = yr[0][3 + c] - yr[1][3 + c];
+    v[8 * c + 7] = yi[0][3 + c] - yi[1][3 + c];
+  }
+}
+
+}  // namespace qwsg

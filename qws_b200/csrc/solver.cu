@@ -1,0 +1,503 @@
+// Host orchestration of the DD solver on the GPU: SAP preconditioner and the
+// two BiCGStab loops.  Follows the reference's algorithms step by step
+// (qws.cc:776-975, static_solver.cc:65-140, bicgstab_precdd_s.cc:85-559,
+// bicgstab_dd_mix.cc:76-388) with its halo/aliasing bookkeeping replaced by
+// fused kernels over the resident lattice.
+#include <cmath>
+#include <cstring>
+
+#include "ctx.h"
+
+namespace qwsg {
+
+namespace {
+
+int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+template <typename R>
+HopArgs<R> hop_args(Ctx& c, const R* U, const R* C) {
+  HopArgs<R> a{};
+  a.G = c.G;
+  a.U = U;
+  a.C = C;
+  a.dom = -1;
+  a.zero_col = -1;
+  return a;
+}
+
+// algorithmic reals moved per handled site (sites of the launch range)
+int hop_reals(int sel, int epi) {
+  if (epi == EPI_JINV) return 24 * 3 + 72 + 72;  // src, b, out, links, clover
+  if (epi == EPI_SAPE) return 24 * 4 + 72 + 72;  // a, in, s (r+w), links, clover
+  if (epi == EPI_ADD) return 24 * 3 + 72 + 72;   // out (r+w), one face neighbour, links, clover
+  return 24 * 2 + 72 + 72;                       // in, out, links, clover
+}
+
+int kind_of(int sel, int epi, int sz) {
+  bool d = sz == 8;
+  if (sel == HOP_ALL) return d ? K_D_F64 : K_D_F32;
+  if (sel == HOP_OUTER) return d ? K_OUT_F64 : K_OUT_F32;
+  if (epi == EPI_JINV) return K_JINV_F32;
+  if (epi == EPI_SAPE) return K_SAPE_F32;
+  return d ? K_DIN_F64 : K_DIN_F32;
+}
+
+// sites of one colour that touch a block face
+long face_sites_per_colour(const Geom& G) {
+  long inner = 1;
+  for (int mu = 0; mu < 4; mu++) inner *= (G.B[mu] > 2 ? G.B[mu] - 2 : 0);
+  long nblk_c = (long)G.NB[0] * G.NB[1] * G.NB[2] * G.NB[3] / 2;
+  return nblk_c * (G.Vb - inner);
+}
+
+template <typename R>
+void run_hop(Ctx& c, int sel, int epi, const HopArgs<R>& a) {
+  if (!c.timing) {
+    launch_hop<R>(sel, epi, a, c.st);
+    return;
+  }
+  cudaEvent_t e0 = c.next_event(), e1 = c.next_event();
+  QWSG_CUDA(cudaEventRecord(e0, c.st));
+  launch_hop<R>(sel, epi, a, c.st);
+  QWSG_CUDA(cudaEventRecord(e1, c.st));
+  long sites = a.nsites;
+  if (sel == HOP_OUTER) sites = face_sites_per_colour(c.G) * (a.nsites == c.G.V ? 2 : 1);
+  if (a.dom >= 0) sites /= 2;
+  c.recs.push_back({kind_of(sel, epi, (int)sizeof(R)), e0, e1,
+                    (double)sites * hop_reals(sel, epi) * sizeof(R)});
+}
+
+}  // namespace
+
+const char* kernel_kind_name(int k) {
+  static const char* n[K_NKIND] = {"dslash_full_f64", "dslash_full_f32", "dslash_block_f64",
+                                   "dslash_block_f32", "jinv_step_f32", "sap_update_f32",
+                                   "dslash_face_f64", "dslash_face_f32"};
+  return (k >= 0 && k < K_NKIND) ? n[k] : "?";
+}
+
+cudaEvent_t Ctx::next_event() {
+  if (ev_next == ev_pool.size()) {
+    cudaEvent_t e;
+    QWSG_CUDA(cudaEventCreate(&e));
+    ev_pool.push_back(e);
+  }
+  return ev_pool[ev_next++];
+}
+
+void kernel_stats(Ctx& c, long* launches, double* ms, double* bytes) {
+  QWSG_CUDA(cudaStreamSynchronize(c.st));
+  for (const auto& r : c.recs) {
+    float t = 0;
+    QWSG_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+    launches[r.kind] += 1;
+    ms[r.kind] += t;
+    bytes[r.kind] += r.bytes;
+  }
+  c.recs.clear();
+  c.ev_next = 0;
+}
+
+Ctx::Ctx(const int L[4], const int NB[4], int tbc) {
+  for (int mu = 0; mu < 4; mu++) {
+    if (L[mu] <= 0 || NB[mu] <= 0 || L[mu] % NB[mu] != 0)
+      throw Error(1, "lattice extent not divisible by the block grid");
+    G.L[mu] = L[mu];
+    G.NB[mu] = NB[mu];
+    G.B[mu] = L[mu] / NB[mu];
+  }
+  if (NB[0] % 2 != 0) throw Error(1, "block grid NB[0] must be even (two x-halves per rank)");
+  for (int mu = 1; mu < 4; mu++)
+    if (NB[mu] != 1 && NB[mu] % 2 != 0)
+      throw Error(1, "block grid NB[1..3] must be 1 or even (red-black block colouring)");
+  long V = (long)L[0] * L[1] * L[2] * L[3];
+  if (V >= (1L << 30)) throw Error(1, "lattice too large for 32-bit site indices");
+  G.V = (int)V;
+  G.Vh = G.V / 2;
+  G.Vb = G.B[0] * G.B[1] * G.B[2] * G.B[3];
+  G.nbh0 = NB[0] / 2;
+  G.tbc = tbc;
+  G.pad = round_up(G.V, 128);
+  G.str[0] = 1;
+  G.str[1] = G.B[0];
+  G.str[2] = G.B[0] * G.B[1];
+  G.str[3] = G.B[0] * G.B[1] * G.B[2];
+  QWSG_CUDA(cudaGetDevice(&device));
+  QWSG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  own_stream = true;
+  rb.nblk = 148 * 8;
+  QWSG_CUDA(cudaMalloc(&rb.partial, sizeof(double) * 8 * rb.nblk));
+  QWSG_CUDA(cudaMalloc(&rb.counter, sizeof(unsigned) * 4));
+  QWSG_CUDA(cudaMemset(rb.counter, 0, sizeof(unsigned) * 4));
+  QWSG_CUDA(cudaMalloc(&d_res, sizeof(double) * 8));
+  QWSG_CUDA(cudaMallocHost(&h_res, sizeof(double) * 8));
+}
+
+Ctx::~Ctx() {
+  if (st) cudaStreamSynchronize(st);
+  for (void* p : owned) cudaFree(p);
+  if (stage) cudaFree(stage);
+  for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+  cudaFree(Ud);
+  cudaFree(Cd);
+  cudaFree(Us);
+  cudaFree(Cs);
+  cudaFree(rb.partial);
+  cudaFree(rb.counter);
+  cudaFree(d_res);
+  cudaFreeHost(h_res);
+  if (own_stream && st) cudaStreamDestroy(st);
+}
+
+template <typename R>
+R* Ctx::alloc_spinor() {
+  R* p = nullptr;
+  QWSG_CUDA(cudaMalloc(&p, sizeof(R) * spinor_elems()));
+  QWSG_CUDA(cudaMemsetAsync(p, 0, sizeof(R) * spinor_elems(), st));
+  owned.push_back(p);
+  return p;
+}
+template float* Ctx::alloc_spinor<float>();
+template double* Ctx::alloc_spinor<double>();
+
+void Ctx::ensure_sap() {
+  if (!sap_s) {
+    sap_s = alloc_spinor<float>();
+    sap_a = alloc_spinor<float>();
+    sap_t = alloc_spinor<float>();
+  }
+}
+void Ctx::ensure_inner() {
+  ensure_sap();
+  if (!in_q) {
+    in_q = alloc_spinor<float>();
+    in_r = alloc_spinor<float>();
+    in_p = alloc_spinor<float>();
+    in_t = alloc_spinor<float>();
+    in_r0 = alloc_spinor<float>();
+  }
+}
+void Ctx::ensure_outer() {
+  ensure_inner();
+  if (!out_q) {
+    out_q = alloc_spinor<double>();
+    out_r = alloc_spinor<double>();
+    out_p = alloc_spinor<double>();
+    out_t = alloc_spinor<double>();
+    out_u = alloc_spinor<double>();
+    out_r0 = alloc_spinor<double>();
+    ai_b = alloc_spinor<float>();
+    ai_t = alloc_spinor<float>();
+    ai_x = alloc_spinor<float>();
+  }
+}
+void Ctx::ensure_fields_d() {
+  if (!Ud) {
+    QWSG_CUDA(cudaMalloc(&Ud, sizeof(double) * 72 * (size_t)G.pad));
+    QWSG_CUDA(cudaMalloc(&Cd, sizeof(double) * 72 * (size_t)G.pad));
+    QWSG_CUDA(cudaMemsetAsync(Ud, 0, sizeof(double) * 72 * (size_t)G.pad, st));
+    QWSG_CUDA(cudaMemsetAsync(Cd, 0, sizeof(double) * 72 * (size_t)G.pad, st));
+  }
+}
+void Ctx::ensure_fields_s() {
+  if (!Us) {
+    QWSG_CUDA(cudaMalloc(&Us, sizeof(float) * 72 * (size_t)G.pad));
+    QWSG_CUDA(cudaMalloc(&Cs, sizeof(float) * 72 * (size_t)G.pad));
+    QWSG_CUDA(cudaMemsetAsync(Us, 0, sizeof(float) * 72 * (size_t)G.pad, st));
+    QWSG_CUDA(cudaMemsetAsync(Cs, 0, sizeof(float) * 72 * (size_t)G.pad, st));
+  }
+}
+
+const double* Ctx::fetch(int n) {
+  QWSG_CUDA(cudaMemcpyAsync(h_res, d_res, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+  QWSG_CUDA(cudaStreamSynchronize(st));
+  return h_res;
+}
+
+void Ctx::check_launch(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) throw Error(3, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------
+// operators
+// ---------------------------------------------------------------------------
+void dslash_full_d(Ctx& c, double* out, const double* in) {
+  auto a = hop_args<double>(c, c.Ud, c.Cd);
+  a.src = in;
+  a.out = out;
+  a.coef = -c.kappa;
+  a.site0 = 0;
+  a.nsites = c.G.V;
+  run_hop<double>(c, HOP_ALL, EPI_D, a);
+  c.n_dslash_d++;
+  c.check_launch("dslash_full_d");
+}
+
+void dslash_full_s(Ctx& c, float* out, const float* in) {
+  auto a = hop_args<float>(c, c.Us, c.Cs);
+  a.src = in;
+  a.out = out;
+  a.coef = -(float)c.kappa;
+  a.site0 = 0;
+  a.nsites = c.G.V;
+  run_hop<float>(c, HOP_ALL, EPI_D, a);
+  c.check_launch("dslash_full_s");
+}
+
+template <typename R>
+static const R* gauge_of(Ctx& c);
+template <>
+const float* gauge_of<float>(Ctx& c) { return c.Us; }
+template <>
+const double* gauge_of<double>(Ctx& c) { return c.Ud; }
+template <typename R>
+static const R* clover_of(Ctx& c);
+template <>
+const float* clover_of<float>(Ctx& c) { return c.Cs; }
+template <>
+const double* clover_of<double>(Ctx& c) { return c.Cd; }
+
+static void site_range(const Ctx& c, int col, int& site0, int& n) {
+  if (col >= 0) {
+    site0 = col * c.G.Vh;
+    n = c.G.Vh;
+  } else {
+    site0 = 0;
+    n = c.G.V;
+  }
+}
+
+template <typename R>
+void dslash_inner(Ctx& c, R* out, const R* in, int col, int dom) {
+  auto a = hop_args<R>(c, gauge_of<R>(c), clover_of<R>(c));
+  a.src = in;
+  a.out = out;
+  a.coef = (R)(-c.kappa);
+  site_range(c, col, a.site0, a.nsites);
+  a.dom = dom;
+  run_hop<R>(c, HOP_INNER, EPI_D, a);
+  c.check_launch("dslash_inner");
+}
+template void dslash_inner<float>(Ctx&, float*, const float*, int, int);
+template void dslash_inner<double>(Ctx&, double*, const double*, int, int);
+
+template <typename R>
+void dslash_outer(Ctx& c, R* out, const R* in, int col, int dom, double factor, int zero_col) {
+  auto a = hop_args<R>(c, gauge_of<R>(c), clover_of<R>(c));
+  a.src = in;
+  a.out = out;
+  a.coef = (R)factor;
+  site_range(c, col, a.site0, a.nsites);
+  a.dom = dom;
+  a.zero_col = zero_col;
+  run_hop<R>(c, HOP_OUTER, EPI_ADD, a);
+  c.check_launch("dslash_outer");
+}
+template void dslash_outer<float>(Ctx&, float*, const float*, int, int, double, int);
+template void dslash_outer<double>(Ctx&, double*, const double*, int, int, double, int);
+
+// jinv_ddd_in_s_: nm Richardson steps x <- b + kappa A^-1 H_blk x from x = b
+// (static_solver.cc:65-140; at least one step, as the reference's first
+// step is unconditional).  Ping-pongs between x and the SAP scratch so the
+// last step lands in x.
+void jinv_s(Ctx& c, float* x, const float* b, int col, int nm) {
+  c.ensure_sap();
+  const int steps = nm < 1 ? 1 : nm;
+  auto a = hop_args<float>(c, c.Us, c.Cs);
+  a.aux = b;
+  a.coef = (float)c.kappa;
+  site_range(c, col, a.site0, a.nsites);
+  const float* src = b;
+  for (int k = 1; k <= steps; k++) {
+    float* dst = ((steps - k) % 2 == 0) ? x : c.sap_t;
+    a.src = src;
+    a.out = dst;
+    run_hop<float>(c, HOP_INNER, EPI_JINV, a);
+    src = dst;
+  }
+  c.n_jinv++;
+  c.check_launch("jinv_s");
+}
+
+// The alternating SAP sweeps of prec_ddd_s_/prec_s_ (qws.cc:802-841).
+// With a_c the block solution of colour c and s the running right-hand side:
+//   a_e = J_e(s_e);  s_e += in_e - D_blk,e a_e;  s_o += kappa A^-1 H_face a
+// for (e,o) = (E,O) then (O,E).  The reference's first sweep reads the odd
+// colour's block solution as zero (qws.cc:806-808); zero_col expresses that.
+static void sap_sweeps(Ctx& c, float* s, float* a, const float* in, int nsap, int nm) {
+  const float k = (float)c.kappa;
+  for (int isap = 0; isap < nsap; isap++) {
+    for (int e = 0; e < 2; e++) {
+      const int o = 1 - e;
+      jinv_s(c, a, s, e, nm);
+      auto h = hop_args<float>(c, c.Us, c.Cs);
+      h.src = a;
+      h.aux = in;
+      h.out = s;
+      h.coef = -k;
+      site_range(c, e, h.site0, h.nsites);
+      run_hop<float>(c, HOP_INNER, EPI_SAPE, h);
+      dslash_outer<float>(c, s, a, o, -1, k, (isap == 0 && e == 0) ? 1 : -1);
+    }
+  }
+}
+
+// prec_ddd_s_ (qws.cc:776-926): out = D M_SAP in.  Both of the reference's
+// final-stage branches compute a_E = J_E(s_E), a_O = J_O(s_O - D_face,O (a_E, 0)),
+// out = D (a_E, a_O); here the last product is one full-lattice D.
+void prec_ddd_s(Ctx& c, float* out, const float* in, int nsap, int nm) {
+  if (nsap > 10 || nm > 10) throw Error(2, "prec_ddd_s_: nsap and nm must be <= 10 (qws.cc:798-799)");
+  c.ensure_sap();
+  float *s = c.sap_s, *a = c.sap_a;
+  blas_copy<float>(c.G, s, in, 0, c.G.V, c.st);
+  sap_sweeps(c, s, a, in, nsap, nm);
+  jinv_s(c, a, s, 0, nm);
+  dslash_outer<float>(c, s, a, 1, -1, (float)c.kappa, 1);
+  jinv_s(c, a, s, 1, nm);
+  dslash_full_s(c, out, a);
+  c.n_prec_ddd++;
+}
+
+// prec_s_ (qws.cc:929-975): out = M_SAP in.
+void prec_s(Ctx& c, float* out, const float* in, int nsap, int nm) {
+  c.ensure_sap();
+  float *s = c.sap_s, *a = c.sap_a;
+  blas_copy<float>(c.G, s, in, 0, c.G.V, c.st);
+  sap_sweeps(c, s, a, in, nsap, nm);
+  jinv_s(c, out, s, 0, nm);
+  dslash_outer<float>(c, s, out, 1, -1, (float)c.kappa, 1);
+  jinv_s(c, out, s, 1, nm);
+  c.n_prec_s++;
+}
+
+// bicgstab_precdd_s_ (bicgstab_precdd_s.cc:85-559).  Returns the number of
+// iterations run (a half iteration that converged counts as one).
+int bicgstab_precdd_s(Ctx& c, float* x, const float* b, double tol, int maxiter, int nsap, int nm,
+                      double* final_rel) {
+  c.ensure_inner();
+  const Geom& G = c.G;
+  float *q = c.in_q, *r = c.in_r, *p = c.in_p, *t = c.in_t, *r0 = c.in_r0;
+  blas_zero<float>(G, x, 0, G.V, c.st);
+  blas_bicg_init<float>(G, b, nullptr, r, p, r0, c.d_res, c.rb, c.st);
+  const double* h = c.fetch(2);
+  const float bnorm = (float)h[0];
+  std::complex<float> rho0(bnorm, 0), rho, beta, omega, alpha, ctmp;
+  float rnorm = bnorm;
+  int done = maxiter;
+  for (int iter = 0; iter < maxiter; iter++) {
+    c.n_inner_iter++;
+    prec_ddd_s(c, q, p, nsap, nm);
+    blas_cdot<float>(G, r0, q, c.d_res, c.rb, c.st);
+    h = c.fetch(2);
+    ctmp = std::complex<float>((float)h[0], (float)h[1]);
+    alpha = rho0 / ctmp;
+    if (std::abs(ctmp) == 0) alpha = 0;
+    blas_bicg_update<float>(G, x, r, p, q, alpha.real(), alpha.imag(), nullptr, c.d_res, c.rb,
+                            c.st);
+    rnorm = (float)c.fetch(1)[0];
+    if (std::sqrt(rnorm / bnorm) < tol) {
+      done = iter + 1;
+      break;
+    }
+    prec_ddd_s(c, t, r, nsap, nm);
+    blas_norm_cdot<float>(G, t, r, c.d_res, c.rb, c.st);
+    h = c.fetch(3);
+    const float redu0 = (float)h[0], redu1 = (float)h[1], redu2 = (float)h[2];
+    omega = std::complex<float>(redu1 / redu0, redu2 / redu0);
+    if (redu0 == 0) omega = 0;
+    blas_bicg_update<float>(G, x, r, r, t, omega.real(), omega.imag(), r0, c.d_res, c.rb, c.st);
+    h = c.fetch(3);
+    rnorm = (float)h[0];
+    rho = std::complex<float>((float)h[1], (float)h[2]);
+    if (std::sqrt(rnorm / bnorm) < tol) {
+      done = iter + 1;
+      break;
+    }
+    beta = alpha * rho / (rho0 * omega);
+    rho0 = rho;
+    if (std::abs(omega) == 0 || std::abs(rho0) == 0) beta = 0;
+    blas_bicg_p<float>(G, p, r, q, beta.real(), beta.imag(), omega.real(), omega.imag(), c.st);
+  }
+  if (final_rel) *final_rel = std::sqrt((double)rnorm / (double)bnorm);
+  c.check_launch("bicgstab_precdd_s");
+  return done;
+}
+
+// approx_inv_dirac_op (bicgstab_dd_mix.cc:76-102) with the renormalising
+// FP64<->FP32 converters (reordering.cc:108-204).
+static int approx_inv(Ctx& c, double* x, const double* b, double tol_s, int maxiter_s, int nsap,
+                      int nm) {
+  blas_norm2<double>(c.G, b, c.d_res, c.rb, c.st);
+  const double bn = std::sqrt(c.fetch(1)[0]);
+  blas_d2s(c.G, c.ai_b, b, 1.0 / bn, c.st);
+  int it = bicgstab_precdd_s(c, c.ai_t, c.ai_b, tol_s, maxiter_s, nsap, nm, nullptr);
+  prec_s(c, c.ai_x, c.ai_t, nsap, nm);
+  blas_s2d(c.G, x, c.ai_x, bn, c.st);
+  return it;
+}
+
+// bicgstab_dd_mix_ (bicgstab_dd_mix.cc:105-388): flexible FP64 BiCGStab,
+// iter = 1 .. maxiter-1, two preconditioned inner solves + two D per iteration.
+void bicgstab_dd_mix(Ctx& c, double* x, const double* b, double tol, int maxiter, double tol_s,
+                     int maxiter_s, int nsap, int nm, SolveStats* stats, double* hist,
+                     int hist_len) {
+  c.ensure_outer();
+  const Geom& G = c.G;
+  double *q = c.out_q, *r = c.out_r, *p = c.out_p, *t = c.out_t, *u = c.out_u, *r0 = c.out_r0;
+  dslash_full_d(c, q, x);
+  blas_bicg_init<double>(G, b, q, r, p, r0, c.d_res, c.rb, c.st);
+  const double* h = c.fetch(2);
+  const double bnorm = h[0];
+  std::complex<double> rho0(h[1], 0), rho, beta, omega, alpha, ctmp;
+  double rnorm = h[1];
+  long inner = 0;
+  int iter, nh = 0;
+  for (iter = 1; iter < maxiter; iter++) {
+    inner += approx_inv(c, u, p, tol_s, maxiter_s, nsap, nm);
+    dslash_full_d(c, q, u);
+    blas_cdot<double>(G, r0, q, c.d_res, c.rb, c.st);
+    h = c.fetch(2);
+    ctmp = std::complex<double>(h[0], h[1]);
+    alpha = rho0 / ctmp;
+    if (std::abs(ctmp) == 0) alpha = 0;
+    blas_bicg_update<double>(G, x, r, u, q, alpha.real(), alpha.imag(), nullptr, c.d_res, c.rb,
+                             c.st);
+    rnorm = c.fetch(1)[0];
+    if (hist && nh < hist_len) hist[nh++] = std::sqrt(rnorm / bnorm);
+    if (std::sqrt(rnorm / bnorm) < tol) break;
+    inner += approx_inv(c, u, r, tol_s, maxiter_s, nsap, nm);
+    dslash_full_d(c, t, u);
+    blas_norm_cdot<double>(G, t, r, c.d_res, c.rb, c.st);
+    h = c.fetch(3);
+    omega = std::complex<double>(h[1] / h[0], h[2] / h[0]);
+    if (h[0] == 0) omega = 0;
+    blas_bicg_update<double>(G, x, r, u, t, omega.real(), omega.imag(), r0, c.d_res, c.rb, c.st);
+    h = c.fetch(3);
+    rnorm = h[0];
+    rho = std::complex<double>(h[1], h[2]);
+    if (hist && nh < hist_len) hist[nh++] = std::sqrt(rnorm / bnorm);
+    if (std::sqrt(rnorm / bnorm) < tol) break;
+    beta = alpha * rho / (rho0 * omega);
+    rho0 = rho;
+    if (std::abs(omega) == 0 || std::abs(rho0) == 0) beta = 0;
+    blas_bicg_p<double>(G, p, r, q, beta.real(), beta.imag(), omega.real(), omega.imag(), c.st);
+  }
+  if (stats) {
+    stats->outer_iters = iter;
+    stats->inner_iters = inner;
+    stats->rel_resid_recursive = std::sqrt(rnorm / bnorm);
+  }
+  c.check_launch("bicgstab_dd_mix");
+}
+
+// |b - D x| / |b| in FP64 (the true residual main.cc:286-311 prints).
+double true_residual(Ctx& c, const double* x, const double* b) {
+  c.ensure_outer();
+  dslash_full_d(c, c.out_t, x);
+  blas_bicg_init<double>(c.G, b, c.out_t, c.out_q, c.out_p, c.out_r0, c.d_res, c.rb, c.st);
+  const double* h = c.fetch(2);
+  return std::sqrt(h[1] / h[0]);
+}
+
+}  // namespace qwsg

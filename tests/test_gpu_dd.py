@@ -1,0 +1,146 @@
+"""GPU parity of the DD Wilson-clover path against the CPU oracle.
+
+Tolerances (relative norm of the difference):
+  FP64 operators            1e-13   (the reference's own ddd_d_ vs oracle: 1.5e-16)
+  FP32 single operators     1e-6    (a few FP32 unit roundoffs, 2^-24 = 6e-8)
+  FP32 SAP preconditioner   5e-6    (~15 Dirac applications in FP32)
+  inner FP32 BiCGStab       iteration count within +-1, solution 1e-4
+  outer FP64 mixed solve    outer count within +-1, solution 1e-10 at tol 1e-12
+"""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from qwsref import Oracle, check_sh_ok, gen_main_fields
+
+pytestmark = pytest.mark.gpu
+
+GOLD = json.loads((Path(__file__).parent / "golden" / "case_norms.json").read_text())
+KAPPA = 0.05
+
+# (local lattice, rank grid) -> global lattice with the reference's block grid
+CASES = {
+    "CASE0": ((32, 6, 4, 3), (1, 1, 1, 1)),
+    "CASE1": ((32, 6, 4, 3), (1, 1, 1, 2)),
+    "CASE7": ((32, 6, 4, 3), (1, 2, 2, 2)),
+    "CASE8": ((32, 6, 4, 3), (4, 4, 1, 1)),
+}
+
+
+def rel(a, b, mask=None):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    if mask is not None:
+        a, b = a[mask], b[mask]
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+def colour_mask(L, NB, colour):
+    B = [l // n for l, n in zip(L, NB)]
+    x, y, z, t = np.meshgrid(*[np.arange(l) for l in L], indexing="ij")
+    col = (x // B[0] + y // B[1] + z // B[2] + t // B[3]) % 2
+    # natural site order: x fastest
+    return (col.transpose(3, 2, 1, 0).reshape(-1) == colour)
+
+
+@pytest.fixture(scope="module", params=list(CASES))
+def case(request):
+    import qws_b200
+    lloc, npe = CASES[request.param]
+    L = tuple(a * b for a, b in zip(lloc, npe))
+    NB = (2 * npe[0], npe[1], npe[2], npe[3])
+    U, C, S = gen_main_fields(lloc, npe, 2)
+    o = Oracle(L, NB, tbc=-1, kappa=KAPPA)
+    o.set_fields(U, C)
+    lat = qws_b200.Lattice(L, NB, tbc=-1, kappa=KAPPA)
+    lat.load_fields(U, C)
+    yield request.param, L, NB, o, lat, S[0], S[1]
+    lat.close()
+
+
+def test_ddd_full(case):
+    name, L, NB, o, lat, b, _ = case
+    xd = lat.to_device(b)
+    assert rel(lat.to_host(lat.ddd(xd)), o.ddd_d(b)) < 1e-13
+    bs = b.astype(np.float32)
+    xs = lat.to_device(bs)
+    assert rel(lat.to_host(lat.ddd(xs)), o.ddd_s(bs)) < 1e-6
+
+
+def test_layout_roundtrip(case):
+    name, L, NB, o, lat, b, _ = case
+    np.testing.assert_array_equal(lat.to_host(lat.to_device(b)), b)
+
+
+@pytest.mark.parametrize("colour", [0, 1])
+def test_block_operators(case, colour):
+    name, L, NB, o, lat, b, _ = case
+    m = colour_mask(L, NB, colour)
+    xd = lat.to_device(b)
+    got = lat.to_host(lat.ddd_in(xd, colour))
+    assert rel(got, o.ddd_in_d(b, 0, colour), m) < 1e-13
+    acc0 = np.random.default_rng(1).standard_normal(b.shape)
+    got = lat.to_host(lat.ddd_out(xd, colour, 0.37, out=lat.to_device(acc0)))
+    ref = o.ddd_out_d(b, 0, colour, 0.37, out=acc0.copy())
+    assert rel(got - acc0, ref - acc0, m) < 1e-13
+    bs = b.astype(np.float32)
+    xs = lat.to_device(bs)
+    got = lat.to_host(lat.ddd_in(xs, colour))
+    assert rel(got, o.ddd_in_s(bs, 0, colour), m) < 1e-6
+    got = lat.to_host(lat.jinv(xs, colour, 2))
+    assert rel(got, o.jinv_s(bs, colour, 2), m) < 1e-6
+
+
+def test_sap_preconditioner(case):
+    name, L, NB, o, lat, b, _ = case
+    bs = b.astype(np.float32)
+    xs = lat.to_device(bs)
+    for nsap, nm in ((4, 2), (1, 1), (2, 3)):
+        assert rel(lat.to_host(lat.prec_ddd(xs, nsap, nm)), o.prec_ddd_s(bs, nsap, nm)) < 5e-6
+        assert rel(lat.to_host(lat.prec(xs, nsap, nm)), o.prec_s(bs, nsap, nm)) < 5e-6
+
+
+def test_inner_solver(case):
+    name, L, NB, o, lat, b, _ = case
+    bs = (b / np.linalg.norm(b)).astype(np.float32)
+    xo, it_o, rel_o = o.bicgstab_precdd_s(bs, 1e-6, 50, 4, 2)
+    xg, it_g, rel_g = lat.bicgstab_precdd(lat.to_device(bs), 1e-6, 50, 4, 2)
+    assert abs(it_g - it_o) <= 1
+    assert rel_g < 1e-6
+    assert rel(lat.to_host(xg), xo) < 1e-4
+
+
+def test_mixed_solver_tolerance(case):
+    name, L, NB, o, lat, b, x0 = case
+    xo, stats, _ = o.bicgstab_dd_mix(b, np.zeros_like(b), 1e-12, 20, 1e-6, 50, 4, 2)
+    xd = lat.empty("f64")
+    bd = lat.to_device(b)
+    st = lat.bicgstab_dd_mix(xd, bd, 1e-12, 20, 1e-6, 50, 4, 2)
+    assert abs(st["outer_iters"] - stats[0]) <= 1
+    assert st["rel_resid_recursive"] < 1e-12
+    assert lat.true_residual(xd, bd) < 1e-11
+    assert rel(lat.to_host(xd), xo) < 1e-10
+
+
+def test_golden_dd_solve(case):
+    """The reference's DD-solve golden (tol<0: 5 outer x 2 x 50 inner
+    iterations from the random initial guess, main.cc:258-313)."""
+    name, L, NB, o, lat, b, x0 = case
+    if name not in GOLD:
+        pytest.skip("no golden")
+    g = GOLD[name]
+    a = g["args"]
+    xd = lat.to_device(x0)
+    bd = lat.to_device(b)
+    st = lat.bicgstab_dd_mix(xd, bd, a["tol"], a["maxiter"], a["tol_s"], a["maxiter_s"],
+                             a["nsap"], a["nm"])
+    assert st["outer_iters"] == a["maxiter"]
+    assert st["inner_iters"] == 10 * a["maxiter_s"]
+    x = lat.to_host(xd)
+    r = b - o.ddd_d(x)
+    vals = [v for k, v in g["norms"] if k in ("bnorm^2", "rnorm^2", "xnorm^2")][-3:]
+    for nm_, val, ref in zip(("bnorm^2", "rnorm^2", "xnorm^2"),
+                             (np.sum(b * b), np.sum(r * r), np.sum(x * x)), vals):
+        assert check_sh_ok(nm_, float(val), ref), (nm_, val, ref)
