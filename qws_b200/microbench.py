@@ -1,0 +1,87 @@
+"""Per-kernel microbenchmark of the DD operator kernels on one GPU.
+
+    python -m qws_b200.microbench --lattice 32,32,32,64 --kernel jinv --iters 20
+
+Builds seeded synthetic fields of the given lattice (SU(3) + 5 APE steps,
+clover-leaf clover), then times `iters` launches of one operator with CUDA
+events on the library's stream and prints one JSON line with the average
+launch time and the algorithmic HBM bandwidth (bytes each launch must move:
+spinors read and written once, links and clover once per site).
+
+Kernels: jinv (one Richardson step on one colour), dslash_s / dslash_d (full
+D in FP32 / FP64), block_s (block-interior D on one colour), face_s (face hops
+of one colour), prec (the whole SAP preconditioner prec_ddd_s_).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+import numpy as np
+
+
+def main():
+    import torch
+
+    import qws_b200
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--lattice", default="32,32,32,64")
+    ap.add_argument("--blocks", default="2,1,1,1")
+    ap.add_argument("--kernel", default="jinv")
+    ap.add_argument("--iters", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--kappa", type=float, default=0.1365)
+    ap.add_argument("--csw", type=float, default=1.7)
+    a = ap.parse_args()
+    L = tuple(int(v) for v in a.lattice.split(","))
+    NB = tuple(int(v) for v in a.blocks.split(","))
+    U, plaq = qws_b200.gen_gauge(L, 11, 5, 0.36)
+    C = qws_b200.gen_clover(U, L, a.csw, a.kappa)
+    b = qws_b200.gen_source(L, 12)
+    st = torch.cuda.Stream()
+    lat = qws_b200.Lattice(L, NB, tbc=-1, kappa=a.kappa, stream=st)
+    lat.load_fields(U, C)
+    del U, C
+    V = lat.V
+    with torch.cuda.stream(st):
+        bs = lat.to_device(b.astype(np.float32))
+        bd = lat.to_device(b)
+        out_s = lat.empty("f32")
+        out_d = lat.empty("f64")
+        k = a.kernel
+        if k == "jinv":
+            fn, nbytes = (lambda: lat.jinv(bs, 0, 1, out=out_s)), (V // 2) * 216 * 4
+        elif k == "dslash_s":
+            fn, nbytes = (lambda: lat.ddd(bs, out=out_s)), V * 192 * 4
+        elif k == "dslash_d":
+            fn, nbytes = (lambda: lat.ddd(bd, out=out_d)), V * 192 * 8
+        elif k == "block_s":
+            fn, nbytes = (lambda: lat.ddd_in(bs, 0, out=out_s)), (V // 2) * 192 * 4
+        elif k == "face_s":
+            fn, nbytes = (lambda: lat.ddd_out(bs, 0, 0.1, out=out_s)), None
+        elif k == "prec":
+            fn, nbytes = (lambda: lat.prec_ddd(bs, 4, 2, out=out_s)), None
+        else:
+            raise SystemExit(f"unknown kernel {k}")
+        for _ in range(a.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(a.iters):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize()
+    us = e0.elapsed_time(e1) * 1e3 / a.iters
+    res = {"kernel": k, "lattice": "x".join(map(str, L)), "blocks": list(NB), "us_per_launch": us,
+           "plaquette": plaq}
+    if nbytes:
+        res["bytes_per_launch"] = nbytes
+        res["GBps"] = nbytes / (us * 1e-6) / 1e9
+    print(json.dumps(res), flush=True)
+    lat.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,79 @@
+"""Properties of the synthetic benchmark fields (host code of the library,
+no GPU needed).  The reference only loads fields built elsewhere, so these
+conventions are checked by their properties rather than against it."""
+import numpy as np
+import pytest
+
+import qws_b200
+from qwsref import Oracle
+
+L = (8, 4, 4, 8)
+
+
+@pytest.fixture(scope="module")
+def gauge():
+    return qws_b200.gen_gauge(L, seed=5, n_smear=5, alpha=0.36)
+
+
+def as_complex(U):
+    u = U.reshape(4, -1, 3, 3, 2)
+    return u[..., 0] + 1j * u[..., 1]
+
+
+def test_su3(gauge):
+    U, plaq = gauge
+    u = as_complex(U)
+    eye = np.einsum("...ij,...kj->...ik", u, u.conj())
+    assert np.abs(eye - np.eye(3)).max() < 1e-12
+    assert np.abs(np.linalg.det(u) - 1).max() < 1e-12
+
+
+def test_plaquette_target(gauge):
+    U, plaq = gauge
+    assert abs(plaq - qws_b200.plaquette(U, L)) < 1e-12
+    assert 0.50 < plaq < 0.60  # 5 APE steps at alpha 0.36 -> ~0.55
+    U0, p0 = qws_b200.gen_gauge(L, seed=5, n_smear=0)
+    assert abs(p0) < 0.05  # Haar-like random links
+
+
+def test_deterministic(gauge):
+    U, _ = gauge
+    U2, _ = qws_b200.gen_gauge(L, seed=5, n_smear=5, alpha=0.36)
+    np.testing.assert_array_equal(U, U2)
+
+
+def test_clover_inverse_and_hermiticity(gauge):
+    U, _ = gauge
+    C, T = qws_b200.gen_clover(U, L, csw=1.7, kappa=0.1365, with_T=True)
+    Tc = T[..., 0] + 1j * T[..., 1]
+    assert np.abs(Tc - np.conj(np.swapaxes(Tc, 1, 2))).max() < 1e-14
+    assert np.linalg.eigvalsh(Tc).min() > 0
+    # QWS's packed-clover kernel (oracle, clover_def.h) applied to T v gives v
+    V = int(np.prod(L))
+    o = Oracle(L, (2, 1, 1, 1), tbc=1, kappa=0.1365)
+    o.set_fields(U.reshape(4, V, 18), C)
+    v = np.random.default_rng(0).standard_normal((V, 24))
+    w = o.clover_d(v)
+    vc, wc = v[:, 0::2] + 1j * v[:, 1::2], w[:, 0::2] + 1j * w[:, 1::2]
+    assert np.abs(np.einsum("sij,sj->si", Tc, wc) - vc).max() < 1e-12
+
+
+def test_free_field_limit():
+    V = int(np.prod(L))
+    U = np.zeros((4, V, 18))
+    for a in range(3):
+        U[:, :, 2 * (3 * a + a)] = 1
+    C = qws_b200.gen_clover(U, L, csw=1.7, kappa=0.1365)
+    assert np.allclose(C[:, :6], 0.5) and np.allclose(C[:, 36:42], 0.5)
+    assert np.abs(C[:, 6:36]).max() == 0 and np.abs(C[:, 42:]).max() == 0
+
+
+def test_sources():
+    V = int(np.prod(L))
+    g = qws_b200.gen_source(L, seed=3, kind="gauss")
+    assert abs(np.mean(g ** 2) - 0.5) < 0.05
+    p = qws_b200.gen_source(L, kind="point", arg=4 * 2 + 3)  # colour 2, spin 3
+    assert p.sum() == 1 and p[0, 8 * 2 + 2 * 3] == 1
+    z = qws_b200.gen_source(L, seed=4, kind="z2")
+    assert np.allclose(np.abs(z), 1 / np.sqrt(2))
+    assert z.shape == (V, 24)
