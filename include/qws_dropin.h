@@ -105,6 +105,65 @@ void qws_loadfd_dd_(scd_t* out, double* ine, double* ino);
 void qws_storefd_dd_(double* oute, double* outo, scd_t* in);
 void qws_loadfs_dd_(scs_t* out, double* ine, double* ino);
 void qws_storefs_dd_(double* oute, double* outo, scs_t* in);
+/* even-odd layout (qws_bqcd.cc:66-123, 184-282, 384-498): site (x,y,z,t) of
+ * parity p sits in x-half slot p at compressed x/2; the spinor loaders move
+ * the even sites of a half array only */
+void qws_loadg_bqcd_(double* u, int* volh_tot, double* in_kappa);
+void qws_loadc_bqcd_(double* c, int* volh);
+void qws_loadfd_bqcd_(scd_t* out, double* in);
+void qws_loadfs_bqcd_(scs_t* out, double* in);
+void qws_storefd_bqcd_(double* out, scd_t* in);
+void qws_storefs_bqcd_(double* out, scs_t* in);
+
+/* ---- even-odd (site parity) operators (qws.cc:390-605, deo_in_d.cc:65,
+ *      deo_in_s.cc:65, deo_out_d.cc:88, deo_out_s.cc:93, deo_dag_in.cc,
+ *      deo_dag_out.cc).  Arguments are one-parity half arrays of the
+ *      even-odd layout: out of parity *pe, in of parity *po = 1 - *pe,
+ *      in0 of parity *pe.  H_eo = hopping from po to pe sites (in: inside
+ *      the rank box, out: across its faces), A^-1 the clover inverse:
+ *        deo_*          out  = H in        dee_deo_*   out = A^-1 H in
+ *        *_dag_*        the adjoint hop    one_minus_* out = in0 + f A^-1 H in
+ *        *_out_pre_*    keeps `in` for the following *_out_pos_*
+ *        *_out_pos_*    out += factor (A^-1) H_out (the kept field)
+ *      mtilde_* act on parity-pce half arrays (qws_init_'s pce_f):
+ *        mtilde = 1 - kappa^2 A_ee^-1 H_eo A_oo^-1 H_oe ----------------------- */
+void deo_in_vm_(int* pe, int* po, scd_t* out, scd_t* in);
+void dee_deo_in_vm_(int* pe, int* po, scd_t* out, scd_t* in);
+void deo_dag_in_vm_(int* pe, int* po, scd_t* out, scd_t* in);
+void dee_deo_dag_in_vm_(int* pe, int* po, scd_t* out, scd_t* in);
+void one_minus_dee_deo_in_vm_(int* pe, int* po, scd_t* out, scd_t* in, scd_t* in0, double factor);
+void one_minus_deo_dag_in_vm_(int* pe, int* po, scd_t* out, scd_t* in, scd_t* in0, double factor);
+void deo_out_pre_vm_(int* pe, int* po, scd_t* out, scd_t* in);
+void deo_dag_out_pre_vm_(int* pe, int* po, scd_t* out, scd_t* in);
+void deo_out_pos_vm_(int* pe, int* po, scd_t* out, scd_t* in, double factor);
+void deo_dag_out_pos_vm_(int* pe, int* po, scd_t* out, scd_t* in, double factor);
+void dee_deo_out_pos_vm_(int* pe, int* po, scd_t* out, scd_t* in, double factor);
+void dee_deo_dag_out_pos_vm_(int* pe, int* po, scd_t* out, scd_t* in, double factor);
+void clvd_vm_(int* pe, scd_t* inout);
+void clvd_vm2_(int* pe, scd_t* out, scd_t* in);
+void deo_vm_(int* pe, int* po, scd_t* out, scd_t* in);
+void dee_deo_vm_(int* pe, int* po, scd_t* out, scd_t* in);
+void one_minus_dee_deo_vm_(int* pe, int* po, scd_t* out, scd_t* in, scd_t* in0);
+void deo_dag_vm_(int* pe, int* po, scd_t* out, scd_t* in);
+void dee_deo_dag_vm_(int* pe, int* po, scd_t* out, scd_t* in);
+void one_minus_deo_dag_vm_(int* pe, int* po, scd_t* out, scd_t* in, scd_t* in0);
+void mtilde_vm_(scd_t* out, scd_t* in);
+void mtilde_dag_vm_(scd_t* out, scd_t* in);
+void mtdagmt_vm_(scd_t* out, scd_t* in);
+/* bicgstab.cc:68 ; x: initial guess in, solution out; conviter = iterations */
+void bicgstab_vm_(scd_t* x, scd_t* b, int* conviter, int* maxiter);
+void deo_in_s_(int* pe, int* po, scs_t* out, scs_t* in);
+void dee_deo_in_s_(int* pe, int* po, scs_t* out, scs_t* in);
+void one_minus_dee_deo_in_s_(int* pe, int* po, scs_t* out, scs_t* in, scs_t* in0, float factor);
+void deo_out_pre_s_(const int* pe, const int* po, const scs_t* out, const scs_t* in);
+/* writes *out although the reference declares it const (qws.cc:578) */
+void deo_out_pos_s_(const int* pe, const int* po, const scs_t* out, const scs_t* in, float factor);
+void dee_deo_out_pos_s_(int* pe, int* po, scs_t* out, scs_t* in, float factor);
+void clv_s_(int* pe, scs_t* inout);
+void deo_s_(int* pe, int* po, scs_t* out, scs_t* in);
+void dee_deo_s_(int* pe, int* po, scs_t* out, scs_t* in);
+void one_minus_dee_deo_s_(int* pe, int* po, scs_t* out, scs_t* in, scs_t* in0);
+void mtilde_s_(scs_t* out, scs_t* in);
 
 /* ---- solvers ------------------------------------------------------------- */
 /* bicgstab_dd_mix.cc:105 ; conviter = outer iterations */
@@ -114,6 +173,19 @@ void bicgstab_dd_mix_(scd_t* x, scd_t* b, double* tol, int* conviter, int* maxit
  * that count only under _DEBUG_ and returns 0 otherwise) */
 void bicgstab_precdd_s_(scs_t* x, scs_t* b, double* tol, int* conviter, int* maxiter, int* nsap,
                         int* nm);
+
+/* ---- half-precision pair (qws_h.h:60-62, bicgstab_precdd_s_h.cc:83,
+ *      bicgstab_dd_mix2_hf.cc:110, qws_bqcd.cc:647).  Here the SAP runs with
+ *      FP16 storage and per-site FP32 scales, arithmetic in FP32. ---------- */
+void qws_h_init_(const glus_t* glus, const clvs_t* clvs);
+void bqcd_qws_h_init_(void);
+void assign_mult_mSAP_s_h_(scs_t* xs, const scs_t* bs, const int* nsap, const int* nm);
+void assign_mult_wd_s_(scs_t* x, const scs_t* b);
+void bicgstab_precdd_s_h_(scs_t* x, const scs_t* b, const double* tol, int* conviter,
+                          const int* maxiter, const int* nsap, const int* nm);
+void bicgstab_dd_mix2_hf_(scd_t* x, const scd_t* b, const double* tol, int* conviter,
+                          const int* maxiter, const double* tol_s, const int* maxiter_s,
+                          const int* nsap, const int* nm);
 
 /* ---- SAP preconditioner (qws.cc:776, 929; static_solver.cc:141) --------- */
 void prec_ddd_s_(scs_t* out, scs_t* in, int* nsap, int* nm);

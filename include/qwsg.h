@@ -94,6 +94,23 @@ int qwsg_bicgstab_dd_mix(qwsg_lattice* lat, double* x, const double* b, double t
 /* |b - D x| / |b| in FP64 */
 int qwsg_true_residual(qwsg_lattice* lat, const double* x, const double* b, double* rel);
 
+/* ---- precision form: FP16 storage with per-site FP32 scales, FP32
+ *      arithmetic, for the SAP preconditioner ----------------------------- */
+/* assign_mult_mSAP_s_h_ (prec_ddd_s_h.h:63): out = M_SAP in with nsap-1 sweeps
+ * + the final stage, fields and spinors stored in FP16 (the reference stores
+ * the spinor with one global scale and computes in FP16, qws_h.cc:175-269) */
+int qwsg_prec_s_h(qwsg_lattice* lat, float* out, const float* in, int nsap, int nm);
+/* bicgstab_precdd_s_h_ (bicgstab_precdd_s_h.cc:83): flexible FP32 BiCGStab
+ * with the FP16 SAP preconditioner; x solves D x = b */
+int qwsg_bicgstab_precdd_s_h(qwsg_lattice* lat, float* x, const float* b, double tol, int maxiter,
+                             int nsap, int nm, int* iters, double* final_rel);
+/* bicgstab_dd_mix2_hf_ (bicgstab_dd_mix2_hf.cc:110): FP64 outer around it.
+ * reliable > 0: restart from the recomputed FP64 true residual (at most that
+ * many times) until |b - D x| / |b| < tol; stats->rel_resid_true is set. */
+int qwsg_bicgstab_dd_mix2_hf(qwsg_lattice* lat, double* x, const double* b, double tol, int maxiter,
+                             double tol_s, int maxiter_s, int nsap, int nm, int reliable,
+                             qwsg_solve_stats* stats);
+
 /* ---- synthetic fields (host, OpenMP; conventions in qws_b200/csrc/fields.cu) */
 /* seeded SU(3) links, n_smear APE-style projected averaging steps with
  * weight alpha; writes the average plaquette (Re tr / 3) to *plaq */
@@ -107,6 +124,33 @@ int qwsg_gen_clover(double* C, const double* U, const int L[4], double csw, doub
 /* sources: kind 0 Gaussian, 1 point at the origin (arg = 4*colour + spin),
  * 2 Z2 noise */
 int qwsg_gen_source(double* S, const int L[4], unsigned long long seed, int kind, int arg);
+
+/* ---- even-odd (site parity) family -------------------------------------
+ * Parity vectors are full device fields whose other-parity sites are zero.
+ * deo: sites of parity pe receive the hops from the other parity.
+ *   which 1 = hops inside the rank box L/(NB0/2, NB1, NB2, NB3) (deo_in_*,
+ *         deo_in_d.cc:65), 2 = hops across its faces (deo_out_pre/pos_*,
+ *         deo_out_d.cc:88,156), 3 = both (deo_vm_, qws.cc:518);
+ *   dag   1 = the adjoint hopping (deo_dag_*, deo_dag_in.cc:64);
+ *   clov  1 = multiply by the parity's A^-1 (dee_*);
+ *   mode  0 out = hops, 1 out += factor*hops, 2 out = in0 + factor*hops
+ *         (one_minus_*). */
+int qwsg_set_parities(qwsg_lattice* lat, int pce, int pco);
+int qwsg_deo_d(qwsg_lattice* lat, double* out, const double* in, int pe, int which, int dag,
+               int clov, int mode, double factor, const double* in0);
+int qwsg_deo_s(qwsg_lattice* lat, float* out, const float* in, int pe, int which, int dag,
+               int clov, int mode, double factor, const float* in0);
+/* clvd_vm2_/clv_s_ (qws.cc:390-441): out = A^-1 in on the parity-pe sites */
+int qwsg_clv_d(qwsg_lattice* lat, double* out, const double* in, int pe);
+int qwsg_clv_s(qwsg_lattice* lat, float* out, const float* in, int pe);
+/* mtilde_vm_ (qws.cc:551): 1 - kappa^2 A_ee^-1 D_eo A_oo^-1 D_oe on parity pce;
+ * mtilde_dag_vm_ (qws.cc:557); mtilde_s_ (qws.cc:598) */
+int qwsg_mtilde_d(qwsg_lattice* lat, double* out, const double* in);
+int qwsg_mtilde_dag_d(qwsg_lattice* lat, double* out, const double* in);
+int qwsg_mtilde_s(qwsg_lattice* lat, float* out, const float* in);
+/* bicgstab_vm_ (bicgstab.cc:68): BiCGStab on mtilde, x = initial guess in,
+ * solution out; iters = the reference's conviter */
+int qwsg_bicgstab_vm(qwsg_lattice* lat, double* x, const double* b, int maxiter, int* iters);
 
 /* per-kernel CUDA-event timing on the handle's stream: enable (clears the
  * records) or disable; stats fills, per kernel kind k < *nkind, the number

@@ -105,10 +105,23 @@ inline void mul_u(const T* u, const cx<T> h[3][2], cx<T> r[3][2], bool dagger) {
 // prec_ddd_s_).  With pair_halves set, a y/z/t hop that leaves the rank
 // (NB[mu] > 1) lands on the same offset in the other x-half of the
 // neighbouring rank.
+//
+// box: extents that define "inside" (default the SAP block; the even-odd
+// operators use the rank's local volume).  dag: the adjoint hopping term
+// H^dagger (deo_dag_*): a forward hop projects with (1 + gamma_mu) and a
+// backward hop with (1 - gamma_mu), the links being used as in H.
+//
+// eo_index: model of the even-odd face packers (deo_out_d.cc:88-153): a y/z/t
+// hop that leaves the rank box reads the other parity's site at the SAME
+// compressed index x/2 of the wrapped row.  That is the geometric neighbour
+// when the wrapped extent is even; with an odd extent the lattice is not
+// bipartite across the wrap and the reference reads the adjacent x site.
 template <typename T>
 void hop_site(const orc_lat* l, const T* in, long s, int which, cx<T> acc[3][4],
-              bool pair_halves = false) {
+              bool pair_halves = false, const int* box = nullptr, bool dag = false,
+              bool eo_index = false) {
   const T* U = gauge<T>(l);
+  const int* B = box ? box : l->B;
   int c[4];
   coords(l, s, c);
   for (int a = 0; a < 3; a++)
@@ -116,7 +129,8 @@ void hop_site(const orc_lat* l, const T* in, long s, int which, cx<T> acc[3][4],
   const cx<T> I(0, 1);
   for (int mu = 0; mu < 4; mu++) {
     for (int dir = 0; dir < 2; dir++) {  // 0 forward, 1 backward
-      bool inner = dir == 0 ? (c[mu] % l->B[mu]) != l->B[mu] - 1 : (c[mu] % l->B[mu]) != 0;
+      bool inner = dir == 0 ? (c[mu] % B[mu]) != B[mu] - 1 : (c[mu] % B[mu]) != 0;
+      const int pd = dag ? 1 - dir : dir;  // projector/reconstruction of this hop
       if (!((inner && (which & 1)) || (!inner && (which & 2)))) continue;
       int cn[4] = {c[0], c[1], c[2], c[3]};
       cn[mu] = dir == 0 ? (c[mu] + 1) % l->L[mu] : (c[mu] - 1 + l->L[mu]) % l->L[mu];
@@ -124,13 +138,17 @@ void hop_site(const orc_lat* l, const T* in, long s, int which, cx<T> acc[3][4],
         int B0 = l->B[0], base = (c[0] / (2 * B0)) * 2 * B0, h = (c[0] / B0) & 1;
         cn[0] = base + (1 - h) * B0 + c[0] % B0;
       }
+      if (eo_index && !inner && mu > 0) {
+        const int po = 1 - ((c[0] + c[1] + c[2] + c[3]) & 1);
+        cn[0] = 2 * (c[0] / 2) + ((po + cn[1] + cn[2] + cn[3]) & 1);
+      }
       long sn = site_of(l, cn);
       const T* v = in + 24 * sn;
       cx<T> h[3][2], r[3][2];
       for (int a = 0; a < 3; a++) {
         cx<T> v0(v[8 * a + 0], v[8 * a + 1]), v1(v[8 * a + 2], v[8 * a + 3]);
         cx<T> v2(v[8 * a + 4], v[8 * a + 5]), v3(v[8 * a + 6], v[8 * a + 7]);
-        switch (mu * 2 + dir) {
+        switch (mu * 2 + pd) {
           case 0: h[a][0] = v0 - I * v3; h[a][1] = v1 - I * v2; break;
           case 1: h[a][0] = v0 + I * v3; h[a][1] = v1 + I * v2; break;
           case 2: h[a][0] = v0 - v3; h[a][1] = v1 + v2; break;
@@ -153,7 +171,7 @@ void hop_site(const orc_lat* l, const T* in, long s, int which, cx<T> acc[3][4],
       }
       for (int a = 0; a < 3; a++) {
         cx<T> r0 = r[a][0], r1 = r[a][1];
-        switch (mu * 2 + dir) {
+        switch (mu * 2 + pd) {
           case 0: acc[a][0] += r0; acc[a][1] += r1; acc[a][2] += I * r1; acc[a][3] += I * r0; break;
           case 1: acc[a][0] += r0; acc[a][1] += r1; acc[a][2] -= I * r1; acc[a][3] -= I * r0; break;
           case 2: acc[a][0] += r0; acc[a][1] += r1; acc[a][2] += r1; acc[a][3] -= r0; break;
@@ -742,6 +760,332 @@ void orc_bicgstab_dd_mix(orc_lat* l, double* x, const double* b, double tol, int
     stats[1] = (double)inner;
     stats[2] = rnorm / bnorm;
   }
+}
+
+}  // extern "C"
+
+namespace {
+
+// assign_mult_mSAP_s_h_ in exact(er) arithmetic: prec_s_ with nsap-1 sweeps
+void prec_s_h_fp32(orc_lat* l, float* out, const float* in, int nsap, int nm) {
+  orc_prec_s(l, out, in, nsap - 1, nm);
+}
+
+}  // namespace
+
+extern "C" {
+
+// bicgstab_precdd_s_h_ (bicgstab_precdd_s_h.cc:83-369): flexible BiCGStab,
+// w = M p, q = D w, x += alpha w, breakdown guards |ctmp| <= 1e-15 and
+// |t|^2 <= 1e-30 (:165, :250).
+int orc_bicgstab_precdd_s_h(orc_lat* l, float* x, const float* b, double tol, int maxiter,
+                            int nsap, int nm, double* final_rel) {
+  const long n = 24 * l->V;
+  std::vector<float> q(n), r(b, b + n), p(b, b + n), t(n), r0(b, b + n), w(n);
+  std::memset(x, 0, sizeof(float) * n);
+  float bnorm = (float)orc_norm2_s(b, n);
+  cx<float> rho0(bnorm, 0), rho, beta, omega, alpha, ctmp;
+  float rnorm = bnorm;
+  int done = maxiter;
+  for (int iter = 0; iter < maxiter; iter++) {
+    prec_s_h_fp32(l, w.data(), p.data(), nsap, nm);
+    orc_ddd_s(l, q.data(), w.data());
+    cx<double> d = cdot(r0.data(), q.data(), n);
+    ctmp = cx<float>((float)d.real(), (float)d.imag());
+    alpha = rho0 / ctmp;
+    if (std::abs(ctmp) <= 1e-15f) alpha = 0;
+    float ar = alpha.real(), ai = alpha.imag();
+    for (long i = 0; i < n; i += 2) {
+      x[i] += ar * w[i] - ai * w[i + 1];
+      x[i + 1] += ar * w[i + 1] + ai * w[i];
+      r[i] += -ar * q[i] + ai * q[i + 1];
+      r[i + 1] += -ar * q[i + 1] - ai * q[i];
+    }
+    rnorm = (float)orc_norm2_s(r.data(), n);
+    if (std::sqrt(rnorm / bnorm) < tol) { done = iter + 1; break; }
+    prec_s_h_fp32(l, w.data(), r.data(), nsap, nm);
+    orc_ddd_s(l, t.data(), w.data());
+    double tt = orc_norm2_s(t.data(), n);
+    cx<double> tr = cdot(t.data(), r.data(), n);
+    float redu0 = (float)tt, redu1 = (float)tr.real(), redu2 = (float)tr.imag();
+    omega = cx<float>(redu1 / redu0, redu2 / redu0);
+    if (redu0 <= 1e-30f) omega = 0;
+    ar = omega.real();
+    ai = omega.imag();
+    for (long i = 0; i < n; i += 2) {
+      x[i] += ar * w[i] - ai * w[i + 1];
+      x[i + 1] += ar * w[i + 1] + ai * w[i];
+      r[i] += -ar * t[i] + ai * t[i + 1];
+      r[i + 1] += -ar * t[i + 1] - ai * t[i];
+    }
+    rnorm = (float)orc_norm2_s(r.data(), n);
+    if (std::sqrt(rnorm / bnorm) < tol) { done = iter + 1; break; }
+    cx<double> rr0 = cdot(r0.data(), r.data(), n);
+    rho = cx<float>((float)rr0.real(), (float)rr0.imag());
+    beta = alpha * rho / (rho0 * omega);
+    rho0 = rho;
+    if (std::abs(omega) == 0 || std::abs(rho0) == 0) beta = 0;
+    ar = omega.real();
+    ai = omega.imag();
+    float br = beta.real(), bi = beta.imag();
+    for (long i = 0; i < n; i += 2) {
+      float cr = p[i] - ar * q[i] + ai * q[i + 1];
+      float ci = p[i + 1] - ar * q[i + 1] - ai * q[i];
+      p[i] = br * cr - bi * ci + r[i];
+      p[i + 1] = br * ci + bi * cr + r[i + 1];
+    }
+  }
+  if (final_rel) *final_rel = std::sqrt((double)rnorm / (double)bnorm);
+  return done;
+}
+
+// bicgstab_dd_mix2_hf_ (bicgstab_dd_mix2_hf.cc:110-373) around it: the
+// approximate inverse has no trailing prec_s_ (approx_inv_dirac_op_hf,
+// :88-107); iter = 0..maxiter-1 and conviter = the iteration of convergence.
+void orc_bicgstab_dd_mix2_hf(orc_lat* l, double* x, const double* b, double tol, int maxiter,
+                             double tol_s, int maxiter_s, int nsap, int nm, double* stats) {
+  const long n = 24 * l->V;
+  std::vector<double> q(n), r(n), p(n), t(n), u(n), r0(n);
+  std::vector<float> bs(n), xs(n);
+  auto approx = [&](double* out, const double* in) {
+    double bn = std::sqrt(orc_norm2_d(in, n)), inv = 1.0 / bn;
+    for (long i = 0; i < n; i++) bs[i] = (float)(in[i] * inv);
+    int it = orc_bicgstab_precdd_s_h(l, xs.data(), bs.data(), tol_s, maxiter_s, nsap, nm, nullptr);
+    for (long i = 0; i < n; i++) out[i] = (double)xs[i] * bn;
+    return it;
+  };
+  orc_ddd_d(l, q.data(), x);
+  for (long i = 0; i < n; i++) r[i] = p[i] = r0[i] = b[i] - q[i];
+  double bnorm = orc_norm2_d(b, n);
+  cx<double> rho0(orc_norm2_d(r.data(), n), 0), rho, beta, omega, alpha, ctmp;
+  double rnorm = rho0.real();
+  long inner = 0;
+  int iter, conv = maxiter;
+  for (iter = 0; iter < maxiter; iter++) {
+    inner += approx(u.data(), p.data());
+    orc_ddd_d(l, q.data(), u.data());
+    ctmp = cdot(r0.data(), q.data(), n);
+    alpha = rho0 / ctmp;
+    if (std::abs(ctmp) == 0) alpha = 0;
+    double ar = alpha.real(), ai = alpha.imag();
+    for (long i = 0; i < n; i += 2) {
+      x[i] += ar * u[i] - ai * u[i + 1];
+      x[i + 1] += ar * u[i + 1] + ai * u[i];
+      r[i] += -ar * q[i] + ai * q[i + 1];
+      r[i + 1] += -ar * q[i + 1] - ai * q[i];
+    }
+    rnorm = orc_norm2_d(r.data(), n);
+    if (std::sqrt(rnorm / bnorm) < tol) { conv = iter; break; }
+    inner += approx(u.data(), r.data());
+    orc_ddd_d(l, t.data(), u.data());
+    double tt = orc_norm2_d(t.data(), n);
+    cx<double> tr = cdot(t.data(), r.data(), n);
+    omega = cx<double>(tr.real() / tt, tr.imag() / tt);
+    if (tt == 0) omega = 0;
+    ar = omega.real();
+    ai = omega.imag();
+    for (long i = 0; i < n; i += 2) {
+      x[i] += ar * u[i] - ai * u[i + 1];
+      x[i + 1] += ar * u[i + 1] + ai * u[i];
+      r[i] += -ar * t[i] + ai * t[i + 1];
+      r[i + 1] += -ar * t[i + 1] - ai * t[i];
+    }
+    rnorm = orc_norm2_d(r.data(), n);
+    if (std::sqrt(rnorm / bnorm) < tol) { conv = iter; break; }
+    rho = cdot(r0.data(), r.data(), n);
+    beta = alpha * rho / (rho0 * omega);
+    rho0 = rho;
+    if (std::abs(omega) == 0 || std::abs(rho0) == 0) beta = 0;
+    ar = omega.real();
+    ai = omega.imag();
+    double br = beta.real(), bi = beta.imag();
+    for (long i = 0; i < n; i += 2) {
+      double cr = p[i] - ar * q[i] + ai * q[i + 1];
+      double ci = p[i + 1] - ar * q[i + 1] - ai * q[i];
+      p[i] = br * cr - bi * ci + r[i];
+      p[i + 1] = br * ci + bi * cr + r[i + 1];
+    }
+  }
+  if (stats) {
+    stats[0] = conv;
+    stats[1] = (double)inner;
+    stats[2] = rnorm / bnorm;
+  }
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Even-odd (site parity) operators, deo_in_d.cc:65-445, deo_out_d.cc:88-286,
+// deo_dag_in.cc, deo_dag_out.cc, deo_in_s.cc, deo_out_s.cc, and their
+// compositions in qws.cc:518-605.  Sites of parity pe = (x+y+z+t)%2 receive
+// hops from the other parity.  "in" hops stay inside the rank's local box
+// (L/npe, npe = (NB0/2, NB1, NB2, NB3)); "out" hops cross its faces (halo).
+// ---------------------------------------------------------------------------
+namespace {
+
+template <typename T>
+void deo_t(const orc_lat* l, T* out, const T* in, int pe, int which, int dag, int clov, int mode,
+           T factor, const T* in0) {
+  const T* C = clover<T>(l);
+  int box[4] = {l->L[0] / (l->NB[0] / 2), l->L[1] / l->NB[1], l->L[2] / l->NB[2],
+                l->L[3] / l->NB[3]};
+#pragma omp parallel for schedule(static)
+  for (long s = 0; s < l->V; s++) {
+    int c[4];
+    coords(l, s, c);
+    if (((c[0] + c[1] + c[2] + c[3]) & 1) != pe) continue;
+    cx<T> acc[3][4];
+    hop_site<T>(l, in, s, which, acc, false, box, dag != 0, true);
+    if (clov) clover_site<T>(C + 72 * s, acc);
+    for (int a = 0; a < 3; a++)
+      for (int sp = 0; sp < 4; sp++) {
+        long o = 24 * s + 8 * a + 2 * sp;
+        T re = acc[a][sp].real(), im = acc[a][sp].imag();
+        if (mode == 0) {  // __store_sc
+          out[o] = re;
+          out[o + 1] = im;
+        } else if (mode == 1) {  // __store_add_sc(out, tmp, factor)
+          out[o] += re * factor;
+          out[o + 1] += im * factor;
+        } else {  // __load_sc(out, in0); __store_add_sc(out, tmp, factor)
+          out[o] = in0[o] + re * factor;
+          out[o + 1] = in0[o + 1] + im * factor;
+        }
+      }
+  }
+}
+
+// parity-pe clover multiplication (clvd_vm_/clv_s_, qws.cc:390-425)
+template <typename T>
+void clv_parity(const orc_lat* l, T* out, const T* in, int pe) {
+  const T* C = clover<T>(l);
+#pragma omp parallel for schedule(static)
+  for (long s = 0; s < l->V; s++) {
+    int c[4];
+    coords(l, s, c);
+    if (((c[0] + c[1] + c[2] + c[3]) & 1) != pe) continue;
+    cx<T> a[3][4];
+    for (int cc = 0; cc < 3; cc++)
+      for (int sp = 0; sp < 4; sp++)
+        a[cc][sp] = cx<T>(in[24 * s + 8 * cc + 2 * sp], in[24 * s + 8 * cc + 2 * sp + 1]);
+    clover_site<T>(C + 72 * s, a);
+    for (int cc = 0; cc < 3; cc++)
+      for (int sp = 0; sp < 4; sp++) {
+        out[24 * s + 8 * cc + 2 * sp] = a[cc][sp].real();
+        out[24 * s + 8 * cc + 2 * sp + 1] = a[cc][sp].imag();
+      }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+void orc_deo_d(orc_lat* l, double* out, const double* in, int pe, int which, int dag, int clov,
+               int mode, double factor, const double* in0) {
+  deo_t<double>(l, out, in, pe, which, dag, clov, mode, factor, in0);
+}
+void orc_deo_s(orc_lat* l, float* out, const float* in, int pe, int which, int dag, int clov,
+               int mode, float factor, const float* in0) {
+  deo_t<float>(l, out, in, pe, which, dag, clov, mode, factor, in0);
+}
+void orc_clv_d(orc_lat* l, double* out, const double* in, int pe) { clv_parity<double>(l, out, in, pe); }
+void orc_clv_s(orc_lat* l, float* out, const float* in, int pe) { clv_parity<float>(l, out, in, pe); }
+
+// mtilde_vm_ (qws.cc:551-556): out_e = in_e - kappa^2 A_ee^-1 H_eo A_oo^-1 H_oe in_e
+// (pce = 0, pco = 1 as main.cc:163-164 passes them)
+void orc_mtilde_d(orc_lat* l, double* out, const double* in) {
+  std::vector<double> tmp(24 * l->V, 0.0);
+  deo_t<double>(l, tmp.data(), in, 1, 3, 0, 1, 0, 0.0, nullptr);
+  deo_t<double>(l, out, tmp.data(), 0, 3, 0, 1, 2, -l->kappa * l->kappa, in);
+}
+// mtilde_dag_vm_ (qws.cc:557-565)
+void orc_mtilde_dag_d(orc_lat* l, double* out, const double* in) {
+  std::vector<double> t0(24 * l->V, 0.0), t1(24 * l->V, 0.0);
+  clv_parity<double>(l, t0.data(), in, 0);
+  deo_t<double>(l, t1.data(), t0.data(), 1, 3, 1, 1, 0, 0.0, nullptr);
+  deo_t<double>(l, out, t1.data(), 0, 3, 1, 0, 2, -l->kappa * l->kappa, in);
+}
+
+// bicgstab_vm_ (bicgstab.cc:68-333): BiCGStab on mtilde_vm_ for the even
+// parity, iter = 1..maxiter-1, stops when sqrt(|r|^2/|b|^2) < 1e-14 after the
+// omega step; returns the iteration count.
+int orc_bicgstab_vm(orc_lat* l, double* x, const double* b, int maxiter) {
+  const long n = 24 * l->V;
+  std::vector<double> q(n, 0.0), r(n, 0.0), p(n, 0.0), t(n, 0.0), r0(n, 0.0);
+  auto even = [&](long s) {
+    int c[4];
+    coords(l, s, c);
+    return ((c[0] + c[1] + c[2] + c[3]) & 1) == 0;
+  };
+  std::vector<char> ev(l->V);
+  for (long s = 0; s < l->V; s++) ev[s] = even(s);
+  auto dot = [&](const double* a, const double* bb) {
+    double re = 0, im = 0;
+    for (long s = 0; s < l->V; s++)
+      if (ev[s])
+        for (int k = 0; k < 24; k += 2) {
+          long i = 24 * s + k;
+          re += a[i] * bb[i] + a[i + 1] * bb[i + 1];
+          im += a[i] * bb[i + 1] - a[i + 1] * bb[i];
+        }
+    return cx<double>(re, im);
+  };
+  orc_mtilde_d(l, q.data(), x);
+  for (long s = 0; s < l->V; s++)
+    if (ev[s])
+      for (int k = 0; k < 24; k++) {
+        long i = 24 * s + k;
+        r[i] = b[i] - q[i];
+        p[i] = r0[i] = r[i];
+      }
+  double bnorm = dot(b, b).real();
+  cx<double> rho0(dot(r.data(), r.data()).real(), 0), rho, beta, omega, alpha, ctmp;
+  int iter;
+  for (iter = 1; iter < maxiter; iter++) {
+    orc_mtilde_d(l, q.data(), p.data());
+    ctmp = dot(r0.data(), q.data());
+    alpha = rho0 / ctmp;
+    for (long s = 0; s < l->V; s++)
+      if (ev[s])
+        for (int k = 0; k < 24; k += 2) {
+          long i = 24 * s + k;
+          cx<double> xv(x[i], x[i + 1]), pv(p[i], p[i + 1]), rv(r[i], r[i + 1]), qv(q[i], q[i + 1]);
+          xv += alpha * pv;
+          rv -= alpha * qv;
+          x[i] = xv.real(); x[i + 1] = xv.imag();
+          r[i] = rv.real(); r[i + 1] = rv.imag();
+        }
+    orc_mtilde_d(l, t.data(), r.data());
+    double tt = dot(t.data(), t.data()).real();
+    cx<double> tr = dot(t.data(), r.data());
+    omega = cx<double>(tr.real() / tt, tr.imag() / tt);
+    for (long s = 0; s < l->V; s++)
+      if (ev[s])
+        for (int k = 0; k < 24; k += 2) {
+          long i = 24 * s + k;
+          cx<double> xv(x[i], x[i + 1]), rv(r[i], r[i + 1]), tv(t[i], t[i + 1]);
+          xv += omega * rv;
+          rv -= omega * tv;
+          x[i] = xv.real(); x[i + 1] = xv.imag();
+          r[i] = rv.real(); r[i + 1] = rv.imag();
+        }
+    double rnorm = dot(r.data(), r.data()).real();
+    if (std::sqrt(rnorm / bnorm) < 1e-14) break;
+    rho = dot(r0.data(), r.data());
+    beta = alpha * rho / (rho0 * omega);
+    rho0 = rho;
+    for (long s = 0; s < l->V; s++)
+      if (ev[s])
+        for (int k = 0; k < 24; k += 2) {
+          long i = 24 * s + k;
+          cx<double> pv(p[i], p[i + 1]), qv(q[i], q[i + 1]), rv(r[i], r[i + 1]);
+          pv = rv + beta * (pv - omega * qv);
+          p[i] = pv.real(); p[i + 1] = pv.imag();
+        }
+  }
+  return iter;
 }
 
 }  // extern "C"

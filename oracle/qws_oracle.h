@@ -82,6 +82,16 @@ void orc_bicgstab_dd_mix(orc_lat*, double* x, const double* b, double tol,
                          int maxiter, double tol_s, int maxiter_s, int nsap,
                          int nm, double* stats, double* hist);
 
+/* ---- half-precision solver pair, restated in FP32 ----------------------- */
+/* assign_mult_mSAP_s_h_ (prec_ddd_s_h.h:63-231) is prec_s_ with nsap-1 sweeps;
+ * the flexible inner solver (bicgstab_precdd_s_h.cc:83-369) with that M and the
+ * FP32 D, and its FP64 outer loop (bicgstab_dd_mix2_hf.cc:110-373,
+ * iter = 0..maxiter-1).  Same return conventions as the plain pair. */
+int orc_bicgstab_precdd_s_h(orc_lat*, float* x, const float* b, double tol, int maxiter,
+                            int nsap, int nm, double* final_rel);
+void orc_bicgstab_dd_mix2_hf(orc_lat*, double* x, const double* b, double tol, int maxiter,
+                             double tol_s, int maxiter_s, int nsap, int nm, double* stats);
+
 /* ---- norms -------------------------------------------------------------- */
 double orc_norm2_d(const double* v, long n);
 double orc_norm2_s(const float* v, long n);

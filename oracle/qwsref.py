@@ -89,6 +89,22 @@ def load_oracle():
     lib.orc_bicgstab_dd_mix.argtypes = [vp, _dp, _dp, ctypes.c_double, ctypes.c_int,
                                         ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_int, _dp, _dp]
+    lib.orc_bicgstab_precdd_s_h.restype = ctypes.c_int
+    lib.orc_bicgstab_precdd_s_h.argtypes = [vp, _fp, _fp, ctypes.c_double, ctypes.c_int,
+                                            ctypes.c_int, ctypes.c_int, _dp]
+    lib.orc_bicgstab_dd_mix2_hf.argtypes = [vp, _dp, _dp, ctypes.c_double, ctypes.c_int,
+                                            ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int, _dp]
+    lib.orc_deo_d.argtypes = [vp, _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                              ctypes.c_int, ctypes.c_double, _dp]
+    lib.orc_deo_s.argtypes = [vp, _fp, _fp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                              ctypes.c_int, ctypes.c_float, _fp]
+    lib.orc_clv_d.argtypes = [vp, _dp, _dp, ctypes.c_int]
+    lib.orc_clv_s.argtypes = [vp, _fp, _fp, ctypes.c_int]
+    lib.orc_mtilde_d.argtypes = [vp, _dp, _dp]
+    lib.orc_mtilde_dag_d.argtypes = [vp, _dp, _dp]
+    lib.orc_bicgstab_vm.restype = ctypes.c_int
+    lib.orc_bicgstab_vm.argtypes = [vp, _dp, _dp, ctypes.c_int]
     lib.orc_norm2_d.restype = ctypes.c_double
     lib.orc_norm2_d.argtypes = [_dp, ctypes.c_long]
     lib.orc_norm2_s.restype = ctypes.c_double
@@ -194,6 +210,56 @@ class Oracle:
                                             maxiter, nsap, nm, ctypes.byref(rel))
         return x, it, rel.value
 
+    def bicgstab_precdd_s_h(self, b, tol, maxiter, nsap, nm):
+        x = self.spinor_s()
+        rel = ctypes.c_double(0)
+        it = self.lib.orc_bicgstab_precdd_s_h(self.h, fptr(x), fptr(np.ascontiguousarray(b)), tol,
+                                              maxiter, nsap, nm, ctypes.byref(rel))
+        return x, it, rel.value
+
+    def bicgstab_dd_mix2_hf(self, b, x0, tol, maxiter, tol_s, maxiter_s, nsap, nm):
+        x = np.array(x0, np.float64, copy=True)
+        stats = np.zeros(3)
+        self.lib.orc_bicgstab_dd_mix2_hf(self.h, dptr(x), dptr(np.ascontiguousarray(b)), tol,
+                                         maxiter, tol_s, maxiter_s, nsap, nm, dptr(stats))
+        return x, stats
+
+    # ---- even-odd operators ------------------------------------------------
+    # deo(x, pe, which, dag, clov, mode, factor, in0): sites of parity pe get
+    # the hops from the other parity; which 1 = inside the rank box (deo_in),
+    # 2 = across its faces (deo_out), 3 = all; mode 0 store, 1 out += factor*,
+    # 2 out = in0 + factor*.
+    def deo(self, x, pe, which=3, dag=0, clov=0, mode=0, factor=0.0, in0=None, out=None):
+        dbl = np.asarray(x).dtype == np.float64
+        out = (self.spinor_d() if dbl else self.spinor_s()) if out is None else out
+        if dbl:
+            p0 = dptr(in0) if in0 is not None else None
+            self.lib.orc_deo_d(self.h, dptr(out), dptr(np.ascontiguousarray(x)), pe, which, dag,
+                               clov, mode, factor, p0)
+        else:
+            p0 = fptr(in0) if in0 is not None else None
+            self.lib.orc_deo_s(self.h, fptr(out), fptr(np.ascontiguousarray(x)), pe, which, dag,
+                               clov, mode, factor, p0)
+        return out
+
+    def clv(self, x, pe, out=None):
+        dbl = np.asarray(x).dtype == np.float64
+        out = np.array(x, copy=True) if out is None else out
+        fn, pp = (self.lib.orc_clv_d, dptr) if dbl else (self.lib.orc_clv_s, fptr)
+        fn(self.h, pp(out), pp(np.ascontiguousarray(x)), pe)
+        return out
+
+    def mtilde(self, x, dag=False):
+        out = self.spinor_d()
+        fn = self.lib.orc_mtilde_dag_d if dag else self.lib.orc_mtilde_d
+        fn(self.h, dptr(out), dptr(np.ascontiguousarray(x)))
+        return out
+
+    def bicgstab_vm(self, b, x0, maxiter):
+        x = np.array(x0, np.float64, copy=True)
+        it = self.lib.orc_bicgstab_vm(self.h, dptr(x), dptr(np.ascontiguousarray(b)), maxiter)
+        return x, it
+
     def bicgstab_dd_mix(self, b, x0, tol, maxiter, tol_s, maxiter_s, nsap, nm):
         x = np.array(x0, np.float64, copy=True)
         stats = np.zeros(3)
@@ -250,6 +316,58 @@ def nat_to_qws_clover(C, L, vlen):
     a = np.asarray(C).reshape(Lt, Lz, Ly, 2, nxh // vlen, vlen, 72)
     a = a.transpose(3, 0, 1, 2, 4, 6, 5)
     return np.ascontiguousarray(a).reshape(-1)
+
+
+# BQCD host layout (qws_bqcd.cc:66-642): site index i-1 = lex//2 inside its
+# parity eo = (x+y+z+t)%2 (the default std_xyzt2i_/e_o_ of this library)
+def _bqcd_slots(L):
+    lex = np.arange(int(np.prod(L)))
+    Lx, Ly, Lz, Lt = L
+    x, y = lex % Lx, (lex // Lx) % Ly
+    z, t = (lex // (Lx * Ly)) % Lz, lex // (Lx * Ly * Lz)
+    return lex // 2, (x + y + z + t) % 2
+
+
+# BQCD's 36 reals of one chiral block -> QWS packing index (qws_bqcd.cc:301-377)
+BQCD_CLV_PERM = np.array([0, 1, 20, 21, 32, 33, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15,
+                          16, 17, 18, 19, 22, 23, 24, 25, 26, 27, 28, 29, 30, 31, 34, 35])
+
+
+def nat_to_bqcd_gauge(U, L):
+    """natural [4,V,(row,col,ri)] -> u[ri + 2 row + 6 col + 18 i + 18 volh eo + 36 volh mu]."""
+    V = int(np.prod(L))
+    i, eo = _bqcd_slots(L)
+    out = np.zeros((4, 2, V // 2, 3, 3, 2))  # mu, eo, i, col, row, ri
+    out[:, eo, i] = np.asarray(U).reshape(4, V, 3, 3, 2).transpose(0, 1, 3, 2, 4)
+    return out.reshape(-1)
+
+
+def nat_to_bqcd_clover(C, L):
+    """natural [V,72] (QWS packing) -> c[perm[k] + 36 ud + 72 i + 72 volh eo]."""
+    V = int(np.prod(L))
+    i, eo = _bqcd_slots(L)
+    out = np.zeros((2, V // 2, 2, 36))
+    Cn = np.asarray(C).reshape(V, 2, 36)
+    blk = np.zeros_like(Cn)
+    blk[:, :, BQCD_CLV_PERM] = Cn
+    out[eo, i] = blk
+    return out.reshape(-1)
+
+
+def nat_to_bqcd_spinor(v, L):
+    """natural [V,24] -> (even, odd) arrays in[2 s + 8 c + ri + 24 i]."""
+    V = int(np.prod(L))
+    i, eo = _bqcd_slots(L)
+    out = np.zeros((2, V // 2, 24))
+    out[eo, i] = np.asarray(v).reshape(V, 24)
+    return out[0].reshape(-1), out[1].reshape(-1)
+
+
+def bqcd_to_nat_spinor(e, o, L):
+    V = int(np.prod(L))
+    i, eo = _bqcd_slots(L)
+    both = np.stack([np.asarray(e).reshape(V // 2, 24), np.asarray(o).reshape(V // 2, 24)])
+    return both[eo, i]
 
 
 def aligned_empty(n, dtype, align=256):
@@ -370,3 +488,41 @@ def check_sh_ok(name, val, ref):
     if name.endswith("_s_") or name.endswith("_s"):
         return d / val < 3e-6
     return d / val < 1e-14
+
+
+# --------------------------------------------------------------------------
+# even-odd reading of QWS's arrays
+# --------------------------------------------------------------------------
+def eo_perm(L):
+    """QWS stores even-odd fields in the same array shapes as DD fields
+    (deo_in_d.cc:65-86: parity p at the slot of x-half p, compressed index
+    x_eo = x // 2 at the slot of x_half).  main.cc fills its arrays with the DD
+    generator and then reads them with both operator families, so the field
+    an even-odd operator sees at site (x, y, z, t) is the DD field at
+    (p*nx/2 + x//2, y, z, t) with p = (x+y+z+t) % 2.  Returns that map as an
+    index array over natural site numbers."""
+    Lx, Ly, Lz, Lt = L
+    t, z, y, x = np.meshgrid(np.arange(Lt), np.arange(Lz), np.arange(Ly), np.arange(Lx),
+                             indexing="ij")
+    p = (x + y + z + t) % 2
+    xd = p * (Lx // 2) + x // 2
+    return (xd + Lx * (y + Ly * (z + Lz * t))).reshape(-1)
+
+
+def eo_partner(L):
+    """site of the other parity with the same compressed index: where a
+    half-array argument of one parity aliases the other parity's half
+    (e.g. in0 = in in main.cc:593-611)."""
+    Lx, Ly, Lz, Lt = L
+    t, z, y, x = np.meshgrid(np.arange(Lt), np.arange(Lz), np.arange(Ly), np.arange(Lx),
+                             indexing="ij")
+    p = (x + y + z + t) % 2
+    xo = 2 * (x // 2) + (1 - p + y + z + t) % 2
+    return (xo + Lx * (y + Ly * (z + Lz * t))).reshape(-1)
+
+
+def parity_mask(L, p):
+    Lx, Ly, Lz, Lt = L
+    t, z, y, x = np.meshgrid(np.arange(Lt), np.arange(Lz), np.arange(Ly), np.arange(Lx),
+                             indexing="ij")
+    return ((x + y + z + t) % 2 == p).reshape(-1)

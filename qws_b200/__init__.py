@@ -78,6 +78,20 @@ def load_library(path: str | os.PathLike | None = None):
         "qwsg_bicgstab_dd_mix": [vp, vp, vp, c_double, c_int, c_double, c_int, c_int, c_int,
                                  ctypes.POINTER(SolveStats)],
         "qwsg_true_residual": [vp, vp, vp, ctypes.POINTER(c_double)],
+        "qwsg_set_parities": [vp, c_int, c_int],
+        "qwsg_deo_d": [vp, vp, vp, c_int, c_int, c_int, c_int, c_int, c_double, vp],
+        "qwsg_deo_s": [vp, vp, vp, c_int, c_int, c_int, c_int, c_int, c_double, vp],
+        "qwsg_clv_d": [vp, vp, vp, c_int],
+        "qwsg_clv_s": [vp, vp, vp, c_int],
+        "qwsg_mtilde_d": [vp, vp, vp],
+        "qwsg_mtilde_dag_d": [vp, vp, vp],
+        "qwsg_mtilde_s": [vp, vp, vp],
+        "qwsg_bicgstab_vm": [vp, vp, vp, c_int, ip],
+        "qwsg_prec_s_h": [vp, vp, vp, c_int, c_int],
+        "qwsg_bicgstab_precdd_s_h": [vp, vp, vp, c_double, c_int, c_int, c_int, ip,
+                                     ctypes.POINTER(c_double)],
+        "qwsg_bicgstab_dd_mix2_hf": [vp, vp, vp, c_double, c_int, c_double, c_int, c_int, c_int,
+                                     c_int, ctypes.POINTER(SolveStats)],
         "qwsg_counters": [vp] + [ctypes.POINTER(ctypes.c_long)] * 5,
         "qwsg_kernel_timing": [vp, c_int],
         "qwsg_kernel_stats": [vp, ip, vp, vp, vp],
@@ -300,6 +314,62 @@ class Lattice:
         _check(self.lib.qwsg_bicgstab_dd_mix(self.h, _ptr(x), _ptr(b), float(tol), int(maxiter),
                                              float(tol_s), int(maxiter_s), int(nsap), int(nm),
                                              ctypes.byref(st)))
+        return st.as_dict()
+
+    # ---- even-odd (site parity) family ---------------------------------------
+    def deo(self, x, pe, which=3, dag=0, clov=0, mode=0, factor=0.0, in0=None, out=None):
+        """Sites of parity pe receive the hops from the other parity (see
+        qwsg_deo_d in include/qwsg.h for which/dag/clov/mode)."""
+        out = self._out(x, out)
+        fn = self.lib.qwsg_deo_d if x.dtype == self.torch.float64 else self.lib.qwsg_deo_s
+        _check(fn(self.h, _ptr(out), _ptr(x), int(pe), int(which), int(dag), int(clov), int(mode),
+                  float(factor), _ptr(in0) if in0 is not None else None))
+        return out
+
+    def clv(self, x, pe, out=None):
+        out = self._out(x, out)
+        fn = self.lib.qwsg_clv_d if x.dtype == self.torch.float64 else self.lib.qwsg_clv_s
+        _check(fn(self.h, _ptr(out), _ptr(x), int(pe)))
+        return out
+
+    def mtilde(self, x, dag=False, out=None):
+        out = self._out(x, out)
+        if x.dtype == self.torch.float64:
+            fn = self.lib.qwsg_mtilde_dag_d if dag else self.lib.qwsg_mtilde_d
+        else:
+            if dag:
+                raise QwsgError("mtilde_dag is FP64 only (as in the reference)")
+            fn = self.lib.qwsg_mtilde_s
+        _check(fn(self.h, _ptr(out), _ptr(x)))
+        return out
+
+    def bicgstab_vm(self, x, b, maxiter=100):
+        it = ctypes.c_int()
+        _check(self.lib.qwsg_bicgstab_vm(self.h, _ptr(x), _ptr(b), int(maxiter), ctypes.byref(it)))
+        return it.value
+
+    # ---- precision form (FP16-storage SAP) ----------------------------------
+    def prec_h(self, x, nsap=4, nm=2, out=None):
+        """M_SAP in FP16 storage (nsap-1 sweeps + final stage); FP32 in/out."""
+        out = self._out(x, out)
+        _check(self.lib.qwsg_prec_s_h(self.h, _ptr(out), _ptr(x), int(nsap), int(nm)))
+        return out
+
+    def bicgstab_precdd_h(self, b, tol, maxiter, nsap=4, nm=2, out=None):
+        out = self._out(b, out)
+        it, rel = ctypes.c_int(), ctypes.c_double()
+        _check(self.lib.qwsg_bicgstab_precdd_s_h(self.h, _ptr(out), _ptr(b), float(tol),
+                                                 int(maxiter), int(nsap), int(nm),
+                                                 ctypes.byref(it), ctypes.byref(rel)))
+        return out, it.value, rel.value
+
+    def bicgstab_dd_mix2_hf(self, x, b, tol, maxiter, tol_s, maxiter_s, nsap=4, nm=2,
+                            reliable=0):
+        """FP64 outer / FP16-SAP flexible inner solve of D x = b in place."""
+        st = SolveStats()
+        _check(self.lib.qwsg_bicgstab_dd_mix2_hf(self.h, _ptr(x), _ptr(b), float(tol), int(maxiter),
+                                                 float(tol_s), int(maxiter_s), int(nsap), int(nm),
+                                                 int(reliable), ctypes.byref(st)))
         return st.as_dict()
 
     def true_residual(self, x, b):

@@ -298,6 +298,102 @@ int qwsg_bicgstab_dd_mix(qwsg_lattice* l, double* x, const double* b, double tol
     }
   });
 }
+int qwsg_prec_s_h(qwsg_lattice* l, float* out, const float* in, int nsap, int nm) {
+  return guarded([&] {
+    check_ctx(l);
+    need_fields(*l->c, false);
+    prec_s_h(*l->c, out, in, nsap, nm);
+  });
+}
+int qwsg_bicgstab_precdd_s_h(qwsg_lattice* l, float* x, const float* b, double tol, int maxiter,
+                             int nsap, int nm, int* iters, double* final_rel) {
+  return guarded([&] {
+    check_ctx(l);
+    need_fields(*l->c, false);
+    int it = bicgstab_precdd_s_h(*l->c, x, b, tol, maxiter, nsap, nm, final_rel);
+    if (iters) *iters = it;
+  });
+}
+int qwsg_bicgstab_dd_mix2_hf(qwsg_lattice* l, double* x, const double* b, double tol, int maxiter,
+                             double tol_s, int maxiter_s, int nsap, int nm, int reliable,
+                             qwsg_solve_stats* st) {
+  return guarded([&] {
+    check_ctx(l);
+    need_fields(*l->c, true);
+    need_fields(*l->c, false);
+    SolveStats s;
+    bicgstab_dd_mix2_hf(*l->c, x, b, tol, maxiter, tol_s, maxiter_s, nsap, nm, reliable, &s);
+    if (st) {
+      st->outer_iters = s.outer_iters;
+      st->inner_iters = s.inner_iters;
+      st->rel_resid_recursive = s.rel_resid_recursive;
+      st->rel_resid_true = s.rel_resid_true;
+    }
+  });
+}
+int qwsg_set_parities(qwsg_lattice* l, int pce, int pco) {
+  return guarded([&] {
+    check_ctx(l);
+    if (pce < 0 || pce > 1 || pco != 1 - pce) throw Error(1, "parities must be (0,1) or (1,0)");
+    l->c->pce = pce;
+    l->c->pco = pco;
+  });
+}
+int qwsg_deo_d(qwsg_lattice* l, double* out, const double* in, int pe, int which, int dag,
+               int clov, int mode, double factor, const double* in0) {
+  return guarded([&] {
+    check_ctx(l);
+    deo<double>(*l->c, out, in, pe, which, dag, clov, mode, factor, in0);
+  });
+}
+int qwsg_deo_s(qwsg_lattice* l, float* out, const float* in, int pe, int which, int dag, int clov,
+               int mode, double factor, const float* in0) {
+  return guarded([&] {
+    check_ctx(l);
+    deo<float>(*l->c, out, in, pe, which, dag, clov, mode, factor, in0);
+  });
+}
+int qwsg_clv_d(qwsg_lattice* l, double* out, const double* in, int pe) {
+  return guarded([&] {
+    check_ctx(l);
+    clv<double>(*l->c, out, in, pe);
+  });
+}
+int qwsg_clv_s(qwsg_lattice* l, float* out, const float* in, int pe) {
+  return guarded([&] {
+    check_ctx(l);
+    clv<float>(*l->c, out, in, pe);
+  });
+}
+int qwsg_mtilde_d(qwsg_lattice* l, double* out, const double* in) {
+  return guarded([&] {
+    check_ctx(l);
+    need_fields(*l->c, true);
+    mtilde_d(*l->c, out, in);
+  });
+}
+int qwsg_mtilde_dag_d(qwsg_lattice* l, double* out, const double* in) {
+  return guarded([&] {
+    check_ctx(l);
+    need_fields(*l->c, true);
+    mtilde_dag_d(*l->c, out, in);
+  });
+}
+int qwsg_mtilde_s(qwsg_lattice* l, float* out, const float* in) {
+  return guarded([&] {
+    check_ctx(l);
+    need_fields(*l->c, false);
+    mtilde_s(*l->c, out, in);
+  });
+}
+int qwsg_bicgstab_vm(qwsg_lattice* l, double* x, const double* b, int maxiter, int* iters) {
+  return guarded([&] {
+    check_ctx(l);
+    need_fields(*l->c, true);
+    int it = bicgstab_vm(*l->c, x, b, maxiter);
+    if (iters) *iters = it;
+  });
+}
 int qwsg_true_residual(qwsg_lattice* l, const double* x, const double* b, double* rel) {
   return guarded([&] {
     check_ctx(l);

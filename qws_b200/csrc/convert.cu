@@ -45,6 +45,14 @@ __device__ __forceinline__ QwsIdx qws_index(const Geom& G, const int x[4], int v
   return q;
 }
 
+// Even-odd reading of the same host arrays (qws_bqcd.cc:66-85; deo_in_d.cc:65-86):
+// the site (x,y,z,t) of parity p = (x+y+z+t)%2 sits in the x-half slot p at
+// compressed x index x/2.  Maps x[0] to that slot's x so qws_index applies.
+__device__ __forceinline__ void eo_slot(const Geom& G, int x[4]) {
+  const int p = (x[0] + x[1] + x[2] + x[3]) & 1;
+  x[0] = p * (G.L[0] / 2) + x[0] / 2;
+}
+
 __device__ __forceinline__ long nat_index(const Geom& G, const int x[4]) {
   return x[0] + (long)G.L[0] * (x[1] + (long)G.L[1] * (x[2] + (long)G.L[2] * x[3]));
 }
@@ -114,12 +122,49 @@ __device__ __forceinline__ void store_clover<double>(double* p, int pad, int g, 
   for (int j = 0; j < 36; j++) q[(size_t)j * pad + g] = make_double2(a[2 * j], a[2 * j + 1]);
 }
 
+// Half array of one parity p in the even-odd layout (vol elements, the
+// compressed index x/2) -> full planes, zero on the other parity.
 template <typename R>
-__global__ void k_qws2pl_gauge(Geom G, R* dst, const R* __restrict__ q, int vlen) {
+__global__ void k_qwseo2pl_sp(Geom G, R* dst, const R* __restrict__ q, int vlen, int p) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= G.V) return;
   int x[4];
   global_coords(G, g, x);
+  R v[24];
+  if (((x[0] + x[1] + x[2] + x[3]) & 1) == p) {
+    x[0] /= 2;  // slot 0 of a half array
+    QwsIdx Q = qws_index(G, x, vlen);
+#pragma unroll
+    for (int r = 0; r < 24; r++) v[r] = q[(Q.elem_sp * 24 + r) * vlen + Q.lane];
+  } else {
+#pragma unroll
+    for (int r = 0; r < 24; r++) v[r] = 0;
+  }
+  store_sp(dst, G.pad, g, v);
+}
+
+template <typename R>
+__global__ void k_pl2qwseo_sp(Geom G, R* q, const R* __restrict__ src, int vlen, int p) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G.V) return;
+  int x[4];
+  global_coords(G, g, x);
+  if (((x[0] + x[1] + x[2] + x[3]) & 1) != p) return;
+  x[0] /= 2;
+  QwsIdx Q = qws_index(G, x, vlen);
+  R v[24];
+  IO<R>::load_spinor(src, G.pad, g, v);
+#pragma unroll
+  for (int r = 0; r < 24; r++) q[(Q.elem_sp * 24 + r) * vlen + Q.lane] = v[r];
+}
+
+template <typename R>
+__global__ void k_qws2pl_gauge(Geom G, R* dst, const R* __restrict__ q, int vlen, int eo) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G.V) return;
+  int x[4];
+  global_coords(G, g, x);
+  if (eo) eo_slot(G, x);
   QwsIdx Q = qws_index(G, x, vlen);
   for (int mu = 0; mu < 4; mu++) {
     long elem = Q.elem_g0 + mu * Q.vol;
@@ -136,11 +181,12 @@ __global__ void k_qws2pl_gauge(Geom G, R* dst, const R* __restrict__ q, int vlen
 }
 
 template <typename R>
-__global__ void k_qws2pl_clover(Geom G, R* dst, const R* __restrict__ q, int vlen) {
+__global__ void k_qws2pl_clover(Geom G, R* dst, const R* __restrict__ q, int vlen, int eo) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= G.V) return;
   int x[4];
   global_coords(G, g, x);
+  if (eo) eo_slot(G, x);
   QwsIdx Q = qws_index(G, x, vlen);
   R a[72];
 #pragma unroll
@@ -204,7 +250,64 @@ __global__ void k_nat2pl_clover(Geom G, R* dst, const Rin* __restrict__ nat) {
 
 inline int nb(long n) { return (int)((n + 127) / 128); }
 
+__global__ void k_s2h(Geom G, __half* dst, const float* __restrict__ src) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G.V) return;
+  float v[24];
+  IO<float>::load_spinor(src, G.pad, g, v);
+  IO<H16>::store_spinor(dst, G.pad, g, v);
+}
+
+__global__ void k_h2s(Geom G, float* dst, const __half* __restrict__ src) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G.V) return;
+  float v[24];
+  IO<H16>::load_spinor(src, G.pad, g, v);
+  IO<float>::store_spinor(dst, G.pad, g, v);
+}
+
+__global__ void k_h2h(Geom G, __half* dst, const __half* __restrict__ src) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G.V) return;
+  const uint2* s = reinterpret_cast<const uint2*>(src);
+  uint2* d = reinterpret_cast<uint2*>(dst);
+#pragma unroll
+  for (int j = 0; j < 6; j++) d[(size_t)j * G.pad + g] = s[(size_t)j * G.pad + g];
+  reinterpret_cast<float*>(d + (size_t)6 * G.pad)[g] =
+      reinterpret_cast<const float*>(s + (size_t)6 * G.pad)[g];
+}
+
+__global__ void k_fields_s2h(Geom G, __half* Uh, const float* __restrict__ Us, __half* Ch,
+                             const float* __restrict__ Cs) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G.V) return;
+  const float2* u = reinterpret_cast<const float2*>(Us);
+  __half2* uh = reinterpret_cast<__half2*>(Uh);
+  for (int p = 0; p < 36; p++) uh[(size_t)p * G.pad + g] = __float22half2_rn(u[(size_t)p * G.pad + g]);
+  const float4* c = reinterpret_cast<const float4*>(Cs);
+  uint2* ch = reinterpret_cast<uint2*>(Ch);
+  for (int j = 0; j < 18; j++) {
+    float4 t = c[(size_t)j * G.pad + g];
+    float v[4] = {t.x, t.y, t.z, t.w};
+    ch[(size_t)j * G.pad + g] = IO<H16>::pack4(v, 1.0f);
+  }
+}
+
 }  // namespace
+
+void spinor_s2h(const Geom& G, __half* dst, const float* src, cudaStream_t st) {
+  k_s2h<<<nb(G.V), 128, 0, st>>>(G, dst, src);
+}
+void spinor_h2s(const Geom& G, float* dst, const __half* src, cudaStream_t st) {
+  k_h2s<<<nb(G.V), 128, 0, st>>>(G, dst, src);
+}
+void spinor_h2h(const Geom& G, __half* dst, const __half* src, cudaStream_t st) {
+  k_h2h<<<nb(G.V), 128, 0, st>>>(G, dst, src);
+}
+void fields_s2h(const Geom& G, __half* Uh, const float* Us, __half* Ch, const float* Cs,
+                cudaStream_t st) {
+  k_fields_s2h<<<nb(G.V), 128, 0, st>>>(G, Uh, Us, Ch, Cs);
+}
 
 template <typename R>
 void qws_to_planes_spinor(const Geom& G, R* dst, const R* qws, int vlen, int site0, int n,
@@ -217,12 +320,22 @@ void planes_to_qws_spinor(const Geom& G, R* qws, const R* src, int vlen, int sit
   if (n > 0) k_pl2qws_sp<R><<<nb(n), 128, 0, st>>>(G, qws, src, vlen, site0, n);
 }
 template <typename R>
-void qws_to_planes_gauge(const Geom& G, R* dst, const R* qws, int vlen, cudaStream_t st) {
-  k_qws2pl_gauge<R><<<nb(G.V), 128, 0, st>>>(G, dst, qws, vlen);
+void qws_eo_to_planes_spinor(const Geom& G, R* dst, const R* qws_half, int vlen, int p,
+                             cudaStream_t st) {
+  k_qwseo2pl_sp<R><<<nb(G.V), 128, 0, st>>>(G, dst, qws_half, vlen, p);
 }
 template <typename R>
-void qws_to_planes_clover(const Geom& G, R* dst, const R* qws, int vlen, cudaStream_t st) {
-  k_qws2pl_clover<R><<<nb(G.V), 128, 0, st>>>(G, dst, qws, vlen);
+void planes_to_qws_eo_spinor(const Geom& G, R* qws_half, const R* src, int vlen, int p,
+                             cudaStream_t st) {
+  k_pl2qwseo_sp<R><<<nb(G.V), 128, 0, st>>>(G, qws_half, src, vlen, p);
+}
+template <typename R>
+void qws_to_planes_gauge(const Geom& G, R* dst, const R* qws, int vlen, cudaStream_t st, bool eo) {
+  k_qws2pl_gauge<R><<<nb(G.V), 128, 0, st>>>(G, dst, qws, vlen, eo ? 1 : 0);
+}
+template <typename R>
+void qws_to_planes_clover(const Geom& G, R* dst, const R* qws, int vlen, cudaStream_t st, bool eo) {
+  k_qws2pl_clover<R><<<nb(G.V), 128, 0, st>>>(G, dst, qws, vlen, eo ? 1 : 0);
 }
 template <typename R>
 void nat_to_planes_spinor(const Geom& G, R* dst, const R* nat, cudaStream_t st) {
@@ -244,8 +357,10 @@ void nat_to_planes_clover(const Geom& G, R* dst, const Rin* nat, cudaStream_t st
 #define QWSG_INST(R)                                                                             \
   template void qws_to_planes_spinor<R>(const Geom&, R*, const R*, int, int, int, cudaStream_t); \
   template void planes_to_qws_spinor<R>(const Geom&, R*, const R*, int, int, int, cudaStream_t); \
-  template void qws_to_planes_gauge<R>(const Geom&, R*, const R*, int, cudaStream_t);            \
-  template void qws_to_planes_clover<R>(const Geom&, R*, const R*, int, cudaStream_t);           \
+  template void qws_eo_to_planes_spinor<R>(const Geom&, R*, const R*, int, int, cudaStream_t);   \
+  template void planes_to_qws_eo_spinor<R>(const Geom&, R*, const R*, int, int, cudaStream_t);   \
+  template void qws_to_planes_gauge<R>(const Geom&, R*, const R*, int, cudaStream_t, bool);      \
+  template void qws_to_planes_clover<R>(const Geom&, R*, const R*, int, cudaStream_t, bool);     \
   template void nat_to_planes_spinor<R>(const Geom&, R*, const R*, cudaStream_t);                \
   template void planes_to_nat_spinor<R>(const Geom&, R*, const R*, cudaStream_t);
 QWSG_INST(float)

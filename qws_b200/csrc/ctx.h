@@ -69,6 +69,10 @@ struct Ctx {
   std::vector<void*> owned;
   void* stage = nullptr;  // host<->device conversion staging
   size_t stage_bytes = 0;
+  // sites of each colour that touch a SAP-block face (DD order, ascending)
+  int* face_list[2] = {nullptr, nullptr};
+  int n_face[2] = {0, 0};
+  void ensure_face_lists();
 
   // per-kernel CUDA-event timing (kind = kernel_kind(), see solver.cu)
   struct KRec {
@@ -99,6 +103,34 @@ struct Ctx {
   // synchronous read of n reduction results
   const double* fetch(int n);
   void check_launch(const char* what);
+
+  // FP16-storage SAP (precision form): fields converted from the FP32 ones,
+  // work spinors with per-site scales, and the flexible inner solver's w
+  __half* Uh = nullptr;
+  __half* Ch = nullptr;
+  bool fields_h_valid = false;
+  __half* h_s = nullptr;
+  __half* h_a = nullptr;
+  __half* h_t = nullptr;
+  __half* h_b = nullptr;
+  float* in_w = nullptr;
+  __half* alloc_spinor_h();
+  void ensure_fields_h();
+  void ensure_hp();
+  long n_prec_s_h = 0;
+
+  // even-odd family: the fields the parity operators read (the resident ones
+  // unless set; the drop-in supplies the even-odd reading of QWS's host
+  // arrays), the parities of mtilde (pce_f/pco_f of qws_init_), work buffers
+  const double* eoUd = nullptr;
+  const double* eoCd = nullptr;
+  const float* eoUs = nullptr;
+  const float* eoCs = nullptr;
+  int pce = 0, pco = 1;
+  double* eo_d[6] = {};
+  float* eo_s[2] = {};
+  void ensure_eo();
+  long n_mtilde = 0;
 };
 
 // kernel kinds for timing
@@ -111,7 +143,10 @@ enum {
   K_SAPE_F32 = 5,   // SAP update s_e += in_e - D_blk a_e
   K_OUT_F64 = 6,    // face hops, FP64
   K_OUT_F32 = 7,    // face hops, FP32
-  K_NKIND = 8
+  K_JINV_F16 = 8,   // the same three in FP16 storage
+  K_SAPE_F16 = 9,
+  K_OUT_F16 = 10,
+  K_NKIND = 11
 };
 const char* kernel_kind_name(int k);
 // drain event records into per-kind totals (launches, ms, algorithmic bytes)
@@ -129,6 +164,18 @@ void dslash_outer(Ctx& c, R* out, const R* in, int col, int dom, double factor, 
 void jinv_s(Ctx& c, float* x, const float* b, int col, int nm);
 void prec_ddd_s(Ctx& c, float* out, const float* in, int nsap, int nm);
 void prec_s(Ctx& c, float* out, const float* in, int nsap, int nm);
+// FP16-storage SAP preconditioner with the reference's half-precision sweep
+// count (assign_mult_mSAP_s_h_, prec_ddd_s_h.h:63-231: nsap-1 sweeps + the
+// final stage); FP32 in and out
+void prec_s_h(Ctx& c, float* out, const float* in, int nsap, int nm);
+// flexible inner BiCGStab with the FP16 SAP (bicgstab_precdd_s_h.cc:83-369)
+int bicgstab_precdd_s_h(Ctx& c, float* x, const float* b, double tol, int maxiter, int nsap,
+                        int nm, double* final_rel);
+// outer FP64 loop around it (bicgstab_dd_mix2_hf.cc:110-373); reliable > 0
+// adds restarts from the recomputed true residual until |b - Dx|/|b| < tol
+void bicgstab_dd_mix2_hf(Ctx& c, double* x, const double* b, double tol, int maxiter,
+                         double tol_s, int maxiter_s, int nsap, int nm, int reliable,
+                         SolveStats* stats);
 int bicgstab_precdd_s(Ctx& c, float* x, const float* b, double tol, int maxiter, int nsap, int nm,
                       double* final_rel);
 void bicgstab_dd_mix(Ctx& c, double* x, const double* b, double tol, int maxiter, double tol_s,
@@ -137,6 +184,17 @@ void bicgstab_dd_mix(Ctx& c, double* x, const double* b, double tol, int maxiter
 double true_residual(Ctx& c, const double* x, const double* b);
 
 void set_error(const std::string& m);
+
+// even-odd family (eo_host.cu); which/dag/clov/mode as in EoArgs (kernels.h)
+template <typename R>
+void deo(Ctx& c, R* out, const R* in, int pe, int which, int dag, int clov, int mode,
+         double factor, const R* in0);
+template <typename R>
+void clv(Ctx& c, R* out, const R* in, int pe);
+void mtilde_d(Ctx& c, double* out, const double* in);      // qws.cc:551-556
+void mtilde_dag_d(Ctx& c, double* out, const double* in);  // qws.cc:557-565
+void mtilde_s(Ctx& c, float* out, const float* in);        // qws.cc:598-604
+int bicgstab_vm(Ctx& c, double* x, const double* b, int maxiter);  // bicgstab.cc:68
 
 }  // namespace qwsg
 

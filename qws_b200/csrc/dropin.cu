@@ -44,9 +44,25 @@ struct Dropin {
   float* ps[3] = {nullptr, nullptr, nullptr};   // FP32 planes
   double t_solver = 0;
   long n_calls_dd_mix = 0;
+  // even-odd family: the even-odd reading of the same host fields, and work
+  // planes (0 out, 1 in, 2 in0, 3 the face snapshot of deo_out_pre)
+  bool eo_dirty = true;
+  double* eUd = nullptr;
+  double* eCd = nullptr;
+  float* eUs = nullptr;
+  float* eCs = nullptr;
+  double* ed[4] = {};
+  float* es[4] = {};
+  int pce = 0, pco = 1;
 };
 Dropin g;
 int g_vlend_req = 0, g_vlens_req = 0;
+
+// the host fields changed: both readings must be uploaded again
+void mark_dirty() {
+  g.fields_dirty = true;
+  g.eo_dirty = true;
+}
 
 Ctx& ctx() {
   if (!g.lat) {
@@ -138,6 +154,65 @@ void down(Ctx& c, void* host, const R* planes, int dom, int vlen) {
   QWSG_CUDA(cudaStreamSynchronize(c.st));
 }
 
+// the even-odd operators read glud/clvd/glus/clvs with the parity split
+// (qws_bqcd.cc:66-85): upload that reading next to the DD one when dirty
+void sync_eo(Ctx& c) {
+  sync_fields(c);
+  const size_t n = (size_t)72 * c.G.pad;
+  if (!g.eUd) {
+    QWSG_CUDA(cudaMalloc(&g.eUd, sizeof(double) * n));
+    QWSG_CUDA(cudaMalloc(&g.eCd, sizeof(double) * n));
+    QWSG_CUDA(cudaMalloc(&g.eUs, sizeof(float) * n));
+    QWSG_CUDA(cudaMalloc(&g.eCs, sizeof(float) * n));
+    for (int i = 0; i < 4; i++) {
+      g.ed[i] = c.alloc_spinor<double>();
+      g.es[i] = c.alloc_spinor<float>();
+    }
+    g.eo_dirty = true;
+  }
+  if (g.eo_dirty || g.always_upload) {
+    const size_t V = (size_t)c.G.V;
+    void* d = stage(c, sizeof(double) * 72 * V);
+    QWSG_CUDA(cudaMemcpyAsync(d, glud, sizeof(double) * 72 * V, cudaMemcpyHostToDevice, c.st));
+    qws_to_planes_gauge<double>(c.G, g.eUd, (const double*)d, g.vlend, c.st, true);
+    QWSG_CUDA(cudaMemcpyAsync(d, clvd, sizeof(double) * 72 * V, cudaMemcpyHostToDevice, c.st));
+    qws_to_planes_clover<double>(c.G, g.eCd, (const double*)d, g.vlend, c.st, true);
+    QWSG_CUDA(cudaMemcpyAsync(d, glus, sizeof(float) * 72 * V, cudaMemcpyHostToDevice, c.st));
+    qws_to_planes_gauge<float>(c.G, g.eUs, (const float*)d, g.vlens, c.st, true);
+    QWSG_CUDA(cudaMemcpyAsync(d, clvs, sizeof(float) * 72 * V, cudaMemcpyHostToDevice, c.st));
+    qws_to_planes_clover<float>(c.G, g.eCs, (const float*)d, g.vlens, c.st, true);
+    c.check_launch("even-odd field upload");
+    QWSG_CUDA(cudaStreamSynchronize(c.st));
+    g.eo_dirty = false;
+  }
+  c.eoUd = g.eUd;
+  c.eoCd = g.eCd;
+  c.eoUs = g.eUs;
+  c.eoCs = g.eCs;
+  c.pce = g.pce;
+  c.pco = g.pco;
+}
+
+// host half array of parity p (vol elements, even-odd layout) <-> planes
+template <typename R>
+void up_eo(Ctx& c, R* planes, const void* host, int p, int vlen) {
+  const size_t n = (size_t)c.G.Vh * 24;
+  R* d = (R*)stage(c, sizeof(R) * n);
+  QWSG_CUDA(cudaMemcpyAsync(d, host, sizeof(R) * n, cudaMemcpyHostToDevice, c.st));
+  qws_eo_to_planes_spinor<R>(c.G, planes, d, vlen, p, c.st);
+  c.check_launch("even-odd spinor upload");
+}
+
+template <typename R>
+void down_eo(Ctx& c, void* host, const R* planes, int p, int vlen) {
+  const size_t n = (size_t)c.G.Vh * 24;
+  R* d = (R*)stage(c, sizeof(R) * n);
+  planes_to_qws_eo_spinor<R>(c.G, d, planes, vlen, p, c.st);
+  c.check_launch("even-odd spinor download");
+  QWSG_CUDA(cudaMemcpyAsync(host, d, sizeof(R) * n, cudaMemcpyDeviceToHost, c.st));
+  QWSG_CUDA(cudaStreamSynchronize(c.st));
+}
+
 int xyzt2i(int* j) {
   if (std_xyzt2i_) return std_xyzt2i_(j);
   int lex = j[0] + nx * (j[1] + ny * (j[2] + nz * j[3]));
@@ -175,7 +250,7 @@ int qwsg_set_host_vlen(int vlend, int vlens) {
 }
 
 int qwsg_mark_fields_dirty(void) {
-  g.fields_dirty = true;
+  mark_dirty();
   return 0;
 }
 
@@ -184,9 +259,12 @@ qwsg_lattice* qwsg_dropin_lattice(void) { return g.lat; }
 // qws.cc:130-316 for one process holding the whole lattice
 void qws_init_(int* lx, int* ly, int* lz, int* lt, int* npe_f, int* fbc_f, int* pce_f,
                int* pco_f, int* block_size) {
-  (void)pce_f;
-  (void)pco_f;
   (void)block_size;  // unused by the reference as well (qws.cc:121-122)
+  // the parities of mtilde_vm_/mtilde_s_/bicgstab_vm_ (qws.cc:134-135)
+  if (!((*pce_f == 0 && *pco_f == 1) || (*pce_f == 1 && *pco_f == 0)))
+    die("qws_init_: pce/pco must be (0,1) or (1,0)");
+  g.pce = *pce_f;
+  g.pco = *pco_f;
   const char* e;
   g.vlend = g_vlend_req ? g_vlend_req : ((e = getenv("QWSG_VLEND")) ? atoi(e) : 8);
   g.vlens = g_vlens_req ? g_vlens_req : ((e = getenv("QWSG_VLENS")) ? atoi(e) : 16);
@@ -232,14 +310,24 @@ void qws_init_(int* lx, int* ly, int* lz, int* lt, int* npe_f, int* fbc_f, int* 
   int L[4] = {nx, ny, nz, nt}, NB[4] = {2, 1, 1, 1};
   if (qwsg_create(&g.lat, L, NB, fbc_f[3] == -1 ? -1 : 1) != 0)
     die(std::string("qws_init_: ") + qwsg_last_error());
-  g.fields_dirty = true;
+  mark_dirty();
   guard("qws_init_", [&] { ensure_planes(ctx()); });
 }
 
 void qws_finalize_(void) {
-  if (g.lat) qwsg_destroy(g.lat);
+  if (g.lat) {
+    cudaStreamSynchronize(g.lat->c->st);
+    cudaFree(g.eUd);
+    cudaFree(g.eCd);
+    cudaFree(g.eUs);
+    cudaFree(g.eCs);
+    qwsg_destroy(g.lat);
+  }
   g.lat = nullptr;
   for (int i = 0; i < 3; i++) g.pd[i] = nullptr, g.ps[i] = nullptr;  // freed with the handle
+  for (int i = 0; i < 4; i++) g.ed[i] = nullptr, g.es[i] = nullptr;
+  g.eUd = g.eCd = nullptr;
+  g.eUs = g.eCs = nullptr;
   free(glud);
   free(glus);
   free(clvd);
@@ -251,7 +339,13 @@ void qws_finalize_(void) {
 }
 
 // ---- loaders (qws_bqcd.cc) --------------------------------------------------
-void qws_loadg_dd_(double* u, int* volh_tot, double* in_kappa) {
+}  // extern "C"
+
+// the x position a loader writes site (x,y,z,t) to: the x-halves of the DD
+// layout, or the parity slot with x/2 of the even-odd layout (qws_bqcd.cc:82-85)
+static inline int slot_x(int x, int eo, bool eo_layout) { return eo_layout ? eo * nxh + x / 2 : x; }
+
+static void load_gauge(double* u, int* volh_tot, double* in_kappa, bool eo_layout) {
   kappa = *in_kappa;
   mkappa = -kappa;
   kappa2 = kappa * kappa;
@@ -266,9 +360,10 @@ void qws_loadg_dd_(double* u, int* volh_tot, double* in_kappa) {
           int i = xyzt2i(j), eo = eo_of(j);
           size_t ihh = (size_t)(i - 1) * 18 + (size_t)eo * (*volh_tot) * 18;
           size_t lane_d, lane_s;
-          size_t ed = qws_elem(x, y, z, t, g.vlend, &lane_d);
-          size_t es = qws_elem(x, y, z, t, g.vlens, &lane_s);
-          int dom = x / nxh;
+          const int xs = slot_x(x, eo, eo_layout);
+          size_t ed = qws_elem(xs, y, z, t, g.vlend, &lane_d);
+          size_t es = qws_elem(xs, y, z, t, g.vlens, &lane_s);
+          int dom = xs / nxh;
           size_t vold_ = (size_t)vold, vols_ = (size_t)vols;
           for (int mu = 0; mu < 4; mu++) {
             // link element: dom*4*vol + mu*vol + in-domain index
@@ -283,7 +378,7 @@ void qws_loadg_dd_(double* u, int* volh_tot, double* in_kappa) {
                 }
           }
         }
-  g.fields_dirty = true;
+  mark_dirty();
 }
 
 // BQCD's 36 reals per chiral block -> QWS packing (qws_bqcd.cc:301-377)
@@ -291,7 +386,7 @@ static const int kClvPerm[36] = {0,  1,  20, 21, 32, 33, 2,  3,  4,  5,  6,  7,
                                  8,  9,  10, 11, 12, 13, 14, 15, 16, 17, 18, 19,
                                  22, 23, 24, 25, 26, 27, 28, 29, 30, 31, 34, 35};
 
-void qws_loadc_dd_(double* c, int* volh) {
+static void load_clover(double* c, int* volh, bool eo_layout) {
   double* cd = (double*)clvd;
   float* cs = (float*)clvs;
 #pragma omp parallel for collapse(2)
@@ -303,8 +398,9 @@ void qws_loadc_dd_(double* c, int* volh) {
           int i = xyzt2i(j), eo = eo_of(j);
           size_t ihh = (size_t)(i - 1) * 72 + (size_t)eo * (*volh) * 72;
           size_t lane_d, lane_s;
-          size_t ed = qws_elem(x, y, z, t, g.vlend, &lane_d);
-          size_t es = qws_elem(x, y, z, t, g.vlens, &lane_s);
+          const int xs = slot_x(x, eo, eo_layout);
+          size_t ed = qws_elem(xs, y, z, t, g.vlend, &lane_d);
+          size_t es = qws_elem(xs, y, z, t, g.vlens, &lane_s);
           for (int ud = 0; ud < 2; ud++)
             for (int k = 0; k < 36; k++) {
               double v = c[kClvPerm[k] + ud * 36 + ihh];
@@ -312,9 +408,14 @@ void qws_loadc_dd_(double* c, int* volh) {
               cs[(es * 72 + ud * 36 + k) * g.vlens + lane_s] = (float)v;
             }
         }
-  g.fields_dirty = true;
+  mark_dirty();
 }
 
+extern "C" {
+void qws_loadg_dd_(double* u, int* volh_tot, double* in_kappa) { load_gauge(u, volh_tot, in_kappa, false); }
+void qws_loadc_dd_(double* c, int* volh) { load_clover(c, volh, false); }
+void qws_loadg_bqcd_(double* u, int* volh_tot, double* in_kappa) { load_gauge(u, volh_tot, in_kappa, true); }
+void qws_loadc_bqcd_(double* c, int* volh) { load_clover(c, volh, true); }
 }  // extern "C"
 
 template <typename R>
@@ -357,7 +458,52 @@ static void storef(double* oute, double* outo, const R* in, int vlen) {
         }
 }
 
+// the even sites only, into / out of a half array of the even-odd layout
+// (qws_bqcd.cc:384-498)
+template <typename R>
+static void loadf_even(R* out, const double* in, int vlen) {
+#pragma omp parallel for collapse(2)
+  for (int t = 0; t < nt; t++)
+    for (int z = 0; z < nz; z++)
+      for (int y = 0; y < ny; y++)
+        for (int x = 0; x < nx; x++) {
+          int j[4] = {x, y, z, t};
+          if (eo_of(j) != 0) continue;
+          size_t ihh = (size_t)(xyzt2i(j) - 1) * 24;
+          size_t lane;
+          size_t e = qws_elem(x / 2, y, z, t, vlen, &lane);
+          for (int c = 0; c < 3; c++)
+            for (int s = 0; s < 4; s++)
+              for (int ri = 0; ri < 2; ri++)
+                out[(e * 24 + c * 8 + s * 2 + ri) * vlen + lane] = (R)in[ri + 2 * s + 8 * c + ihh];
+        }
+}
+
+template <typename R>
+static void storef_even(double* out, const R* in, int vlen) {
+#pragma omp parallel for collapse(2)
+  for (int t = 0; t < nt; t++)
+    for (int z = 0; z < nz; z++)
+      for (int y = 0; y < ny; y++)
+        for (int x = 0; x < nx; x++) {
+          int j[4] = {x, y, z, t};
+          if (eo_of(j) != 0) continue;
+          size_t ihh = (size_t)(xyzt2i(j) - 1) * 24;
+          size_t lane;
+          size_t e = qws_elem(x / 2, y, z, t, vlen, &lane);
+          for (int c = 0; c < 3; c++)
+            for (int s = 0; s < 4; s++)
+              for (int ri = 0; ri < 2; ri++)
+                out[ri + 2 * s + 8 * c + ihh] = (double)in[(e * 24 + c * 8 + s * 2 + ri) * vlen + lane];
+        }
+}
+
 extern "C" {
+
+void qws_loadfd_bqcd_(scd_t* out, double* in) { loadf_even<double>((double*)out, in, g.vlend); }
+void qws_loadfs_bqcd_(scs_t* out, double* in) { loadf_even<float>((float*)out, in, g.vlens); }
+void qws_storefd_bqcd_(double* out, scd_t* in) { storef_even<double>(out, (const double*)in, g.vlend); }
+void qws_storefs_bqcd_(double* out, scs_t* in) { storef_even<float>(out, (const float*)in, g.vlens); }
 
 void qws_loadfd_dd_(scd_t* out, double* ine, double* ino) { loadf<double>((double*)out, ine, ino, g.vlend); }
 void qws_storefd_dd_(double* oute, double* outo, scd_t* in) { storef<double>(oute, outo, (const double*)in, g.vlend); }
@@ -392,6 +538,57 @@ void bicgstab_precdd_s_(scs_t* x, scs_t* b, double* tol, int* conviter, int* max
     int it = bicgstab_precdd_s(c, g.ps[0], g.ps[1], *tol, *maxiter, *nsap, *nm, nullptr);
     down<float>(c, x, g.ps[0], -1, g.vlens);
     *conviter = it;
+  });
+}
+
+// half-precision pair: the FP16 copies are made from the resident FP32 fields
+// on first use, so qws_h_init_ only has to mark the host fields as current
+// (qws_h.cc:150-166 converts glus/clvs itself)
+void qws_h_init_(const glus_t* g_s, const clvs_t* c_s) {
+  (void)g_s;
+  (void)c_s;
+  mark_dirty();
+}
+void bqcd_qws_h_init_(void) { qws_h_init_(glus, clvs); }
+
+void assign_mult_mSAP_s_h_(scs_t* xs, const scs_t* bs, const int* nsap, const int* nm) {
+  guard("assign_mult_mSAP_s_h_", [&] {
+    Ctx& c = ctx();
+    sync_fields(c);
+    up<float>(c, g.ps[1], bs, -1, g.vlens);
+    prec_s_h(c, g.ps[0], g.ps[1], *nsap, *nm);
+    down<float>(c, xs, g.ps[0], -1, g.vlens);
+  });
+}
+
+// assign_mult_wd_s_ (prec_ddd_s_h.h:233-277): the FP32 D
+void assign_mult_wd_s_(scs_t* x, const scs_t* b) { ddd_s_(x, (scs_t*)b); }
+
+void bicgstab_precdd_s_h_(scs_t* x, const scs_t* b, const double* tol, int* conviter,
+                          const int* maxiter, const int* nsap, const int* nm) {
+  guard("bicgstab_precdd_s_h_", [&] {
+    Ctx& c = ctx();
+    sync_fields(c);
+    up<float>(c, g.ps[1], b, -1, g.vlens);
+    int it = bicgstab_precdd_s_h(c, g.ps[0], g.ps[1], *tol, *maxiter, *nsap, *nm, nullptr);
+    down<float>(c, x, g.ps[0], -1, g.vlens);
+    *conviter = it;
+  });
+}
+
+void bicgstab_dd_mix2_hf_(scd_t* x, const scd_t* b, const double* tol, int* conviter,
+                          const int* maxiter, const double* tol_s, const int* maxiter_s,
+                          const int* nsap, const int* nm) {
+  guard("bicgstab_dd_mix2_hf_", [&] {
+    Ctx& c = ctx();
+    sync_fields(c);
+    up<double>(c, g.pd[1], b, -1, g.vlend);
+    up<double>(c, g.pd[0], x, -1, g.vlend);
+    SolveStats st;
+    bicgstab_dd_mix2_hf(c, g.pd[0], g.pd[1], *tol, *maxiter, *tol_s, *maxiter_s, *nsap, *nm, 0,
+                        &st);
+    down<double>(c, x, g.pd[0], -1, g.vlend);
+    *conviter = st.outer_iters;
   });
 }
 
@@ -523,6 +720,227 @@ void ddd_out_pos_s_(scs_t* out, scs_t* in, int* DEO, float factor) {
 void ddd_out_pre_s_no_timer_(scs_t* in, int* DEO) { ddd_out_pre_s_(in, DEO); }
 void ddd_out_pos_s_no_timer_(scs_t* out, scs_t* in, int* DEO, float factor) {
   ddd_out_pos_s_(out, in, DEO, factor);
+}
+
+}  // extern "C"
+
+// ---- even-odd (site parity) family (qws.cc:390-605, deo_*.cc) --------------
+// Arguments are one-parity half arrays (vol elements, x/2 compressed):
+// `out` of parity pe, `in` of parity po = 1 - pe, `in0` of parity pe.
+namespace {
+
+struct EoOp {
+  int which, dag, clov, mode;  // hop set (1 in, 2 out, 3 all), adjoint, A^-1, store mode
+};
+constexpr EoOp kIn{1, 0, 0, 0}, kDeeIn{1, 0, 1, 0}, kDagIn{1, 1, 0, 0}, kDeeDagIn{1, 1, 1, 0},
+    kOmDeeIn{1, 0, 1, 2}, kOmDagIn{1, 1, 0, 2}, kPos{2, 0, 0, 1}, kDagPos{2, 1, 0, 1},
+    kDeePos{2, 0, 1, 1}, kDeeDagPos{2, 1, 1, 1}, kAll{3, 0, 0, 0}, kDeeAll{3, 0, 1, 0},
+    kDagAll{3, 1, 0, 0}, kDeeDagAll{3, 1, 1, 0}, kOmDeeAll{3, 0, 1, 2}, kOmDagAll{3, 1, 0, 2};
+
+void check_parities(const char* name, const int* pe, const int* po) {
+  if (!((*pe == 0 && *po == 1) || (*pe == 1 && *po == 0)))
+    die(std::string(name) + ": parities must be (0,1) or (1,0)");
+}
+
+template <typename R>
+int eo_vlen() {
+  return sizeof(R) == 8 ? g.vlend : g.vlens;
+}
+template <typename R>
+R** eo_planes();
+template <>
+double** eo_planes<double>() {
+  return g.ed;
+}
+template <>
+float** eo_planes<float>() {
+  return g.es;
+}
+
+// out = op(in); pos ops (OUT hops, mode 1) read the snapshot taken by the pre
+template <typename R>
+void eo_apply(const char* name, const int* pe, const int* po, void* out, const void* in,
+              const void* in0, EoOp op, double factor) {
+  check_parities(name, pe, po);
+  guard(name, [&] {
+    Ctx& c = ctx();
+    sync_eo(c);
+    R** P = eo_planes<R>();
+    const int vl = eo_vlen<R>();
+    const R* src = P[3];
+    if (op.which != 2) {
+      up_eo<R>(c, P[1], in, *po, vl);
+      src = P[1];
+    }
+    if (op.mode == 1) up_eo<R>(c, P[0], out, *pe, vl);
+    if (op.mode == 2) up_eo<R>(c, P[2], in0, *pe, vl);
+    deo<R>(c, P[0], src, *pe, op.which, op.dag, op.clov, op.mode, factor,
+           op.mode == 2 ? P[2] : nullptr);
+    down_eo<R>(c, out, P[0], *pe, vl);
+  });
+}
+
+// deo_out_pre: keep the field whose faces the following pos reads
+template <typename R>
+void eo_pre(const char* name, const int* pe, const int* po, const void* in) {
+  check_parities(name, pe, po);
+  guard(name, [&] {
+    Ctx& c = ctx();
+    sync_eo(c);
+    up_eo<R>(c, eo_planes<R>()[3], in, *po, eo_vlen<R>());
+  });
+}
+
+template <typename R>
+void eo_clover(const char* name, const int* pe, void* out, const void* in) {
+  if (*pe != 0 && *pe != 1) die(std::string(name) + ": parity must be 0 or 1");
+  guard(name, [&] {
+    Ctx& c = ctx();
+    sync_eo(c);
+    R** P = eo_planes<R>();
+    up_eo<R>(c, P[1], in, *pe, eo_vlen<R>());
+    clv<R>(c, P[0], P[1], *pe);
+    down_eo<R>(c, out, P[0], *pe, eo_vlen<R>());
+  });
+}
+
+// mtilde family on parity-pce half arrays
+template <typename R, typename F>
+void eo_mtilde(const char* name, void* out, const void* in, F&& f) {
+  guard(name, [&] {
+    Ctx& c = ctx();
+    sync_eo(c);
+    R** P = eo_planes<R>();
+    up_eo<R>(c, P[1], in, g.pce, eo_vlen<R>());
+    f(c, P[0], P[1]);
+    down_eo<R>(c, out, P[0], g.pce, eo_vlen<R>());
+  });
+}
+
+}  // namespace
+
+extern "C" {
+
+void deo_in_vm_(int* pe, int* po, scd_t* out, scd_t* in) {
+  eo_apply<double>("deo_in_vm_", pe, po, out, in, nullptr, kIn, 0);
+}
+void dee_deo_in_vm_(int* pe, int* po, scd_t* out, scd_t* in) {
+  eo_apply<double>("dee_deo_in_vm_", pe, po, out, in, nullptr, kDeeIn, 0);
+}
+void deo_dag_in_vm_(int* pe, int* po, scd_t* out, scd_t* in) {
+  eo_apply<double>("deo_dag_in_vm_", pe, po, out, in, nullptr, kDagIn, 0);
+}
+void dee_deo_dag_in_vm_(int* pe, int* po, scd_t* out, scd_t* in) {
+  eo_apply<double>("dee_deo_dag_in_vm_", pe, po, out, in, nullptr, kDeeDagIn, 0);
+}
+void one_minus_dee_deo_in_vm_(int* pe, int* po, scd_t* out, scd_t* in, scd_t* in0, double factor) {
+  eo_apply<double>("one_minus_dee_deo_in_vm_", pe, po, out, in, in0, kOmDeeIn, factor);
+}
+void one_minus_deo_dag_in_vm_(int* pe, int* po, scd_t* out, scd_t* in, scd_t* in0, double factor) {
+  eo_apply<double>("one_minus_deo_dag_in_vm_", pe, po, out, in, in0, kOmDagIn, factor);
+}
+void deo_out_pre_vm_(int* pe, int* po, scd_t* out, scd_t* in) {
+  (void)out;
+  eo_pre<double>("deo_out_pre_vm_", pe, po, in);
+}
+void deo_dag_out_pre_vm_(int* pe, int* po, scd_t* out, scd_t* in) {
+  (void)out;
+  eo_pre<double>("deo_dag_out_pre_vm_", pe, po, in);
+}
+void deo_out_pos_vm_(int* pe, int* po, scd_t* out, scd_t* in, double factor) {
+  eo_apply<double>("deo_out_pos_vm_", pe, po, out, in, nullptr, kPos, factor);
+}
+void deo_dag_out_pos_vm_(int* pe, int* po, scd_t* out, scd_t* in, double factor) {
+  eo_apply<double>("deo_dag_out_pos_vm_", pe, po, out, in, nullptr, kDagPos, factor);
+}
+void dee_deo_out_pos_vm_(int* pe, int* po, scd_t* out, scd_t* in, double factor) {
+  eo_apply<double>("dee_deo_out_pos_vm_", pe, po, out, in, nullptr, kDeePos, factor);
+}
+void dee_deo_dag_out_pos_vm_(int* pe, int* po, scd_t* out, scd_t* in, double factor) {
+  eo_apply<double>("dee_deo_dag_out_pos_vm_", pe, po, out, in, nullptr, kDeeDagPos, factor);
+}
+void clvd_vm_(int* pe, scd_t* inout) { eo_clover<double>("clvd_vm_", pe, inout, inout); }
+void clvd_vm2_(int* pe, scd_t* out, scd_t* in) { eo_clover<double>("clvd_vm2_", pe, out, in); }
+void deo_vm_(int* pe, int* po, scd_t* out, scd_t* in) {
+  eo_apply<double>("deo_vm_", pe, po, out, in, nullptr, kAll, 0);
+}
+void dee_deo_vm_(int* pe, int* po, scd_t* out, scd_t* in) {
+  eo_apply<double>("dee_deo_vm_", pe, po, out, in, nullptr, kDeeAll, 0);
+}
+void one_minus_dee_deo_vm_(int* pe, int* po, scd_t* out, scd_t* in, scd_t* in0) {
+  eo_apply<double>("one_minus_dee_deo_vm_", pe, po, out, in, in0, kOmDeeAll, -kappa2);
+}
+void deo_dag_vm_(int* pe, int* po, scd_t* out, scd_t* in) {
+  eo_apply<double>("deo_dag_vm_", pe, po, out, in, nullptr, kDagAll, 0);
+}
+void dee_deo_dag_vm_(int* pe, int* po, scd_t* out, scd_t* in) {
+  eo_apply<double>("dee_deo_dag_vm_", pe, po, out, in, nullptr, kDeeDagAll, 0);
+}
+void one_minus_deo_dag_vm_(int* pe, int* po, scd_t* out, scd_t* in, scd_t* in0) {
+  eo_apply<double>("one_minus_deo_dag_vm_", pe, po, out, in, in0, kOmDagAll, -kappa2);
+}
+void mtilde_vm_(scd_t* out, scd_t* in) {
+  eo_mtilde<double>("mtilde_vm_", out, in,
+                    [](Ctx& c, double* o, const double* i) { mtilde_d(c, o, i); });
+}
+void mtilde_dag_vm_(scd_t* out, scd_t* in) {
+  eo_mtilde<double>("mtilde_dag_vm_", out, in,
+                    [](Ctx& c, double* o, const double* i) { mtilde_dag_d(c, o, i); });
+}
+void mtdagmt_vm_(scd_t* out, scd_t* in) {
+  eo_mtilde<double>("mtdagmt_vm_", out, in, [](Ctx& c, double* o, const double* i) {
+    double* t = g.ed[2];
+    mtilde_d(c, t, i);
+    mtilde_dag_d(c, o, t);
+  });
+}
+// bicgstab.cc:68-333: x (initial guess in, solution out) and b are parity-pce half arrays
+void bicgstab_vm_(scd_t* x, scd_t* b, int* conviter, int* maxiter) {
+  guard("bicgstab_vm_", [&] {
+    Ctx& c = ctx();
+    sync_eo(c);
+    double** P = g.ed;
+    up_eo<double>(c, P[0], x, g.pce, g.vlend);
+    up_eo<double>(c, P[1], b, g.pce, g.vlend);
+    *conviter = bicgstab_vm(c, P[0], P[1], *maxiter);
+    down_eo<double>(c, x, P[0], g.pce, g.vlend);
+  });
+}
+
+void deo_in_s_(int* pe, int* po, scs_t* out, scs_t* in) {
+  eo_apply<float>("deo_in_s_", pe, po, out, in, nullptr, kIn, 0);
+}
+void dee_deo_in_s_(int* pe, int* po, scs_t* out, scs_t* in) {
+  eo_apply<float>("dee_deo_in_s_", pe, po, out, in, nullptr, kDeeIn, 0);
+}
+void one_minus_dee_deo_in_s_(int* pe, int* po, scs_t* out, scs_t* in, scs_t* in0, float factor) {
+  eo_apply<float>("one_minus_dee_deo_in_s_", pe, po, out, in, in0, kOmDeeIn, factor);
+}
+// deo_out_{pre,pos}_s_ take const pointers in the reference (qws.cc:577-578); pos writes out
+void deo_out_pre_s_(const int* pe, const int* po, const scs_t* out, const scs_t* in) {
+  (void)out;
+  eo_pre<float>("deo_out_pre_s_", pe, po, in);
+}
+void deo_out_pos_s_(const int* pe, const int* po, const scs_t* out, const scs_t* in, float factor) {
+  eo_apply<float>("deo_out_pos_s_", pe, po, (void*)out, in, nullptr, kPos, factor);
+}
+void dee_deo_out_pos_s_(int* pe, int* po, scs_t* out, scs_t* in, float factor) {
+  eo_apply<float>("dee_deo_out_pos_s_", pe, po, out, in, nullptr, kDeePos, factor);
+}
+void clv_s_(int* pe, scs_t* inout) { eo_clover<float>("clv_s_", pe, inout, inout); }
+void deo_s_(int* pe, int* po, scs_t* out, scs_t* in) {
+  eo_apply<float>("deo_s_", pe, po, out, in, nullptr, kAll, 0);
+}
+void dee_deo_s_(int* pe, int* po, scs_t* out, scs_t* in) {
+  eo_apply<float>("dee_deo_s_", pe, po, out, in, nullptr, kDeeAll, 0);
+}
+void one_minus_dee_deo_s_(int* pe, int* po, scs_t* out, scs_t* in, scs_t* in0) {
+  eo_apply<float>("one_minus_dee_deo_s_", pe, po, out, in, in0, kOmDeeAll,
+                  (double)(-(float)kappa2));
+}
+void mtilde_s_(scs_t* out, scs_t* in) {
+  eo_mtilde<float>("mtilde_s_", out, in,
+                   [](Ctx& c, float* o, const float* i) { mtilde_s(c, o, i); });
 }
 
 // ---- converters (reordering.cc) ---------------------------------------------

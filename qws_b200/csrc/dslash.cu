@@ -1,4 +1,5 @@
-// Wilson-clover hopping kernels for the DD solver (FP64 and FP32).
+// Wilson-clover hopping kernels for the DD solver (FP64, FP32, and FP16
+// storage with FP32 arithmetic).
 //
 // One templated kernel covers every operator the reference spreads over
 // ddd_in_*, ddd_out_pre/pos_*, jinv_ddd_in_s_ and the SAP update loops:
@@ -13,6 +14,7 @@
 //                 x + (b - D_blk x), static_solver.cc:77-139)
 //        EPI_SAPE out = out + (aux - (src - kappa*acc)) (s_e += in_e - D_blk a_e,
 //                 qws.cc:815-818 with the ddd_in result kept in registers)
+//   T    storage format (float, double, H16); arithmetic in Arith<T>::R.
 // Faces are not packed: a face hop reads the neighbouring block's site of
 // the source field directly from HBM (the whole lattice is resident).
 #include "kernels.h"
@@ -20,8 +22,8 @@
 
 namespace qwsg {
 
-template <typename R, int SEL, int MU, int DIR>
-__device__ __forceinline__ void do_hop(const HopArgs<R>& a, const Site& s, int g, R acc[24]) {
+template <typename T, int SEL, int MU, int DIR, typename R = typename Arith<T>::R>
+__device__ __forceinline__ void do_hop(const HopArgs<T>& a, const Site& s, int g, R acc[24]) {
   const bool face = DIR > 0 ? (s.lc[MU] == a.G.B[MU] - 1) : (s.lc[MU] == 0);
   if (face) {
     if (!(SEL & HOP_OUTER)) return;
@@ -38,12 +40,12 @@ __device__ __forceinline__ void do_hop(const HopArgs<R>& a, const Site& s, int g
   }
   R v[24];
   if (MU == 3)
-    IO<R>::load_half(a.src, a.G.pad, gn, DIR > 0, v);
+    IO<T>::load_half(a.src, a.G.pad, gn, DIR > 0, v);
   else
-    IO<R>::load_spinor(a.src, a.G.pad, gn, v);
+    IO<T>::load_spinor(a.src, a.G.pad, gn, v);
   R h[12], r[12], u[18];
   project<R, MU, DIR>(v, h);
-  IO<R>::load_link(a.U, a.G.pad, MU, DIR > 0 ? g : gn, u);
+  IO<T>::load_link(a.U, a.G.pad, MU, DIR > 0 ? g : gn, u);
   if (DIR > 0)
     link_mul<R, false>(u, h, r);
   else
@@ -56,11 +58,12 @@ __device__ __forceinline__ void do_hop(const HopArgs<R>& a, const Site& s, int g
   reconstruct<R, MU, DIR>(r, acc, f);
 }
 
-template <typename R, int SEL, int EPI>
-__global__ void __launch_bounds__(128) k_hop(const HopArgs<R> a) {
+template <typename T, int SEL, int EPI>
+__global__ void __launch_bounds__(128) k_hop(const HopArgs<T> a) {
+  using R = typename Arith<T>::R;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.nsites) return;
-  const int g = a.site0 + i;
+  const int g = a.list ? __ldg(a.list + i) : a.site0 + i;
   Site s;
   decode_site(a.G, g, s);
   if (a.dom >= 0 && (s.bc[0] & 1) != a.dom) return;
@@ -73,52 +76,52 @@ __global__ void __launch_bounds__(128) k_hop(const HopArgs<R> a) {
   R acc[24];
 #pragma unroll
   for (int j = 0; j < 24; j++) acc[j] = 0;
-  do_hop<R, SEL, 0, +1>(a, s, g, acc);
-  do_hop<R, SEL, 0, -1>(a, s, g, acc);
-  do_hop<R, SEL, 1, +1>(a, s, g, acc);
-  do_hop<R, SEL, 1, -1>(a, s, g, acc);
-  do_hop<R, SEL, 2, +1>(a, s, g, acc);
-  do_hop<R, SEL, 2, -1>(a, s, g, acc);
-  do_hop<R, SEL, 3, +1>(a, s, g, acc);
-  do_hop<R, SEL, 3, -1>(a, s, g, acc);
-  clover_apply<R>(a.C, a.G.pad, g, acc);
+  do_hop<T, SEL, 0, +1>(a, s, g, acc);
+  do_hop<T, SEL, 0, -1>(a, s, g, acc);
+  do_hop<T, SEL, 1, +1>(a, s, g, acc);
+  do_hop<T, SEL, 1, -1>(a, s, g, acc);
+  do_hop<T, SEL, 2, +1>(a, s, g, acc);
+  do_hop<T, SEL, 2, -1>(a, s, g, acc);
+  do_hop<T, SEL, 3, +1>(a, s, g, acc);
+  do_hop<T, SEL, 3, -1>(a, s, g, acc);
+  clover_apply<T>(a.C, a.G.pad, g, acc);
   R o[24];
   if (EPI == EPI_D) {
-    IO<R>::load_spinor(a.src, a.G.pad, g, o);
+    IO<T>::load_spinor(a.src, a.G.pad, g, o);
 #pragma unroll
     for (int j = 0; j < 24; j++) o[j] = o[j] + a.coef * acc[j];
   } else if (EPI == EPI_ADD) {
-    IO<R>::load_spinor(a.out, a.G.pad, g, o);
+    IO<T>::load_spinor(a.out, a.G.pad, g, o);
 #pragma unroll
     for (int j = 0; j < 24; j++) o[j] = o[j] + a.coef * acc[j];
   } else if (EPI == EPI_JINV) {
-    IO<R>::load_spinor(a.aux, a.G.pad, g, o);
+    IO<T>::load_spinor(a.aux, a.G.pad, g, o);
 #pragma unroll
     for (int j = 0; j < 24; j++) o[j] = o[j] + a.coef * acc[j];
   } else {  // EPI_SAPE: coef = -kappa
     R in[24], av[24];
-    IO<R>::load_spinor(a.out, a.G.pad, g, o);
-    IO<R>::load_spinor(a.aux, a.G.pad, g, in);
-    IO<R>::load_spinor(a.src, a.G.pad, g, av);
+    IO<T>::load_spinor(a.out, a.G.pad, g, o);
+    IO<T>::load_spinor(a.aux, a.G.pad, g, in);
+    IO<T>::load_spinor(a.src, a.G.pad, g, av);
 #pragma unroll
     for (int j = 0; j < 24; j++) o[j] = o[j] + (in[j] - (av[j] + a.coef * acc[j]));
   }
-  IO<R>::store_spinor(a.out, a.G.pad, g, o);
+  IO<T>::store_spinor(a.out, a.G.pad, g, o);
 }
 
-template <typename R, int SEL, int EPI>
-static void launch(const HopArgs<R>& a, cudaStream_t st) {
+template <typename T, int SEL, int EPI>
+static void launch(const HopArgs<T>& a, cudaStream_t st) {
   if (a.nsites <= 0) return;
   const int threads = 128;
   const int blocks = (a.nsites + threads - 1) / threads;
-  k_hop<R, SEL, EPI><<<blocks, threads, 0, st>>>(a);
+  k_hop<T, SEL, EPI><<<blocks, threads, 0, st>>>(a);
 }
 
-template <typename R>
-void launch_hop(int sel, int epi, const HopArgs<R>& a, cudaStream_t st) {
+template <typename T>
+void launch_hop(int sel, int epi, const HopArgs<T>& a, cudaStream_t st) {
 #define QWSG_CASE(S, E)              \
   if (sel == S && epi == E) {        \
-    launch<R, S, E>(a, st);          \
+    launch<T, S, E>(a, st);          \
     return;                          \
   }
   QWSG_CASE(HOP_ALL, EPI_D)
@@ -131,5 +134,6 @@ void launch_hop(int sel, int epi, const HopArgs<R>& a, cudaStream_t st) {
 
 template void launch_hop<float>(int, int, const HopArgs<float>&, cudaStream_t);
 template void launch_hop<double>(int, int, const HopArgs<double>&, cudaStream_t);
+template void launch_hop<H16>(int, int, const HopArgs<H16>&, cudaStream_t);
 
 }  // namespace qwsg

@@ -9,23 +9,50 @@ namespace qwsg {
 enum { HOP_INNER = 1, HOP_OUTER = 2, HOP_ALL = 3 };
 enum { EPI_D = 0, EPI_ADD = 1, EPI_JINV = 2, EPI_SAPE = 3 };
 
-template <typename R>
+// T: storage tag (float, double, H16 = FP16 storage / FP32 arithmetic)
+template <typename T>
 struct HopArgs {
+  using S = typename Store<T>::type;
   Geom G;
-  const R* src;   // field the hops read
-  const R* aux;   // b (EPI_JINV) or the SAP right-hand side `in` (EPI_SAPE)
-  R* out;
-  const R* U;     // gauge planes
-  const R* C;     // clover planes
-  R coef;
+  const S* src;   // field the hops read
+  const S* aux;   // b (EPI_JINV) or the SAP right-hand side `in` (EPI_SAPE)
+  S* out;
+  const S* U;     // gauge planes
+  const S* C;     // clover planes
+  typename Arith<T>::R coef;
+  const int* list;  // if set: thread i handles site list[i], else site0 + i
   int site0;      // first site (DD order) handled
-  int nsites;     // number of consecutive sites handled
+  int nsites;     // number of sites handled
   int dom;        // >= 0: only sites whose block has ibx % 2 == dom
   int zero_col;   // >= 0: face hops landing on this colour contribute zero
 };
 
 template <typename R>
 void launch_hop(int sel, int epi, const HopArgs<R>& a, cudaStream_t st);
+
+// even-odd (site parity) hopping, eo.cu
+template <typename T>
+struct EoArgs {
+  using S = typename Store<T>::type;
+  Geom G;
+  const S* src;
+  const S* in0;
+  S* out;
+  const S* U;
+  const S* C;
+  typename Arith<T>::R coef;
+  int pe;      // parity of the output sites
+  int box[4];  // the rank's local extents (inside / face classification)
+};
+template <typename T>
+void launch_eo(int which, int dag, int clov, int mode, const EoArgs<T>& a, cudaStream_t st);
+template <typename T>
+void launch_clv(const EoArgs<T>& a, cudaStream_t st);
+// dst = src on the sites of parity pe, 0 elsewhere
+template <typename T>
+void parity_select(const Geom& G, typename Store<T>::type* dst, const typename Store<T>::type* src,
+                   int pe, cudaStream_t st);
+[[noreturn]] void throw_unsupported_eo();
 
 // ---------------------------------------------------------------------------
 // BLAS-1 on spinor planes (complex per-site vectors of 12 components).
@@ -63,6 +90,13 @@ void blas_bicg_p(const Geom& G, R* p, const R* r, const R* q, double br, double 
 template <typename R>
 void blas_bicg_init(const Geom& G, const R* b, const R* q, R* r, R* p, R* r0, double* res,
                     RedBuf& rb, cudaStream_t st);
+// FP32 planes <-> FP16 planes with per-site scales (IO<H16> format)
+void spinor_s2h(const Geom& G, __half* dst, const float* src, cudaStream_t st);
+void spinor_h2s(const Geom& G, float* dst, const __half* src, cudaStream_t st);
+void spinor_h2h(const Geom& G, __half* dst, const __half* src, cudaStream_t st);
+// FP16 copies of the FP32 gauge (9 complex planes per mu) and clover planes
+void fields_s2h(const Geom& G, __half* Uh, const float* Us, __half* Ch, const float* Cs,
+                cudaStream_t st);
 // y = (float)(x * s)   /   y = (double)x * s
 void blas_d2s(const Geom& G, float* y, const double* x, double s, cudaStream_t st);
 void blas_s2d(const Geom& G, double* y, const float* x, double s, cudaStream_t st);
@@ -77,10 +111,23 @@ void qws_to_planes_spinor(const Geom& G, R* dst, const R* qws, int vlen, int sit
 template <typename R>
 void planes_to_qws_spinor(const Geom& G, R* qws, const R* src, int vlen, int site0, int n,
                           cudaStream_t st);
+// eo = true reads the arrays the way the even-odd operators do: parity p of
+// site (x,y,z,t) selects the x-half slot, x/2 the position inside it.
 template <typename R>
-void qws_to_planes_gauge(const Geom& G, R* dst, const R* qws, int vlen, cudaStream_t st);
+void qws_to_planes_gauge(const Geom& G, R* dst, const R* qws, int vlen, cudaStream_t st,
+                         bool eo = false);
 template <typename R>
-void qws_to_planes_clover(const Geom& G, R* dst, const R* qws, int vlen, cudaStream_t st);
+void qws_to_planes_clover(const Geom& G, R* dst, const R* qws, int vlen, cudaStream_t st,
+                          bool eo = false);
+// one-parity half arrays of the even-odd operators (vol elements, x/2 compressed)
+// <-> full planes; the upload zeroes the other parity, the download writes
+// parity p only
+template <typename R>
+void qws_eo_to_planes_spinor(const Geom& G, R* dst, const R* qws_half, int vlen, int p,
+                             cudaStream_t st);
+template <typename R>
+void planes_to_qws_eo_spinor(const Geom& G, R* qws_half, const R* src, int vlen, int p,
+                             cudaStream_t st);
 // natural layout (site = x + Lx*(y + Ly*(z + Lz*t))) <-> device planes
 template <typename R>
 void nat_to_planes_spinor(const Geom& G, R* dst, const R* nat, cudaStream_t st);

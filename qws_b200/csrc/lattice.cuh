@@ -21,6 +21,7 @@
 //   clover  : the reference's packed 2x36 chiral blocks (clover_def.h:88-284);
 //             FP32 18 float4 planes, FP64 36 double2 planes.
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -87,8 +88,35 @@ __device__ __forceinline__ int nbr_across(const Geom& G, const Site& s, int mu, 
 }
 
 // ---------------------------------------------------------------------------
-// plane I/O
+// plane I/O.  A storage tag T selects the in-memory format; arithmetic is in
+// Arith<T>::R.  float / double store what they compute; H16 stores FP16 and
+// computes in FP32:
+//   spinor  6 uint2 planes of 4 halves (plane j = colour j/2, spins
+//           2(j%2), 2(j%2)+1 -- the grouping of the FP32 float4 planes) holding
+//           v / n, followed by one float plane of per-site scales
+//           n = max |v_i| over the 24 reals (QUDA-style per-site norm);
+//   gauge   9 half2 planes per direction (entries of SU(3) are <= 1);
+//   clover  18 uint2 planes (block i = planes 9i .. 9i+8).
 // ---------------------------------------------------------------------------
+struct H16 {};
+
+template <typename T>
+struct Arith {
+  using R = T;
+};
+template <>
+struct Arith<H16> {
+  using R = float;
+};
+template <typename T>
+struct Store {
+  using type = T;
+};
+template <>
+struct Store<H16> {
+  using type = __half;
+};
+
 template <typename R>
 struct IO;
 
@@ -202,6 +230,90 @@ struct IO<double> {
       a[2 * j + 1] = t.y;
     }
   }
+};
+
+template <>
+struct IO<H16> {
+  __device__ __forceinline__ static float scale(const __half* p, int pad, int g) {
+    return __ldg(reinterpret_cast<const float*>(reinterpret_cast<const uint2*>(p) + (size_t)6 * pad) +
+                 g);
+  }
+  __device__ __forceinline__ static void unpack4(uint2 t, float s, float* o) {
+    __half2 a, b;
+    memcpy(&a, &t.x, 4);
+    memcpy(&b, &t.y, 4);
+    float2 fa = __half22float2(a), fb = __half22float2(b);
+    o[0] = fa.x * s;
+    o[1] = fa.y * s;
+    o[2] = fb.x * s;
+    o[3] = fb.y * s;
+  }
+  __device__ __forceinline__ static uint2 pack4(const float* v, float inv) {
+    __half2 a = __floats2half2_rn(v[0] * inv, v[1] * inv);
+    __half2 b = __floats2half2_rn(v[2] * inv, v[3] * inv);
+    uint2 t;
+    memcpy(&t.x, &a, 4);
+    memcpy(&t.y, &b, 4);
+    return t;
+  }
+  __device__ __forceinline__ static void load_spinor(const __half* __restrict__ p, int pad, int g,
+                                                     float v[24]) {
+    const uint2* q = reinterpret_cast<const uint2*>(p);
+    const float s = scale(p, pad, g);
+#pragma unroll
+    for (int j = 0; j < 6; j++) unpack4(__ldg(q + (size_t)j * pad + g), s, v + 4 * j);
+  }
+  __device__ __forceinline__ static void load_half(const __half* __restrict__ p, int pad, int g,
+                                                   int upper, float v[24]) {
+    const uint2* q = reinterpret_cast<const uint2*>(p);
+    const float s = scale(p, pad, g);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      int j = 2 * c + (upper ? 1 : 0);
+      unpack4(__ldg(q + (size_t)j * pad + g), s, v + 4 * j);
+    }
+  }
+  __device__ __forceinline__ static void store_spinor(__half* __restrict__ p, int pad, int g,
+                                                      const float v[24]) {
+    float n = 0;
+#pragma unroll
+    for (int j = 0; j < 24; j++) n = fmaxf(n, fabsf(v[j]));
+    const float inv = n > 0 ? 1.0f / n : 0.0f;
+    uint2* q = reinterpret_cast<uint2*>(p);
+#pragma unroll
+    for (int j = 0; j < 6; j++) q[(size_t)j * pad + g] = pack4(v + 4 * j, inv);
+    reinterpret_cast<float*>(q + (size_t)6 * pad)[g] = n;
+  }
+  __device__ __forceinline__ static void load_link(const __half* __restrict__ U, int pad, int mu,
+                                                   int g, float u[18]) {
+    const __half2* q = reinterpret_cast<const __half2*>(U);
+#pragma unroll
+    for (int e = 0; e < 9; e++) {
+      float2 f = __half22float2(__ldg(q + (size_t)(mu * 9 + e) * pad + g));
+      u[2 * e] = f.x;
+      u[2 * e + 1] = f.y;
+    }
+  }
+  __device__ __forceinline__ static void load_clover_block(const __half* __restrict__ C, int pad,
+                                                           int g, int blk, float a[36]) {
+    const uint2* q = reinterpret_cast<const uint2*>(C);
+#pragma unroll
+    for (int j = 0; j < 9; j++) unpack4(__ldg(q + (size_t)(9 * blk + j) * pad + g), 1.0f, a + 4 * j);
+  }
+};
+
+// bytes each format moves per site (algorithmic traffic accounting)
+template <typename T>
+struct Bytes {
+  static constexpr int spinor = 24 * sizeof(T);
+  static constexpr int links = 72 * sizeof(T);  // 4 directions
+  static constexpr int clover = 72 * sizeof(T);
+};
+template <>
+struct Bytes<H16> {
+  static constexpr int spinor = 48 + 4;
+  static constexpr int links = 72 * 2;
+  static constexpr int clover = 72 * 2;
 };
 
 // ---------------------------------------------------------------------------
@@ -318,8 +430,9 @@ __device__ __forceinline__ void reconstruct(const R r[12], R acc[24], R f) {
 // v <- A^-1 v with the packed chiral clover (clover_def.h:88-284):
 // x0 = (s0+s2, s1+s3), x1 = (s0-s2, s1-s3) per colour (no 1/2), y_i = A_i x_i,
 // s0 = y0+y1, s2 = y0-y1 (colours 0..2), s1/s3 likewise from entries 3..5.
-template <typename R>
-__device__ __forceinline__ void clover_apply(const R* __restrict__ C, int pad, int g, R v[24]) {
+template <typename T, typename R = typename Arith<T>::R>
+__device__ __forceinline__ void clover_apply(const typename Store<T>::type* __restrict__ C, int pad,
+                                             int g, R v[24]) {
   R xr[2][6], xi[2][6];
 #pragma unroll
   for (int c = 0; c < 3; c++) {
@@ -334,7 +447,7 @@ __device__ __forceinline__ void clover_apply(const R* __restrict__ C, int pad, i
 #pragma unroll
   for (int i = 0; i < 2; i++) {
     R a[36];
-    IO<R>::load_clover_block(C, pad, g, i, a);
+    IO<T>::load_clover_block(C, pad, g, i, a);
 #pragma unroll
     for (int j = 0; j < 6; j++) {
       yr[i][j] = a[j] * xr[i][j];

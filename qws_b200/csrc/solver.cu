@@ -1,8 +1,11 @@
 // Host orchestration of the DD solver on the GPU: SAP preconditioner and the
-// two BiCGStab loops.  Follows the reference's algorithms step by step
+// BiCGStab loops.  Follows the reference's algorithms step by step
 // (qws.cc:776-975, static_solver.cc:65-140, bicgstab_precdd_s.cc:85-559,
-// bicgstab_dd_mix.cc:76-388) with its halo/aliasing bookkeeping replaced by
-// fused kernels over the resident lattice.
+// bicgstab_dd_mix.cc:76-388, and the half-precision pair
+// bicgstab_precdd_s_h.cc:83-369 / bicgstab_dd_mix2_hf.cc:88-373) with its
+// halo/aliasing bookkeeping replaced by fused kernels over the resident
+// lattice.  The SAP sweep is written once for every storage format (FP32,
+// FP16 with per-site scales).
 #include <cmath>
 #include <cstring>
 
@@ -14,10 +17,11 @@ namespace {
 
 int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
-template <typename R>
-HopArgs<R> hop_args(Ctx& c, const R* U, const R* C) {
-  HopArgs<R> a{};
-  a.G = c.G;
+template <typename T>
+HopArgs<T> hop_args(const Geom& G, const typename Store<T>::type* U,
+                    const typename Store<T>::type* C) {
+  HopArgs<T> a{};
+  a.G = G;
   a.U = U;
   a.C = C;
   a.dom = -1;
@@ -25,20 +29,25 @@ HopArgs<R> hop_args(Ctx& c, const R* U, const R* C) {
   return a;
 }
 
-// algorithmic reals moved per handled site (sites of the launch range)
-int hop_reals(int sel, int epi) {
-  if (epi == EPI_JINV) return 24 * 3 + 72 + 72;  // src, b, out, links, clover
-  if (epi == EPI_SAPE) return 24 * 4 + 72 + 72;  // a, in, s (r+w), links, clover
-  if (epi == EPI_ADD) return 24 * 3 + 72 + 72;   // out (r+w), one face neighbour, links, clover
-  return 24 * 2 + 72 + 72;                       // in, out, links, clover
+// algorithmic bytes moved per handled site
+template <typename T>
+double hop_bytes(int sel, int epi) {
+  const double sp = Bytes<T>::spinor, lc = Bytes<T>::links + Bytes<T>::clover;
+  if (epi == EPI_JINV) return 3 * sp + lc;  // src, b, out
+  if (epi == EPI_SAPE) return 4 * sp + lc;  // a, in, s (r+w)
+  if (epi == EPI_ADD) return 3 * sp + lc;   // out (r+w), one face neighbour
+  (void)sel;
+  return 2 * sp + lc;                       // in, out
 }
 
-int kind_of(int sel, int epi, int sz) {
-  bool d = sz == 8;
+template <typename T>
+int kind_of(int sel, int epi) {
+  const bool d = sizeof(typename Store<T>::type) == 8;
+  const bool h = sizeof(typename Store<T>::type) == 2;
   if (sel == HOP_ALL) return d ? K_D_F64 : K_D_F32;
-  if (sel == HOP_OUTER) return d ? K_OUT_F64 : K_OUT_F32;
-  if (epi == EPI_JINV) return K_JINV_F32;
-  if (epi == EPI_SAPE) return K_SAPE_F32;
+  if (sel == HOP_OUTER) return h ? K_OUT_F16 : d ? K_OUT_F64 : K_OUT_F32;
+  if (epi == EPI_JINV) return h ? K_JINV_F16 : K_JINV_F32;
+  if (epi == EPI_SAPE) return h ? K_SAPE_F16 : K_SAPE_F32;
   return d ? K_DIN_F64 : K_DIN_F32;
 }
 
@@ -50,21 +59,47 @@ long face_sites_per_colour(const Geom& G) {
   return nblk_c * (G.Vb - inner);
 }
 
-template <typename R>
-void run_hop(Ctx& c, int sel, int epi, const HopArgs<R>& a) {
+template <typename T>
+void run_hop(Ctx& c, int sel, int epi, const HopArgs<T>& a) {
   if (!c.timing) {
-    launch_hop<R>(sel, epi, a, c.st);
+    launch_hop<T>(sel, epi, a, c.st);
     return;
   }
   cudaEvent_t e0 = c.next_event(), e1 = c.next_event();
   QWSG_CUDA(cudaEventRecord(e0, c.st));
-  launch_hop<R>(sel, epi, a, c.st);
+  launch_hop<T>(sel, epi, a, c.st);
   QWSG_CUDA(cudaEventRecord(e1, c.st));
   long sites = a.nsites;
-  if (sel == HOP_OUTER) sites = face_sites_per_colour(c.G) * (a.nsites == c.G.V ? 2 : 1);
+  if (sel == HOP_OUTER && !a.list) sites = face_sites_per_colour(c.G) * (a.nsites == c.G.V ? 2 : 1);
   if (a.dom >= 0) sites /= 2;
-  c.recs.push_back({kind_of(sel, epi, (int)sizeof(R)), e0, e1,
-                    (double)sites * hop_reals(sel, epi) * sizeof(R)});
+  c.recs.push_back({kind_of<T>(sel, epi), e0, e1, (double)sites * hop_bytes<T>(sel, epi)});
+}
+
+template <typename T>
+const typename Store<T>::type* gauge_of(Ctx& c);
+template <>
+const float* gauge_of<float>(Ctx& c) { return c.Us; }
+template <>
+const double* gauge_of<double>(Ctx& c) { return c.Ud; }
+template <>
+const __half* gauge_of<H16>(Ctx& c) { return c.Uh; }
+template <typename T>
+const typename Store<T>::type* clover_of(Ctx& c);
+template <>
+const float* clover_of<float>(Ctx& c) { return c.Cs; }
+template <>
+const double* clover_of<double>(Ctx& c) { return c.Cd; }
+template <>
+const __half* clover_of<H16>(Ctx& c) { return c.Ch; }
+
+void site_range(const Ctx& c, int col, int& site0, int& n) {
+  if (col >= 0) {
+    site0 = col * c.G.Vh;
+    n = c.G.Vh;
+  } else {
+    site0 = 0;
+    n = c.G.V;
+  }
 }
 
 }  // namespace
@@ -72,7 +107,8 @@ void run_hop(Ctx& c, int sel, int epi, const HopArgs<R>& a) {
 const char* kernel_kind_name(int k) {
   static const char* n[K_NKIND] = {"dslash_full_f64", "dslash_full_f32", "dslash_block_f64",
                                    "dslash_block_f32", "jinv_step_f32", "sap_update_f32",
-                                   "dslash_face_f64", "dslash_face_f32"};
+                                   "dslash_face_f64", "dslash_face_f32", "jinv_step_f16",
+                                   "sap_update_f16", "dslash_face_f16"};
   return (k >= 0 && k < K_NKIND) ? n[k] : "?";
 }
 
@@ -142,6 +178,10 @@ Ctx::~Ctx() {
   cudaFree(Cd);
   cudaFree(Us);
   cudaFree(Cs);
+  cudaFree(Uh);
+  cudaFree(Ch);
+  cudaFree(face_list[0]);
+  cudaFree(face_list[1]);
   cudaFree(rb.partial);
   cudaFree(rb.counter);
   cudaFree(d_res);
@@ -159,6 +199,16 @@ R* Ctx::alloc_spinor() {
 }
 template float* Ctx::alloc_spinor<float>();
 template double* Ctx::alloc_spinor<double>();
+
+// FP16 spinor: 6 uint2 planes + one float plane of per-site scales
+__half* Ctx::alloc_spinor_h() {
+  void* p = nullptr;
+  const size_t bytes = (size_t)(6 * 8 + 4) * G.pad;
+  QWSG_CUDA(cudaMalloc(&p, bytes));
+  QWSG_CUDA(cudaMemsetAsync(p, 0, bytes, st));
+  owned.push_back(p);
+  return (__half*)p;
+}
 
 void Ctx::ensure_sap() {
   if (!sap_s) {
@@ -191,6 +241,17 @@ void Ctx::ensure_outer() {
     ai_x = alloc_spinor<float>();
   }
 }
+void Ctx::ensure_hp() {
+  ensure_inner();
+  ensure_fields_h();
+  if (!h_s) {
+    h_s = alloc_spinor_h();
+    h_a = alloc_spinor_h();
+    h_t = alloc_spinor_h();
+    h_b = alloc_spinor_h();
+    in_w = alloc_spinor<float>();
+  }
+}
 void Ctx::ensure_fields_d() {
   if (!Ud) {
     QWSG_CUDA(cudaMalloc(&Ud, sizeof(double) * 72 * (size_t)G.pad));
@@ -205,6 +266,21 @@ void Ctx::ensure_fields_s() {
     QWSG_CUDA(cudaMalloc(&Cs, sizeof(float) * 72 * (size_t)G.pad));
     QWSG_CUDA(cudaMemsetAsync(Us, 0, sizeof(float) * 72 * (size_t)G.pad, st));
     QWSG_CUDA(cudaMemsetAsync(Cs, 0, sizeof(float) * 72 * (size_t)G.pad, st));
+  }
+  fields_h_valid = false;  // the FP16 copies follow the FP32 fields
+}
+// FP16 copies of the FP32 gauge and clover planes (made on first use after
+// every load)
+void Ctx::ensure_fields_h() {
+  if (!Us) throw Error(4, "gauge/clover fields not loaded");
+  if (!Uh) {
+    QWSG_CUDA(cudaMalloc(&Uh, sizeof(__half) * 72 * (size_t)G.pad));
+    QWSG_CUDA(cudaMalloc(&Ch, sizeof(__half) * 72 * (size_t)G.pad));
+  }
+  if (!fields_h_valid) {
+    fields_s2h(G, Uh, Us, Ch, Cs, st);
+    check_launch("fields_s2h");
+    fields_h_valid = true;
   }
 }
 
@@ -223,7 +299,7 @@ void Ctx::check_launch(const char* what) {
 // operators
 // ---------------------------------------------------------------------------
 void dslash_full_d(Ctx& c, double* out, const double* in) {
-  auto a = hop_args<double>(c, c.Ud, c.Cd);
+  auto a = hop_args<double>(c.G, c.Ud, c.Cd);
   a.src = in;
   a.out = out;
   a.coef = -c.kappa;
@@ -235,7 +311,7 @@ void dslash_full_d(Ctx& c, double* out, const double* in) {
 }
 
 void dslash_full_s(Ctx& c, float* out, const float* in) {
-  auto a = hop_args<float>(c, c.Us, c.Cs);
+  auto a = hop_args<float>(c.G, c.Us, c.Cs);
   a.src = in;
   a.out = out;
   a.coef = -(float)c.kappa;
@@ -246,31 +322,8 @@ void dslash_full_s(Ctx& c, float* out, const float* in) {
 }
 
 template <typename R>
-static const R* gauge_of(Ctx& c);
-template <>
-const float* gauge_of<float>(Ctx& c) { return c.Us; }
-template <>
-const double* gauge_of<double>(Ctx& c) { return c.Ud; }
-template <typename R>
-static const R* clover_of(Ctx& c);
-template <>
-const float* clover_of<float>(Ctx& c) { return c.Cs; }
-template <>
-const double* clover_of<double>(Ctx& c) { return c.Cd; }
-
-static void site_range(const Ctx& c, int col, int& site0, int& n) {
-  if (col >= 0) {
-    site0 = col * c.G.Vh;
-    n = c.G.Vh;
-  } else {
-    site0 = 0;
-    n = c.G.V;
-  }
-}
-
-template <typename R>
 void dslash_inner(Ctx& c, R* out, const R* in, int col, int dom) {
-  auto a = hop_args<R>(c, gauge_of<R>(c), clover_of<R>(c));
+  auto a = hop_args<R>(c.G, gauge_of<R>(c), clover_of<R>(c));
   a.src = in;
   a.out = out;
   a.coef = (R)(-c.kappa);
@@ -282,65 +335,125 @@ void dslash_inner(Ctx& c, R* out, const R* in, int col, int dom) {
 template void dslash_inner<float>(Ctx&, float*, const float*, int, int);
 template void dslash_inner<double>(Ctx&, double*, const double*, int, int);
 
-template <typename R>
-void dslash_outer(Ctx& c, R* out, const R* in, int col, int dom, double factor, int zero_col) {
-  auto a = hop_args<R>(c, gauge_of<R>(c), clover_of<R>(c));
+// out += factor A^-1 H_face in on the face sites of one colour (or one domain
+// of the reference partition NB = (2,1,1,1), where a domain is a colour)
+template <typename T>
+static void outer_t(Ctx& c, typename Store<T>::type* out, const typename Store<T>::type* in,
+                    int col, int dom, double factor, int zero_col) {
+  auto a = hop_args<T>(c.G, gauge_of<T>(c), clover_of<T>(c));
   a.src = in;
   a.out = out;
-  a.coef = (R)factor;
+  a.coef = (typename Arith<T>::R)factor;
   site_range(c, col, a.site0, a.nsites);
   a.dom = dom;
   a.zero_col = zero_col;
-  run_hop<R>(c, HOP_OUTER, EPI_ADD, a);
+  const bool ref_partition = c.G.NB[0] == 2 && c.G.NB[1] == 1 && c.G.NB[2] == 1 && c.G.NB[3] == 1;
+  const int lc = col >= 0 ? col : (dom >= 0 && ref_partition ? dom : -1);
+  if (lc >= 0) {
+    c.ensure_face_lists();
+    a.list = c.face_list[lc];
+    a.nsites = c.n_face[lc];
+    a.dom = -1;
+  }
+  run_hop<T>(c, HOP_OUTER, EPI_ADD, a);
   c.check_launch("dslash_outer");
+}
+
+template <typename R>
+void dslash_outer(Ctx& c, R* out, const R* in, int col, int dom, double factor, int zero_col) {
+  outer_t<R>(c, out, in, col, dom, factor, zero_col);
 }
 template void dslash_outer<float>(Ctx&, float*, const float*, int, int, double, int);
 template void dslash_outer<double>(Ctx&, double*, const double*, int, int, double, int);
 
+// face-site lists, built once on the host from the block geometry
+void Ctx::ensure_face_lists() {
+  if (face_list[0]) return;
+  std::vector<int> lst[2];
+  for (int g = 0; g < G.V; g++) {
+    int col = g >= G.Vh;
+    int t = (g - col * G.Vh) % G.Vb;
+    bool face = false;
+    for (int mu = 0; mu < 4; mu++) {
+      int l = t % G.B[mu];
+      t /= G.B[mu];
+      face |= (l == 0) || (l == G.B[mu] - 1);
+    }
+    if (face) lst[col].push_back(g);
+  }
+  for (int c2 = 0; c2 < 2; c2++) {
+    n_face[c2] = (int)lst[c2].size();
+    QWSG_CUDA(cudaMalloc(&face_list[c2], sizeof(int) * (lst[c2].size() + 1)));
+    QWSG_CUDA(cudaMemcpy(face_list[c2], lst[c2].data(), sizeof(int) * lst[c2].size(),
+                         cudaMemcpyHostToDevice));
+  }
+}
+
 // jinv_ddd_in_s_: nm Richardson steps x <- b + kappa A^-1 H_blk x from x = b
 // (static_solver.cc:65-140; at least one step, as the reference's first
-// step is unconditional).  Ping-pongs between x and the SAP scratch so the
-// last step lands in x.
-void jinv_s(Ctx& c, float* x, const float* b, int col, int nm) {
-  c.ensure_sap();
+// step is unconditional).  Ping-pongs between x and tmp so the last step
+// lands in x.
+template <typename T>
+static void jinv_t(Ctx& c, typename Store<T>::type* x, const typename Store<T>::type* b, int col,
+                   int nm, typename Store<T>::type* tmp) {
   const int steps = nm < 1 ? 1 : nm;
-  auto a = hop_args<float>(c, c.Us, c.Cs);
+  auto a = hop_args<T>(c.G, gauge_of<T>(c), clover_of<T>(c));
   a.aux = b;
-  a.coef = (float)c.kappa;
+  a.coef = (typename Arith<T>::R)c.kappa;
   site_range(c, col, a.site0, a.nsites);
-  const float* src = b;
+  const typename Store<T>::type* src = b;
   for (int k = 1; k <= steps; k++) {
-    float* dst = ((steps - k) % 2 == 0) ? x : c.sap_t;
+    typename Store<T>::type* dst = ((steps - k) % 2 == 0) ? x : tmp;
     a.src = src;
     a.out = dst;
-    run_hop<float>(c, HOP_INNER, EPI_JINV, a);
+    run_hop<T>(c, HOP_INNER, EPI_JINV, a);
     src = dst;
   }
   c.n_jinv++;
-  c.check_launch("jinv_s");
+  c.check_launch("jinv");
 }
 
-// The alternating SAP sweeps of prec_ddd_s_/prec_s_ (qws.cc:802-841).
+void jinv_s(Ctx& c, float* x, const float* b, int col, int nm) {
+  c.ensure_sap();
+  jinv_t<float>(c, x, b, col, nm, c.sap_t);
+}
+
+// The alternating SAP sweeps of prec_ddd_s_/prec_s_ (qws.cc:802-841) and of
+// the half-precision assign_mult_mSAP_s_h_ (prec_ddd_s_h.h:133-170).
 // With a_c the block solution of colour c and s the running right-hand side:
 //   a_e = J_e(s_e);  s_e += in_e - D_blk,e a_e;  s_o += kappa A^-1 H_face a
 // for (e,o) = (E,O) then (O,E).  The reference's first sweep reads the odd
 // colour's block solution as zero (qws.cc:806-808); zero_col expresses that.
-static void sap_sweeps(Ctx& c, float* s, float* a, const float* in, int nsap, int nm) {
-  const float k = (float)c.kappa;
-  for (int isap = 0; isap < nsap; isap++) {
+template <typename T>
+static void sap_sweeps_t(Ctx& c, typename Store<T>::type* s, typename Store<T>::type* a,
+                         typename Store<T>::type* tmp, const typename Store<T>::type* in,
+                         int nsweep, int nm) {
+  const double k = c.kappa;
+  for (int isap = 0; isap < nsweep; isap++) {
     for (int e = 0; e < 2; e++) {
       const int o = 1 - e;
-      jinv_s(c, a, s, e, nm);
-      auto h = hop_args<float>(c, c.Us, c.Cs);
+      jinv_t<T>(c, a, s, e, nm, tmp);
+      auto h = hop_args<T>(c.G, gauge_of<T>(c), clover_of<T>(c));
       h.src = a;
       h.aux = in;
       h.out = s;
-      h.coef = -k;
+      h.coef = (typename Arith<T>::R)(-k);
       site_range(c, e, h.site0, h.nsites);
-      run_hop<float>(c, HOP_INNER, EPI_SAPE, h);
-      dslash_outer<float>(c, s, a, o, -1, k, (isap == 0 && e == 0) ? 1 : -1);
+      run_hop<T>(c, HOP_INNER, EPI_SAPE, h);
+      outer_t<T>(c, s, a, o, -1, k, (isap == 0 && e == 0) ? 1 : -1);
     }
   }
+}
+
+// the final stage of prec_s_ / assign_mult_mSAP_s_h_ (qws.cc:966-973,
+// prec_ddd_s_h.h:173-186): out_E = J_E(s_E), s_O += kappa A^-1 H_face (out_E, 0),
+// out_O = J_O(s_O)
+template <typename T>
+static void sap_final_t(Ctx& c, typename Store<T>::type* out, typename Store<T>::type* s,
+                        typename Store<T>::type* tmp, int nm) {
+  jinv_t<T>(c, out, s, 0, nm, tmp);
+  outer_t<T>(c, s, out, 1, -1, c.kappa, 1);
+  jinv_t<T>(c, out, s, 1, nm, tmp);
 }
 
 // prec_ddd_s_ (qws.cc:776-926): out = D M_SAP in.  Both of the reference's
@@ -351,10 +464,8 @@ void prec_ddd_s(Ctx& c, float* out, const float* in, int nsap, int nm) {
   c.ensure_sap();
   float *s = c.sap_s, *a = c.sap_a;
   blas_copy<float>(c.G, s, in, 0, c.G.V, c.st);
-  sap_sweeps(c, s, a, in, nsap, nm);
-  jinv_s(c, a, s, 0, nm);
-  dslash_outer<float>(c, s, a, 1, -1, (float)c.kappa, 1);
-  jinv_s(c, a, s, 1, nm);
+  sap_sweeps_t<float>(c, s, a, c.sap_t, in, nsap, nm);
+  sap_final_t<float>(c, a, s, c.sap_t, nm);
   dslash_full_s(c, out, a);
   c.n_prec_ddd++;
 }
@@ -364,11 +475,26 @@ void prec_s(Ctx& c, float* out, const float* in, int nsap, int nm) {
   c.ensure_sap();
   float *s = c.sap_s, *a = c.sap_a;
   blas_copy<float>(c.G, s, in, 0, c.G.V, c.st);
-  sap_sweeps(c, s, a, in, nsap, nm);
-  jinv_s(c, out, s, 0, nm);
-  dslash_outer<float>(c, s, out, 1, -1, (float)c.kappa, 1);
-  jinv_s(c, out, s, 1, nm);
+  sap_sweeps_t<float>(c, s, a, c.sap_t, in, nsap, nm);
+  sap_final_t<float>(c, out, s, c.sap_t, nm);
   c.n_prec_s++;
+}
+
+// assign_mult_mSAP_s_h_ (prec_ddd_s_h.h:63-231) with FP16 storage: the input
+// is stored with per-site scales instead of the reference's one global
+// scale (assign_q_s2h, qws_h.cc:175-207), arithmetic is FP32, and the sweep
+// count is the reference's half-precision one (isap = 1 .. nsap-1).
+void prec_s_h(Ctx& c, float* out, const float* in, int nsap, int nm) {
+  if (nsap > 10 || nm > 10)
+    throw Error(2, "assign_mult_mSAP_s_h_: nsap and nm must be <= 10 (prec_ddd_s_h.h:100-101)");
+  c.ensure_hp();
+  spinor_s2h(c.G, c.h_b, in, c.st);
+  spinor_h2h(c.G, c.h_s, c.h_b, c.st);
+  sap_sweeps_t<H16>(c, c.h_s, c.h_a, c.h_t, c.h_b, nsap - 1, nm);
+  sap_final_t<H16>(c, c.h_a, c.h_s, c.h_t, nm);
+  spinor_h2s(c.G, out, c.h_a, c.st);
+  c.n_prec_s_h++;
+  c.check_launch("prec_s_h");
 }
 
 // bicgstab_precdd_s_ (bicgstab_precdd_s.cc:85-559).  Returns the number of
@@ -424,25 +550,89 @@ int bicgstab_precdd_s(Ctx& c, float* x, const float* b, double tol, int maxiter,
   return done;
 }
 
+// bicgstab_precdd_s_h_ (bicgstab_precdd_s_h.cc:83-369): flexible BiCGStab,
+// w = M p, q = D w, x += alpha w (and likewise for the omega step), with the
+// FP16-storage SAP as M and the FP32 D (assign_mult_wd_s_, prec_ddd_s_h.h:233).
+int bicgstab_precdd_s_h(Ctx& c, float* x, const float* b, double tol, int maxiter, int nsap,
+                        int nm, double* final_rel) {
+  c.ensure_hp();
+  const Geom& G = c.G;
+  float *q = c.in_q, *r = c.in_r, *p = c.in_p, *t = c.in_t, *r0 = c.in_r0, *w = c.in_w;
+  blas_zero<float>(G, x, 0, G.V, c.st);
+  blas_bicg_init<float>(G, b, nullptr, r, p, r0, c.d_res, c.rb, c.st);
+  const double* h = c.fetch(2);
+  const float bnorm = (float)h[0];
+  std::complex<float> rho0(bnorm, 0), rho, beta, omega, alpha, ctmp;
+  float rnorm = bnorm;
+  int done = maxiter;
+  for (int iter = 0; iter < maxiter; iter++) {
+    c.n_inner_iter++;
+    prec_s_h(c, w, p, nsap, nm);
+    dslash_full_s(c, q, w);
+    blas_cdot<float>(G, r0, q, c.d_res, c.rb, c.st);
+    h = c.fetch(2);
+    ctmp = std::complex<float>((float)h[0], (float)h[1]);
+    alpha = rho0 / ctmp;
+    if (std::abs(ctmp) <= 1e-15f) alpha = 0;
+    blas_bicg_update<float>(G, x, r, w, q, alpha.real(), alpha.imag(), nullptr, c.d_res, c.rb,
+                            c.st);
+    rnorm = (float)c.fetch(1)[0];
+    if (std::sqrt(rnorm / bnorm) < tol) {
+      done = iter + 1;
+      break;
+    }
+    prec_s_h(c, w, r, nsap, nm);
+    dslash_full_s(c, t, w);
+    blas_norm_cdot<float>(G, t, r, c.d_res, c.rb, c.st);
+    h = c.fetch(3);
+    const float redu0 = (float)h[0], redu1 = (float)h[1], redu2 = (float)h[2];
+    omega = std::complex<float>(redu1 / redu0, redu2 / redu0);
+    if (redu0 <= 1e-30f) omega = 0;
+    blas_bicg_update<float>(G, x, r, w, t, omega.real(), omega.imag(), r0, c.d_res, c.rb, c.st);
+    h = c.fetch(3);
+    rnorm = (float)h[0];
+    rho = std::complex<float>((float)h[1], (float)h[2]);
+    if (std::sqrt(rnorm / bnorm) < tol) {
+      done = iter + 1;
+      break;
+    }
+    beta = alpha * rho / (rho0 * omega);
+    rho0 = rho;
+    if (std::abs(omega) == 0 || std::abs(rho0) == 0) beta = 0;
+    blas_bicg_p<float>(G, p, r, q, beta.real(), beta.imag(), omega.real(), omega.imag(), c.st);
+  }
+  if (final_rel) *final_rel = std::sqrt((double)rnorm / (double)bnorm);
+  c.check_launch("bicgstab_precdd_s_h");
+  return done;
+}
+
 // approx_inv_dirac_op (bicgstab_dd_mix.cc:76-102) with the renormalising
-// FP64<->FP32 converters (reordering.cc:108-204).
+// FP64<->FP32 converters (reordering.cc:108-204); the half-precision variant
+// (approx_inv_dirac_op_hf, bicgstab_dd_mix2_hf.cc:88-107) has no trailing
+// prec_s_ because its inner solve is flexible.
 static int approx_inv(Ctx& c, double* x, const double* b, double tol_s, int maxiter_s, int nsap,
-                      int nm) {
+                      int nm, bool hf) {
   blas_norm2<double>(c.G, b, c.d_res, c.rb, c.st);
   const double bn = std::sqrt(c.fetch(1)[0]);
   blas_d2s(c.G, c.ai_b, b, 1.0 / bn, c.st);
-  int it = bicgstab_precdd_s(c, c.ai_t, c.ai_b, tol_s, maxiter_s, nsap, nm, nullptr);
-  prec_s(c, c.ai_x, c.ai_t, nsap, nm);
+  int it;
+  if (hf) {
+    it = bicgstab_precdd_s_h(c, c.ai_x, c.ai_b, tol_s, maxiter_s, nsap, nm, nullptr);
+  } else {
+    it = bicgstab_precdd_s(c, c.ai_t, c.ai_b, tol_s, maxiter_s, nsap, nm, nullptr);
+    prec_s(c, c.ai_x, c.ai_t, nsap, nm);
+  }
   blas_s2d(c.G, x, c.ai_x, bn, c.st);
   return it;
 }
 
-// bicgstab_dd_mix_ (bicgstab_dd_mix.cc:105-388): flexible FP64 BiCGStab,
-// iter = 1 .. maxiter-1, two preconditioned inner solves + two D per iteration.
-void bicgstab_dd_mix(Ctx& c, double* x, const double* b, double tol, int maxiter, double tol_s,
-                     int maxiter_s, int nsap, int nm, SolveStats* stats, double* hist,
-                     int hist_len) {
-  c.ensure_outer();
+// The flexible FP64 BiCGStab of bicgstab_dd_mix_ (bicgstab_dd_mix.cc:105-388)
+// and bicgstab_dd_mix2_hf_ (bicgstab_dd_mix2_hf.cc:110-373): two
+// preconditioned inner solves + two D per iteration.  iter runs
+// [iter_begin, iter_end); returns the reference's conviter.
+static int outer_loop(Ctx& c, double* x, const double* b, double tol, int iter_begin, int iter_end,
+                      double tol_s, int maxiter_s, int nsap, int nm, bool hf, long* inner_out,
+                      double* rel_out, double* hist, int hist_len) {
   const Geom& G = c.G;
   double *q = c.out_q, *r = c.out_r, *p = c.out_p, *t = c.out_t, *u = c.out_u, *r0 = c.out_r0;
   dslash_full_d(c, q, x);
@@ -452,9 +642,9 @@ void bicgstab_dd_mix(Ctx& c, double* x, const double* b, double tol, int maxiter
   std::complex<double> rho0(h[1], 0), rho, beta, omega, alpha, ctmp;
   double rnorm = h[1];
   long inner = 0;
-  int iter, nh = 0;
-  for (iter = 1; iter < maxiter; iter++) {
-    inner += approx_inv(c, u, p, tol_s, maxiter_s, nsap, nm);
+  int iter, nh = 0, conv = iter_end;
+  for (iter = iter_begin; iter < iter_end; iter++) {
+    inner += approx_inv(c, u, p, tol_s, maxiter_s, nsap, nm, hf);
     dslash_full_d(c, q, u);
     blas_cdot<double>(G, r0, q, c.d_res, c.rb, c.st);
     h = c.fetch(2);
@@ -465,8 +655,11 @@ void bicgstab_dd_mix(Ctx& c, double* x, const double* b, double tol, int maxiter
                              c.st);
     rnorm = c.fetch(1)[0];
     if (hist && nh < hist_len) hist[nh++] = std::sqrt(rnorm / bnorm);
-    if (std::sqrt(rnorm / bnorm) < tol) break;
-    inner += approx_inv(c, u, r, tol_s, maxiter_s, nsap, nm);
+    if (std::sqrt(rnorm / bnorm) < tol) {
+      conv = iter;
+      break;
+    }
+    inner += approx_inv(c, u, r, tol_s, maxiter_s, nsap, nm, hf);
     dslash_full_d(c, t, u);
     blas_norm_cdot<double>(G, t, r, c.d_res, c.rb, c.st);
     h = c.fetch(3);
@@ -477,16 +670,32 @@ void bicgstab_dd_mix(Ctx& c, double* x, const double* b, double tol, int maxiter
     rnorm = h[0];
     rho = std::complex<double>(h[1], h[2]);
     if (hist && nh < hist_len) hist[nh++] = std::sqrt(rnorm / bnorm);
-    if (std::sqrt(rnorm / bnorm) < tol) break;
+    if (std::sqrt(rnorm / bnorm) < tol) {
+      conv = iter;
+      break;
+    }
     beta = alpha * rho / (rho0 * omega);
     rho0 = rho;
     if (std::abs(omega) == 0 || std::abs(rho0) == 0) beta = 0;
     blas_bicg_p<double>(G, p, r, q, beta.real(), beta.imag(), omega.real(), omega.imag(), c.st);
   }
+  *inner_out += inner;
+  *rel_out = std::sqrt(rnorm / bnorm);
+  return conv;
+}
+
+void bicgstab_dd_mix(Ctx& c, double* x, const double* b, double tol, int maxiter, double tol_s,
+                     int maxiter_s, int nsap, int nm, SolveStats* stats, double* hist,
+                     int hist_len) {
+  c.ensure_outer();
+  long inner = 0;
+  double rel = 0;
+  int conv = outer_loop(c, x, b, tol, 1, maxiter, tol_s, maxiter_s, nsap, nm, false, &inner, &rel,
+                        hist, hist_len);
   if (stats) {
-    stats->outer_iters = iter;
+    stats->outer_iters = conv;
     stats->inner_iters = inner;
-    stats->rel_resid_recursive = std::sqrt(rnorm / bnorm);
+    stats->rel_resid_recursive = rel;
   }
   c.check_launch("bicgstab_dd_mix");
 }
@@ -498,6 +707,36 @@ double true_residual(Ctx& c, const double* x, const double* b) {
   blas_bicg_init<double>(c.G, b, c.out_t, c.out_q, c.out_p, c.out_r0, c.d_res, c.rb, c.st);
   const double* h = c.fetch(2);
   return std::sqrt(h[1] / h[0]);
+}
+
+// bicgstab_dd_mix2_hf_: iter = 0 .. maxiter-1, conviter = the 0-based
+// iteration of convergence.  With reliable > 0, the loop is restarted from
+// the recomputed FP64 true residual (at most `reliable` times) until
+// |b - D x| / |b| < tol: the recursive residual of the flexible outer loop can
+// drift from the true one when the inner solve is low precision.
+void bicgstab_dd_mix2_hf(Ctx& c, double* x, const double* b, double tol, int maxiter,
+                         double tol_s, int maxiter_s, int nsap, int nm, int reliable,
+                         SolveStats* stats) {
+  c.ensure_outer();
+  c.ensure_hp();
+  long inner = 0;
+  double rel = 0, truerel = -1;
+  int conv = 0, total = 0;
+  for (int pass = 0; pass <= reliable; pass++) {
+    conv = outer_loop(c, x, b, tol, 0, maxiter, tol_s, maxiter_s, nsap, nm, true, &inner, &rel,
+                      nullptr, 0);
+    total += (conv < maxiter ? conv + 1 : maxiter);
+    if (reliable <= 0) break;
+    truerel = true_residual(c, x, b);
+    if (truerel < tol) break;
+  }
+  if (stats) {
+    stats->outer_iters = reliable > 0 ? total : conv;
+    stats->inner_iters = inner;
+    stats->rel_resid_recursive = rel;
+    stats->rel_resid_true = truerel;
+  }
+  c.check_launch("bicgstab_dd_mix2_hf");
 }
 
 }  // namespace qwsg

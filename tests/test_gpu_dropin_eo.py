@@ -1,0 +1,241 @@
+"""The drop-in even-odd entry points driven exactly as the reference's main.cc
+drives them (main.cc:584-790: test_double_prec_functions /
+test_single_prec_functions, then bicgstab_vm_ at main.cc:203-230): the DD
+generator's arrays are written into glud/clvd/glus/clvs, the source's first
+half array is read as a parity-0 field, and each printed norm is checked
+against the reference's CASE0 golden output with check.sh's tolerances.
+Also covers the even-odd (BQCD) loaders.
+"""
+import ctypes
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from qwsref import (aligned_empty, check_sh_ok, gen_main_fields, nat_to_qws_clover,
+                    nat_to_qws_gauge, nat_to_qws_spinor)
+
+pytestmark = pytest.mark.gpu
+
+REPO = Path(__file__).resolve().parents[1]
+GOLD = json.loads((REPO / "tests" / "golden" / "case_norms.json").read_text())
+L = (32, 6, 4, 3)
+VLEND, VLENS = 8, 16
+KAPPA = 0.05
+VOLD = 16 // VLEND * 6 * 4 * 3
+VOLS = 16 // VLENS * 6 * 4 * 3
+HALF_D = VOLD * 24 * VLEND  # reals of one half array
+HALF_S = VOLS * 24 * VLENS
+
+
+def golden(name):
+    return dict(GOLD["CASE0"]["norms"])[name]
+
+
+def P(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def I(v):
+    return ctypes.byref(ctypes.c_int(v))
+
+
+def alloc(n, dt):
+    a = aligned_empty(n, dt)
+    a[:] = 0
+    return a
+
+
+@pytest.fixture(scope="module")
+def qws():
+    import qws_b200
+
+    lib = qws_b200.load_library()
+    for fn in ("one_minus_dee_deo_in_vm_", "one_minus_deo_dag_in_vm_", "deo_out_pos_vm_",
+               "deo_dag_out_pos_vm_", "dee_deo_out_pos_vm_", "dee_deo_dag_out_pos_vm_"):
+        getattr(lib, fn).argtypes = [ctypes.c_void_p] * (5 if fn.startswith("one") else 4) + \
+            [ctypes.c_double]
+    for fn in ("one_minus_dee_deo_in_s_", "deo_out_pos_s_", "dee_deo_out_pos_s_"):
+        getattr(lib, fn).argtypes = [ctypes.c_void_p] * (5 if fn.startswith("one") else 4) + \
+            [ctypes.c_float]
+    U, C, S = gen_main_fields(L, (1, 1, 1, 1), 2)
+    npe = (ctypes.c_int * 4)(1, 1, 1, 1)
+    fbc = (ctypes.c_int * 4)(1, 1, 1, -1)
+    bs_ = (ctypes.c_int * 4)(1, 2, 2, 2)
+    assert lib.qwsg_set_host_vlen(VLEND, VLENS) == 0
+    lib.qws_init_(*[I(v) for v in L], npe, fbc, I(0), I(1), bs_)
+    ctypes.c_double.in_dll(lib, "kappa").value = KAPPA
+    ctypes.c_double.in_dll(lib, "mkappa").value = -KAPPA
+    ctypes.c_double.in_dll(lib, "kappa2").value = KAPPA * KAPPA
+    for name, arr in (("glud", nat_to_qws_gauge(U, L, VLEND)),
+                      ("clvd", nat_to_qws_clover(C, L, VLEND)),
+                      ("glus", nat_to_qws_gauge(U, L, VLENS).astype(np.float32)),
+                      ("clvs", nat_to_qws_clover(C, L, VLENS).astype(np.float32))):
+        ctypes.memmove(ctypes.c_void_p.in_dll(lib, name).value, arr.ctypes.data, arr.nbytes)
+    lib.qwsg_mark_fields_dirty()
+    b = alloc(2 * HALF_D, np.float64)
+    b[:] = nat_to_qws_spinor(S[0], L, VLEND)
+    bs = alloc(2 * HALF_S, np.float32)
+    bs[:] = nat_to_qws_spinor(np.asarray(S[1], np.float32), L, VLENS)
+    yield lib, b, bs
+    lib.qws_finalize_()
+
+
+def n2(a, n):
+    a = np.asarray(a[:n], np.float64)
+    return float(np.dot(a, a))
+
+
+def test_double_prec_functions(qws):
+    """main.cc:584-720 in order: (pe, po) = (1, 0) for the parity operators."""
+    lib, inp, _ = qws
+    out = alloc(2 * HALF_D, np.float64)
+    fac = -KAPPA * KAPPA
+    pe, po = I(1), I(0)
+    got = {"input": n2(inp, 2 * HALF_D)}
+
+    def run(name, f):
+        out[:] = 0
+        f()
+        got[name] = n2(out, HALF_D)
+
+    run("deo_in_vm_", lambda: lib.deo_in_vm_(pe, po, P(out), P(inp)))
+    run("dee_deo_in_vm_", lambda: lib.dee_deo_in_vm_(pe, po, P(out), P(inp)))
+    run("deo_dag_in_vm_", lambda: lib.deo_dag_in_vm_(pe, po, P(out), P(inp)))
+    run("dee_deo_dag_in_vm_", lambda: lib.dee_deo_dag_in_vm_(pe, po, P(out), P(inp)))
+    run("one_minus_dee_deo_in_vm_",
+        lambda: lib.one_minus_dee_deo_in_vm_(pe, po, P(out), P(inp), P(inp), fac))
+    run("one_minus_deo_dag_in_vm_",
+        lambda: lib.one_minus_deo_dag_in_vm_(pe, po, P(out), P(inp), P(inp), fac))
+    for nm, pre, pos in (("deo_out_pre|pos_vm_", "deo_out_pre_vm_", "deo_out_pos_vm_"),
+                         ("deo_dag_out_pre|pos_vm_", "deo_dag_out_pre_vm_", "deo_dag_out_pos_vm_"),
+                         ("dee_deo_out_pre|pos_vm_", "deo_out_pre_vm_", "dee_deo_out_pos_vm_"),
+                         ("dee_deo_dag_out_pre|pos_vm_", "deo_dag_out_pre_vm_",
+                          "dee_deo_dag_out_pos_vm_")):
+        run(nm, lambda: (getattr(lib, pre)(pe, po, P(out), P(inp)),
+                         getattr(lib, pos)(pe, po, P(out), P(inp), fac)))
+    out[:] = 0
+    out[:HALF_D] = inp[:HALF_D]
+    lib.clvd_vm_(I(0), P(out))
+    got["clvd_vm_"] = n2(out, HALF_D)
+    run("clvd_vm2_", lambda: lib.clvd_vm2_(I(0), P(out), P(inp)))
+    for nm in ("deo_vm_", "dee_deo_vm_", "deo_dag_vm_", "dee_deo_dag_vm_"):
+        run(nm, lambda: getattr(lib, nm)(pe, po, P(out), P(inp)))
+    for nm in ("one_minus_dee_deo_vm_", "one_minus_deo_dag_vm_"):
+        run(nm, lambda: getattr(lib, nm)(pe, po, P(out), P(inp), P(inp)))
+    for nm in ("mtilde_vm_", "mtilde_dag_vm_", "mtdagmt_vm_"):
+        run(nm, lambda: getattr(lib, nm)(P(out), P(inp)))
+    bad = {k: (v, golden(k)) for k, v in got.items() if not check_sh_ok(k, v, golden(k))}
+    assert not bad, bad
+
+
+def test_single_prec_functions(qws):
+    """main.cc:724-790, the FP32 parity operators."""
+    lib, _, inp = qws
+    out = alloc(2 * HALF_S, np.float32)
+    fac = np.float32(-KAPPA * KAPPA)
+    pe, po = I(1), I(0)
+    got = {"input_s_": n2(inp, 2 * HALF_S)}
+
+    def run(name, f):
+        out[:] = 0
+        f()
+        got[name] = n2(out, HALF_S)
+
+    run("deo_in_s_", lambda: lib.deo_in_s_(pe, po, P(out), P(inp)))
+    run("dee_deo_in_s_", lambda: lib.dee_deo_in_s_(pe, po, P(out), P(inp)))
+    run("one_minus_dee_deo_in_s_",
+        lambda: lib.one_minus_dee_deo_in_s_(pe, po, P(out), P(inp), P(inp), fac))
+    run("deo_out_pre|pos_s_", lambda: (lib.deo_out_pre_s_(pe, po, P(out), P(inp)),
+                                       lib.deo_out_pos_s_(pe, po, P(out), P(inp), fac)))
+    run("dee_deo_out_pre|pos_s_", lambda: (lib.deo_out_pre_s_(pe, po, P(out), P(inp)),
+                                           lib.dee_deo_out_pos_s_(pe, po, P(out), P(inp), fac)))
+    out[:] = 0
+    out[:HALF_S] = inp[:HALF_S]
+    lib.clv_s_(I(0), P(out))
+    got["clv_s_"] = n2(out, HALF_S)
+    run("deo_s_", lambda: lib.deo_s_(pe, po, P(out), P(inp)))
+    run("dee_deo_s_", lambda: lib.dee_deo_s_(pe, po, P(out), P(inp)))
+    run("one_minus_dee_deo_s_", lambda: lib.one_minus_dee_deo_s_(pe, po, P(out), P(inp), P(inp)))
+    run("mtilde_s_", lambda: lib.mtilde_s_(P(out), P(inp)))
+    bad = {k: (v, golden(k)) for k, v in got.items() if not check_sh_ok(k, v, golden(k))}
+    assert not bad, bad
+
+
+def test_bicgstab_vm(qws):
+    """main.cc:203-230: 91 iterations on CASE0, then |b - mtilde x|^2."""
+    lib, b, _ = qws
+    x = alloc(2 * HALF_D, np.float64)
+    r = alloc(2 * HALF_D, np.float64)
+    it = ctypes.c_int(0)
+    lib.bicgstab_vm_(P(x), P(b), ctypes.byref(it), I(100))
+    lib.mtilde_vm_(P(r), P(x))
+    assert it.value == 91
+    vals = {"bnorm^2": n2(b, HALF_D), "rnorm^2": n2(b[:HALF_D] - r[:HALF_D], HALF_D),
+            "xnorm^2": n2(x, HALF_D)}
+    ref = [v for k, v in GOLD["CASE0"]["norms"] if k in vals][:3]
+    for (k, v), rv in zip(vals.items(), ref):
+        assert check_sh_ok(k, v, rv), (k, v, rv)
+
+
+def test_bqcd_loaders_roundtrip(qws):
+    """qws_{load,store}f{d,s}_bqcd_ move the even sites of one half array
+    and invert each other (FP32 through one rounding)."""
+    lib, _, _ = qws
+    rng = np.random.default_rng(3)
+    volh = int(np.prod(L)) // 2
+    src = rng.standard_normal(volh * 24)
+    xd = alloc(2 * HALF_D, np.float64)
+    lib.qws_loadfd_bqcd_(P(xd), P(src))
+    back = np.zeros(volh * 24)
+    lib.qws_storefd_bqcd_(P(back), P(xd))
+    np.testing.assert_array_equal(back, src)
+    xs = alloc(2 * HALF_S, np.float32)
+    lib.qws_loadfs_bqcd_(P(xs), P(src))
+    backs = np.zeros(volh * 24)
+    lib.qws_storefs_bqcd_(P(backs), P(xs))
+    np.testing.assert_array_equal(backs, src.astype(np.float32).astype(np.float64))
+
+
+def test_bqcd_path_both_layouts(qws):
+    """A BQCD-style caller: fields and source through the loaders
+    (qws_bqcd.cc:66-642) instead of direct writes.  The DD loaders feed the
+    DD operator, the even-odd loaders feed mtilde_vm_; both are compared with
+    the oracle on the natural fields.  Runs last: it replaces the fields."""
+    from qwsref import Oracle, bqcd_to_nat_spinor, nat_to_bqcd_clover, nat_to_bqcd_gauge, \
+        nat_to_bqcd_spinor, parity_mask
+
+    lib, _, _ = qws
+    rng = np.random.default_rng(5)
+    U, C, _ = gen_main_fields(L, (1, 1, 1, 1), 1)
+    V = int(np.prod(L))
+    v = rng.standard_normal((V, 24))
+    o = Oracle(L, (2, 1, 1, 1), tbc=-1, kappa=KAPPA)
+    o.set_fields(U, C)
+    u, c = nat_to_bqcd_gauge(U, L), nat_to_bqcd_clover(C, L)
+    e, od = nat_to_bqcd_spinor(v, L)
+    volh, kap = ctypes.c_int(V // 2), ctypes.c_double(KAPPA)
+    # DD layout: D on the whole lattice
+    lib.qws_loadg_dd_(P(u), ctypes.byref(volh), ctypes.byref(kap))
+    lib.qws_loadc_dd_(P(c), ctypes.byref(volh))
+    x, y = alloc(2 * HALF_D, np.float64), alloc(2 * HALF_D, np.float64)
+    lib.qws_loadfd_dd_(P(x), P(e), P(od))
+    lib.ddd_d_(P(y), P(x))
+    oe, oo = np.zeros_like(e), np.zeros_like(od)
+    lib.qws_storefd_dd_(P(oe), P(oo), P(y))
+    got, ref = bqcd_to_nat_spinor(oe, oo, L), o.ddd_d(v)
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-13
+    # even-odd layout: mtilde on the even sites
+    lib.qws_loadg_bqcd_(P(u), ctypes.byref(volh), ctypes.byref(kap))
+    lib.qws_loadc_bqcd_(P(c), ctypes.byref(volh))
+    x[:] = 0
+    lib.qws_loadfd_bqcd_(P(x), P(e))
+    lib.mtilde_vm_(P(y), P(x))
+    oe[:] = 0
+    lib.qws_storefd_bqcd_(P(oe), P(y))
+    m0 = parity_mask(L, 0)
+    ve = v * m0[:, None]
+    ref = o.mtilde(ve)[m0]
+    got = bqcd_to_nat_spinor(oe, np.zeros_like(oe), L)[m0]
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-13

@@ -87,3 +87,79 @@ def test_dd_solve_norms_rank_grid(case):
     for name, val in (("bnorm^2", np.sum(b * b)), ("rnorm^2", np.sum(r * r)),
                       ("xnorm^2", np.sum(x * x))):
         assert check_sh_ok(name, float(val), _golden(g, name))
+
+
+# ---------------------------------------------------------------------------
+# even-odd family (deo_*, mtilde, bicgstab_vm_) on CASE0 (main.cc:584-721)
+# ---------------------------------------------------------------------------
+def _eo_setup():
+    from qwsref import eo_partner, eo_perm, parity_mask
+
+    g = GOLD["CASE0"]
+    L = tuple(g["lloc"])
+    U, C, S = gen_main_fields(L, (1, 1, 1, 1), 2)
+    P, Q = eo_perm(L), eo_partner(L)
+    o = Oracle(L, (2, 1, 1, 1), tbc=-1, kappa=KAPPA)
+    o.set_fields(U[:, P], C[P])
+    return g, o, S[0][P], Q, parity_mask(L, 0), parity_mask(L, 1)
+
+
+def test_eo_operator_norms_case0():
+    g, o, b, Q, m0, m1 = _eo_setup()
+    fac = -KAPPA * KAPPA
+    n2 = lambda a, m: float(np.sum(np.asarray(a, np.float64)[m] ** 2))
+    in0 = b[Q]  # main.cc passes in0 = in: parity-1 outputs read the parity-0 half
+    got = {
+        "deo_in_vm_": n2(o.deo(b, 1, 1, 0, 0, 0), m1),
+        "dee_deo_in_vm_": n2(o.deo(b, 1, 1, 0, 1, 0), m1),
+        "deo_dag_in_vm_": n2(o.deo(b, 1, 1, 1, 0, 0), m1),
+        "dee_deo_dag_in_vm_": n2(o.deo(b, 1, 1, 1, 1, 0), m1),
+        "one_minus_dee_deo_in_vm_": n2(o.deo(b, 1, 1, 0, 1, 2, fac, in0), m1),
+        "one_minus_deo_dag_in_vm_": n2(o.deo(b, 1, 1, 1, 0, 2, fac, in0), m1),
+        "deo_out_pre|pos_vm_": n2(o.deo(b, 1, 2, 0, 0, 1, fac), m1),
+        "deo_dag_out_pre|pos_vm_": n2(o.deo(b, 1, 2, 1, 0, 1, fac), m1),
+        "dee_deo_out_pre|pos_vm_": n2(o.deo(b, 1, 2, 0, 1, 1, fac), m1),
+        "dee_deo_dag_out_pre|pos_vm_": n2(o.deo(b, 1, 2, 1, 1, 1, fac), m1),
+        "clvd_vm_": n2(o.clv(b, 0), m0),
+        "deo_vm_": n2(o.deo(b, 1, 3, 0, 0, 0), m1),
+        "dee_deo_vm_": n2(o.deo(b, 1, 3, 0, 1, 0), m1),
+        "one_minus_dee_deo_vm_": n2(o.deo(b, 1, 3, 0, 1, 2, fac, in0), m1),
+        "deo_dag_vm_": n2(o.deo(b, 1, 3, 1, 0, 0), m1),
+        "dee_deo_dag_vm_": n2(o.deo(b, 1, 3, 1, 1, 0), m1),
+        "one_minus_deo_dag_vm_": n2(o.deo(b, 1, 3, 1, 0, 2, fac, in0), m1),
+        "mtilde_vm_": n2(o.mtilde(b), m0),
+        "mtilde_dag_vm_": n2(o.mtilde(b, True), m0),
+        "mtdagmt_vm_": n2(o.mtilde(o.mtilde(b), True), m0),
+    }
+    bs = b.astype(np.float32)
+    fs = np.float32(fac)
+    tmp = o.deo(bs, 1, 3, 0, 1, 0)  # dee_deo_s_(pco, pce, tmp, in)
+    got.update({
+        "deo_in_s_": n2(o.deo(bs, 1, 1, 0, 0, 0), m1),
+        "dee_deo_in_s_": n2(o.deo(bs, 1, 1, 0, 1, 0), m1),
+        "one_minus_dee_deo_in_s_": n2(o.deo(bs, 1, 1, 0, 1, 2, fs, bs[Q]), m1),
+        "deo_out_pre|pos_s_": n2(o.deo(bs, 1, 2, 0, 0, 1, fs), m1),
+        "dee_deo_out_pre|pos_s_": n2(o.deo(bs, 1, 2, 0, 1, 1, fs), m1),
+        "clv_s_": n2(o.clv(bs, 0), m0),
+        "deo_s_": n2(o.deo(bs, 1, 3, 0, 0, 0), m1),
+        "dee_deo_s_": n2(o.deo(bs, 1, 3, 0, 1, 0), m1),
+        "one_minus_dee_deo_s_": n2(o.deo(bs, 1, 3, 0, 1, 2, fs, bs[Q]), m1),
+        "mtilde_s_": n2(o.deo(tmp, 0, 3, 0, 1, 2, fs, bs), m0),
+    })
+    for name, val in got.items():
+        ref = _golden(g, name)
+        assert check_sh_ok(name, val, ref), (name, val, ref)
+
+
+def test_eo_solve_case0():
+    """bicgstab_vm_ (bicgstab.cc:68): 91 iterations on CASE0 (the golden's
+    timing table counts 91 bicgstab_iter_ calls), then the true residual."""
+    g, o, b, Q, m0, m1 = _eo_setup()
+    be = b * m0[:, None]
+    x, it = o.bicgstab_vm(be, np.zeros_like(b), 100)
+    assert it == 91
+    r = be - o.mtilde(x)
+    n2 = lambda a: float(np.sum(a[m0] ** 2))
+    vals = [v for k, v in g["norms"] if k in ("bnorm^2", "rnorm^2", "xnorm^2")][:3]
+    for name, val, ref in zip(("bnorm^2", "rnorm^2", "xnorm^2"), (n2(be), n2(r), n2(x)), vals):
+        assert check_sh_ok(name, val, ref), (name, val, ref)

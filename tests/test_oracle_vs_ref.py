@@ -84,3 +84,57 @@ def test_mixed_solver(setup):
     xo, stats, _ = o.bicgstab_dd_mix(b, x0, 1e-12, 20, 1e-6, 50, 4, 2)
     assert abs(conv.value - stats[0]) <= 1
     assert rel(r.from_d(xr), xo) < 1e-11
+
+
+def test_bqcd_loaders_match_reference(setup):
+    """The reference's own loaders (qws_bqcd.cc:66-642) on arrays made by
+    qwsref's nat_to_bqcd_* helpers: the DD loaders give the DD layout of the
+    natural fields; the even-odd loaders give the layout whose even-odd
+    reading (eo_perm) is the natural field.  This pins the BQCD-format
+    helpers the drop-in tests feed to this library's loaders."""
+    from qwsref import (eo_perm, nat_to_bqcd_clover, nat_to_bqcd_gauge, nat_to_bqcd_spinor,
+                        nat_to_qws_clover, nat_to_qws_gauge, nat_to_qws_spinor)
+
+    o, r, b = setup
+    U, C, _ = gen_main_fields(L, (1, 1, 1, 1), 2)
+    V = int(np.prod(L))
+    volh = ctypes.c_int(V // 2)
+    kap = ctypes.c_double(KAPPA)
+    u, c = nat_to_bqcd_gauge(U, L), nat_to_bqcd_clover(C, L)
+
+    def glob(name, dt):
+        ct = ctypes.c_double if dt == np.float64 else ctypes.c_float
+        return np.ctypeslib.as_array((ct * (72 * V)).from_address(r._global_ptr(name))).copy()
+
+    def expect(Un, Cn):
+        return {"glud": nat_to_qws_gauge(Un, L, r.vlend), "clvd": nat_to_qws_clover(Cn, L, r.vlend),
+                "glus": nat_to_qws_gauge(Un, L, r.vlens).astype(np.float32),
+                "clvs": nat_to_qws_clover(Cn, L, r.vlens).astype(np.float32)}
+
+    try:
+        r.lib.qws_loadg_dd_(ctypes.c_void_p(u.ctypes.data), ctypes.byref(volh), ctypes.byref(kap))
+        r.lib.qws_loadc_dd_(ctypes.c_void_p(c.ctypes.data), ctypes.byref(volh))
+        for name, want in expect(U, C).items():
+            np.testing.assert_array_equal(glob(name, want.dtype), want, err_msg=name)
+        P = eo_perm(L)
+        Ud, Cd = np.zeros_like(U), np.zeros_like(C)
+        Ud[:, P], Cd[P] = U, C
+        r.lib.qws_loadg_bqcd_(ctypes.c_void_p(u.ctypes.data), ctypes.byref(volh),
+                              ctypes.byref(kap))
+        r.lib.qws_loadc_bqcd_(ctypes.c_void_p(c.ctypes.data), ctypes.byref(volh))
+        for name, want in expect(Ud, Cd).items():
+            np.testing.assert_array_equal(glob(name, want.dtype), want, err_msg=name)
+        # spinors: the DD pair loader, and the even sites into a half array
+        e, od = nat_to_bqcd_spinor(b, L)
+        q = aligned_empty(24 * V, np.float64)
+        r.lib.qws_loadfd_dd_(ctypes.c_void_p(q.ctypes.data), ctypes.c_void_p(e.ctypes.data),
+                             ctypes.c_void_p(od.ctypes.data))
+        np.testing.assert_array_equal(q, nat_to_qws_spinor(b, L, r.vlend))
+        q[:] = 0
+        r.lib.qws_loadfd_bqcd_(ctypes.c_void_p(q.ctypes.data), ctypes.c_void_p(e.ctypes.data))
+        bd = np.zeros_like(b)
+        bd[P] = b
+        np.testing.assert_array_equal(q[:12 * V], nat_to_qws_spinor(bd, L, r.vlend)[:12 * V])
+    finally:
+        r.set_kappa(KAPPA)
+        r.set_fields(U, C)
