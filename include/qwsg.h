@@ -79,6 +79,16 @@ int qwsg_ddd_out_d(qwsg_lattice* lat, double* out, const double* in, int colour,
 int qwsg_ddd_out_s(qwsg_lattice* lat, float* out, const float* in, int colour, double factor);
 /* jinv_ddd_in_s_ (static_solver.cc:141): nm Richardson steps on one colour */
 int qwsg_jinv_s(qwsg_lattice* lat, float* x, const float* b, int colour, int nm);
+/* No counterpart in the reference.  Same computation as qwsg_jinv_s, for
+ * callers that cannot let the library allocate device memory (a fixed,
+ * pre-reserved memory budget, or a loop that must not be stalled by the
+ * device synchronisation an allocation can cause).  The intermediate
+ * Richardson iterate lives in a 32 MiB array compiled into the library,
+ * reserved on every GPU that loads it; lattices whose padded volume exceeds
+ * 349,525 sites are rejected (code 2).  The first call on a device looks up
+ * the array's device address (make it before any stream capture).  All calls
+ * share the array: calls that overlap on the GPU race. */
+int qwsg_jinv_s_noalloc(qwsg_lattice* lat, float* x, const float* b, int colour, int nm);
 /* prec_ddd_s_ (qws.cc:776) out = D M_SAP in ; prec_s_ (qws.cc:929) out = M_SAP in */
 int qwsg_prec_ddd_s(qwsg_lattice* lat, float* out, const float* in, int nsap, int nm);
 int qwsg_prec_s(qwsg_lattice* lat, float* out, const float* in, int nsap, int nm);
