@@ -81,8 +81,12 @@ def main():
     outd = aligned_empty(bd.size, np.float64)
     outs = aligned_empty(bs.size, np.float32)
 
-    def timed(fn, reps=1):
-        fn()  # warm-up (first-touch of the reference's static scratch)
+    warm = set()
+
+    def timed(fn, reps=1, key=None):
+        if key not in warm:  # first-touch of the reference's static scratch
+            fn()
+            warm.add(key)
         t = time.perf_counter()
         for _ in range(reps):
             fn()
@@ -91,14 +95,19 @@ def main():
     tol = ctypes.c_double(-1.0)
     it = ctypes.c_int(0)
     mx = ctypes.c_int(SAMPLE_ITERS)
-    t_iter = timed(lambda: r.call("bicgstab_precdd_s_", outs, bs, ctypes.byref(tol),
-                                  ctypes.byref(it), ctypes.byref(mx), ctypes.byref(nsap),
-                                  ctypes.byref(nm))) / SAMPLE_ITERS
-    t_prec_s = timed(lambda: r.call("prec_s_", outs, bs, ctypes.byref(nsap), ctypes.byref(nm)))
-    t_ddd_d = timed(lambda: r.call("ddd_d_", outd, bd))
     counts = spec["counts"]
-    t_solve = (counts["inner_iters"] * t_iter + counts["n_approx"] * t_prec_s +
-               counts["n_ddd_d"] * t_ddd_d)
+    samples = []
+    # repeats > 1: the first `warmup` samples are discarded by the caller
+    for _ in range(int(spec.get("repeats", 1))):
+        t_iter = timed(lambda: r.call("bicgstab_precdd_s_", outs, bs, ctypes.byref(tol),
+                                      ctypes.byref(it), ctypes.byref(mx), ctypes.byref(nsap),
+                                      ctypes.byref(nm)), key="iter") / SAMPLE_ITERS
+        t_prec_s = timed(lambda: r.call("prec_s_", outs, bs, ctypes.byref(nsap),
+                                        ctypes.byref(nm)), key="prec")
+        t_ddd_d = timed(lambda: r.call("ddd_d_", outd, bd), key="ddd")
+        samples.append(counts["inner_iters"] * t_iter + counts["n_approx"] * t_prec_s +
+                       counts["n_ddd_d"] * t_ddd_d)
+    t_solve = samples[-1]
     threads = int(os.environ.get("OMP_NUM_THREADS", "0") or 0) or len(os.sched_getaffinity(0))
     out = {
         "variant": variant,
@@ -108,6 +117,7 @@ def main():
         "t_ddd_d_s": t_ddd_d,
         "t_solve_s": t_solve,
         "solves_per_s": 1.0 / t_solve,
+        "solves_per_s_samples": [1.0 / t for t in samples],
         "plaquette": plaq,
         "t_fieldgen_s": t_gen,
         "sample": (f"reference {variant} on {threads} threads: bicgstab_precdd_s_ "
