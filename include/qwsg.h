@@ -39,6 +39,9 @@ typedef struct {
 
 const char* qwsg_last_error(void);
 const char* qwsg_version(void);
+/* kernels this library has launched in this process (the kernels of a
+ * replayed CUDA graph included) */
+long qwsg_launch_count(void);
 
 /* lattice handle; tbc = +1 periodic / -1 antiperiodic time boundary
  * (fbc_f[3] of qws_init_, qws.cc:298-310) */
@@ -51,6 +54,23 @@ int qwsg_set_kappa(qwsg_lattice* lat, double kappa);
 int qwsg_geometry(const qwsg_lattice* lat, int* volume, int* pad);
 int qwsg_sync(qwsg_lattice* lat);
 
+/* No counterpart in the reference (it solves one right-hand side per call).
+ * A multi-RHS handle on the gauge field, clover term and kappa of `parent`:
+ * nrhs (a power of two, 1..32) right-hand sides share every operator launch,
+ * each link and clover entry being loaded once for all of them.  Its device
+ * spinor buffers hold 24*pad*nrhs reals; the spinor transfer functions move
+ * nrhs natural-layout spinors stored back to back ([nrhs][volume][24]).  The
+ * DD operators, SAP preconditioners and DD solvers accept it; per-RHS scalars
+ * and convergence, a converged RHS frozen at its single-solve iterate.  The
+ * stats of a solve summarise all RHS (most iterations, largest residuals);
+ * qwsg_batch_stats gives each RHS's.  Fields, kappa and the even-odd family
+ * stay on the parent.  Destroy with qwsg_destroy before the parent. */
+int qwsg_create_batch(qwsg_lattice** out, qwsg_lattice* parent, int nrhs);
+int qwsg_nrhs(const qwsg_lattice* lat, int* nrhs);
+/* per-RHS results of the last multi-RHS solve: stats of the DD solvers,
+ * iteration counts of the inner solvers (either pointer may be NULL) */
+int qwsg_batch_stats(qwsg_lattice* lat, qwsg_solve_stats* per_rhs, int* iters_per_rhs);
+
 /* resident fields, from host natural-layout FP64 arrays; the FP32 copies are
  * casts (as qws_loadg_dd_/qws_loadc_dd_ make them, qws_bqcd.cc:125-382) */
 int qwsg_load_gauge(qwsg_lattice* lat, const double* U);
@@ -58,6 +78,20 @@ int qwsg_load_clover(qwsg_lattice* lat, const double* C);
 /* optional explicit FP32 copies (main.cc writes glus/clvs itself) */
 int qwsg_load_gauge_s(qwsg_lattice* lat, const float* U);
 int qwsg_load_clover_s(qwsg_lattice* lat, const float* C);
+
+/* No counterpart in the reference (QWS loads a clover term built and
+ * inverted by BQCD, qws_bqcd.cc:284-382).  Builds the clover term of the
+ * loaded FP64 gauge field on the GPU for this lattice's kappa: clover-leaf
+ * F_{mu nu}, T = 1 - csw*kappa * sum sigma_{mu nu} F_{mu nu}, and the packed
+ * inverse chiral blocks (the conventions of qwsg_gen_clover); replaces the
+ * FP64 and FP32 clover planes.  Code 2 if a block is singular. */
+int qwsg_build_clover(qwsg_lattice* lat, double csw);
+/* No counterpart in the reference.  A seeded SU(3) gauge field smoothed by
+ * n_smear APE-style steps, generated directly into this lattice's FP64 and
+ * FP32 gauge planes with the host generator's construction and random
+ * streams (qwsg_gen_gauge; equal to rounding); *plaq gets the plaquette. */
+int qwsg_gen_gauge_device(qwsg_lattice* lat, unsigned long long seed, int n_smear, double alpha,
+                          double* plaq);
 
 /* host natural <-> device DD-order planes */
 int qwsg_spinor_to_device_d(qwsg_lattice* lat, double* dev, const double* host);
@@ -101,7 +135,7 @@ int qwsg_bicgstab_precdd_s(qwsg_lattice* lat, float* x, const float* b, double t
  * x holds the initial guess on entry.  stats may be NULL. */
 int qwsg_bicgstab_dd_mix(qwsg_lattice* lat, double* x, const double* b, double tol, int maxiter,
                          double tol_s, int maxiter_s, int nsap, int nm, qwsg_solve_stats* stats);
-/* |b - D x| / |b| in FP64 */
+/* |b - D x| / |b| in FP64 (one value per RHS on a multi-RHS handle) */
 int qwsg_true_residual(qwsg_lattice* lat, const double* x, const double* b, double* rel);
 
 /* ---- precision form: FP16 storage with per-site FP32 scales, FP32
@@ -162,6 +196,10 @@ int qwsg_mtilde_s(qwsg_lattice* lat, float* out, const float* in);
  * solution out; iters = the reference's conviter */
 int qwsg_bicgstab_vm(qwsg_lattice* lat, double* x, const double* b, int maxiter, int* iters);
 
+/* CUDA graphs for the SAP preconditioner's launch sequences (default on):
+ * captured on first use per buffers/nsap/nm/kappa, replayed afterwards; not
+ * used while kernel timing is on or on the legacy default stream */
+int qwsg_set_graphs(qwsg_lattice* lat, int enable);
 /* per-kernel CUDA-event timing on the handle's stream: enable (clears the
  * records) or disable; stats fills, per kernel kind k < *nkind, the number
  * of launches, the summed device milliseconds and the summed algorithmic

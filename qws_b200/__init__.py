@@ -56,6 +56,13 @@ def load_library(path: str | os.PathLike | None = None):
         "qwsg_set_kappa": [vp, c_double],
         "qwsg_geometry": [vp, ip, ip],
         "qwsg_sync": [vp],
+        "qwsg_create_batch": [ctypes.POINTER(vp), vp, c_int],
+        "qwsg_nrhs": [vp, ip],
+        "qwsg_batch_stats": [vp, ctypes.POINTER(SolveStats), ip],
+        "qwsg_build_clover": [vp, c_double],
+        "qwsg_set_graphs": [vp, c_int],
+        "qwsg_gen_gauge_device": [vp, ctypes.c_ulonglong, c_int, c_double,
+                                  ctypes.POINTER(c_double)],
         "qwsg_load_gauge": [vp, dp],
         "qwsg_load_clover": [vp, dp],
         "qwsg_load_gauge_s": [vp, fp],
@@ -104,6 +111,8 @@ def load_library(path: str | os.PathLike | None = None):
         fn = getattr(lib, name)
         fn.argtypes = args
         fn.restype = c_int
+    lib.qwsg_launch_count.restype = ctypes.c_long
+    lib.qwsg_launch_count.argtypes = []
     lib.qwsg_kernel_name.restype = ctypes.c_char_p
     lib.qwsg_kernel_name.argtypes = [c_int]
     _lib = lib
@@ -157,6 +166,11 @@ def gen_source(L, seed=2, kind="gauss", arg=0):
     return S
 
 
+def launch_count():
+    """Kernels the library has launched in this process (graph replays included)."""
+    return load_library().qwsg_launch_count()
+
+
 def _check(rc):
     if rc != 0:
         raise QwsgError(f"qwsg error {rc}: {_lib.qwsg_last_error().decode()}")
@@ -194,8 +208,13 @@ class Lattice:
         V, pad = ctypes.c_int(), ctypes.c_int()
         _check(self.lib.qwsg_geometry(self.h, ctypes.byref(V), ctypes.byref(pad)))
         self.V, self.pad = V.value, pad.value
+        self.nr = 1
         self.set_kappa(kappa)
         self.set_stream(stream if stream is not None else torch.cuda.current_stream())
+
+    def batch(self, nrhs, stream=None):
+        """A multi-RHS handle on this lattice's fields (qwsg_create_batch)."""
+        return BatchLattice(self, nrhs, stream)
 
     def close(self):
         if getattr(self, "h", None):
@@ -231,13 +250,32 @@ class Lattice:
             Cs, p = _host(Cs, np.float32)
             _check(self.lib.qwsg_load_clover_s(self.h, p))
 
+    def load_gauge(self, U):
+        """Gauge field only (natural [4,V,3,3,2] FP64); see build_clover."""
+        U, pu = _host(U, np.float64)
+        assert U.size == 72 * self.V
+        _check(self.lib.qwsg_load_gauge(self.h, pu))
+
+    def gen_gauge_device(self, seed, n_smear=5, alpha=0.36):
+        """Seeded SU(3) + APE gauge field generated on the GPU; returns the plaquette."""
+        p = ctypes.c_double()
+        _check(self.lib.qwsg_gen_gauge_device(self.h, int(seed), int(n_smear), float(alpha),
+                                              ctypes.byref(p)))
+        return p.value
+
+    def build_clover(self, csw):
+        """Clover term of the loaded gauge field for this kappa, built on the GPU."""
+        _check(self.lib.qwsg_build_clover(self.h, float(csw)))
+
     # ---- buffers -----------------------------------------------------------
     def empty(self, dtype="f32"):
         t = self.torch.float32 if dtype in ("f32", np.float32) else self.torch.float64
-        return self.torch.zeros(24 * self.pad, dtype=t, device="cuda")
+        return self.torch.zeros(24 * self.pad * self.nr, dtype=t, device="cuda")
 
     def to_device(self, v, out=None):
+        """Host natural-layout spinor(s) ([V,24], or [nrhs,V,24] on a multi-RHS handle)."""
         v = np.asarray(v)
+        assert v.size == 24 * self.V * self.nr
         if v.dtype == np.float64:
             out = self.empty("f64") if out is None else out
             a, p = _host(v, np.float64)
@@ -250,13 +288,15 @@ class Lattice:
 
     def to_host(self, t, out=None):
         """Device planes -> host natural layout (into `out` if given, e.g. pinned)."""
+        shape = (self.V, 24) if self.nr == 1 else (self.nr, self.V, 24)
+        n = 24 * self.V * self.nr
         if t.dtype == self.torch.float64:
-            a = np.empty((self.V, 24), np.float64) if out is None else out
-            assert a.dtype == np.float64 and a.flags.c_contiguous and a.size == 24 * self.V
+            a = np.empty(shape, np.float64) if out is None else out
+            assert a.dtype == np.float64 and a.flags.c_contiguous and a.size == n
             _check(self.lib.qwsg_spinor_to_host_d(self.h, a.ctypes.data_as(ctypes.c_void_p), _ptr(t)))
         else:
-            a = np.empty((self.V, 24), np.float32) if out is None else out
-            assert a.dtype == np.float32 and a.flags.c_contiguous and a.size == 24 * self.V
+            a = np.empty(shape, np.float32) if out is None else out
+            assert a.dtype == np.float32 and a.flags.c_contiguous and a.size == n
             _check(self.lib.qwsg_spinor_to_host_s(self.h, a.ctypes.data_as(ctypes.c_void_p), _ptr(t)))
         return a
 
@@ -373,9 +413,13 @@ class Lattice:
         return st.as_dict()
 
     def true_residual(self, x, b):
-        r = ctypes.c_double()
-        _check(self.lib.qwsg_true_residual(self.h, _ptr(x), _ptr(b), ctypes.byref(r)))
-        return r.value
+        """|b - D x| / |b| (a list with one value per RHS on a multi-RHS handle)."""
+        r = (ctypes.c_double * self.nr)()
+        _check(self.lib.qwsg_true_residual(self.h, _ptr(x), _ptr(b), r))
+        return r[0] if self.nr == 1 else list(r)
+
+    def set_graphs(self, enable=True):
+        _check(self.lib.qwsg_set_graphs(self.h, 1 if enable else 0))
 
     def kernel_timing(self, enable=True):
         _check(self.lib.qwsg_kernel_timing(self.h, 1 if enable else 0))
@@ -394,3 +438,35 @@ class Lattice:
         v = [ctypes.c_long() for _ in range(5)]
         _check(self.lib.qwsg_counters(self.h, *[ctypes.byref(x) for x in v]))
         return dict(zip(("prec_ddd_s", "prec_s", "jinv", "inner_iters", "ddd_d"), [x.value for x in v]))
+
+
+class BatchLattice(Lattice):
+    """nrhs right-hand sides on the fields and kappa of a parent Lattice
+    (qwsg_create_batch): every operator launch serves all RHS.  Device
+    buffers hold 24*pad*nrhs reals; host spinors are [nrhs, V, 24]."""
+
+    def __init__(self, parent, nrhs, stream=None):
+        import torch
+        self.torch = torch
+        self.lib = parent.lib
+        self.parent = parent  # keeps the fields' owner alive
+        self.L, self.NB = parent.L, parent.NB
+        h = ctypes.c_void_p()
+        _check(self.lib.qwsg_create_batch(ctypes.byref(h), parent.h, int(nrhs)))
+        self.h = h
+        self.V, self.pad, self.nr = parent.V, parent.pad, int(nrhs)
+        self.kappa = parent.kappa
+        self.set_stream(stream if stream is not None else torch.cuda.current_stream())
+
+    def set_kappa(self, kappa):
+        raise QwsgError("kappa belongs to the parent lattice")
+
+    def load_fields(self, *a, **k):
+        raise QwsgError("fields belong to the parent lattice")
+
+    def batch_stats(self):
+        """Per-RHS stats of the last DD solve and iteration counts of the last inner solve."""
+        st = (SolveStats * self.nr)()
+        it = (ctypes.c_int * self.nr)()
+        _check(self.lib.qwsg_batch_stats(self.h, st, it))
+        return [s.as_dict() for s in st], list(it)

@@ -60,39 +60,46 @@ __device__ __forceinline__ void dd_add(double& hi, double& lo, double bhi, doubl
   lo = e - (hi - s);
 }
 
+// Per-RHS reductions.  The grid stride is a multiple of nr, so every thread
+// only ever sees RHS r = (thread index) & (nr-1), and lanes l, l+nr, ... of a
+// warp share one RHS: shuffles at offsets 16 .. nr leave the warp's sums in
+// lanes 0..nr-1.  Block partials go to partial[(block*32 + r)*4 + k]; the last
+// block to finish sums every (r, k) over the blocks in block order in
+// double-double and writes res[r*4 + k].
 template <int NR>
-__device__ void finish_reduction(const double (&v)[8], RedBuf rb, double* res) {
-  __shared__ double sh[kThreads / 32][NR > 0 ? NR : 1];
+__device__ void finish_reduction(const double (&v)[8], int nr, RedBuf rb, double* res) {
+  __shared__ double sh[kThreads / 32][32][NR > 0 ? NR : 1];
   __shared__ bool last;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int k = 0; k < NR; k++) {
     double x = v[k];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-    if (lane == 0) sh[warp][k] = x;
+    for (int o = 16; o >= nr; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane < nr) sh[warp][lane][k] = x;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < nr) {
 #pragma unroll
     for (int k = 0; k < NR; k++) {
       double x = 0;
-      for (int w = 0; w < kThreads / 32; w++) x += sh[w][k];
-      rb.partial[blockIdx.x * 8 + k] = x;
+      for (int w = 0; w < kThreads / 32; w++) x += sh[w][threadIdx.x][k];
+      rb.partial[((size_t)blockIdx.x * 32 + threadIdx.x) * 4 + k] = x;
     }
     __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
     unsigned done = atomicAdd(rb.counter, 1u);
     last = (done == gridDim.x - 1);
   }
   __syncthreads();
   if (!last) return;
   __threadfence();
-  // last block: compensated sum of the partials in block order
-#pragma unroll
-  for (int k = 0; k < NR; k++) {
+  for (int pr = warp; pr < nr * NR; pr += kThreads / 32) {
+    const int r = pr / NR, k = pr - r * NR;
     double hi = 0, lo = 0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += kThreads) {
-      double x = *((volatile double*)&rb.partial[b * 8 + k]);
+    for (int b = lane; b < (int)gridDim.x; b += 32) {
+      double x = *((volatile double*)&rb.partial[((size_t)b * 32 + r) * 4 + k]);
       dd_add(hi, lo, x, 0.0);
     }
 #pragma unroll
@@ -101,40 +108,39 @@ __device__ void finish_reduction(const double (&v)[8], RedBuf rb, double* res) {
       double l2 = __shfl_down_sync(0xffffffffu, lo, o);
       dd_add(hi, lo, h2, l2);
     }
-    __shared__ double shh[kThreads / 32], shl[kThreads / 32];
-    if (lane == 0) {
-      shh[warp] = hi;
-      shl[warp] = lo;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double H = 0, Lo = 0;
-      for (int w = 0; w < kThreads / 32; w++) dd_add(H, Lo, shh[w], shl[w]);
-      res[k] = H + Lo;
-    }
-    __syncthreads();
+    if (lane == 0) res[r * 4 + k] = hi + lo;
   }
+  __syncthreads();
   if (threadIdx.x == 0) *rb.counter = 0;
 }
 
+// a per-RHS scalar: cf[r*4 + k] when a table is given, else the value
+template <typename R>
+__device__ __forceinline__ R coef(const double* cf, int r, int k, R v) {
+  return cf ? (R)cf[r * 4 + k] : v;
+}
+
 // ---- per-site operations ---------------------------------------------------
+// every (site, rhs) entry; op(G, entry, rhs, acc)
 template <typename R, int NR, typename Op>
 __global__ void __launch_bounds__(kThreads) k_sites(Geom G, Op op, RedBuf rb, double* res) {
   double acc[8];
 #pragma unroll
   for (int k = 0; k < 8; k++) acc[k] = 0;
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G.V; g += gridDim.x * blockDim.x)
-    op(G, g, acc);
-  if constexpr (NR > 0) finish_reduction<NR>(acc, rb, res);
+  const int n = G.V << G.lgnr;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
+    op(G, e, e & (G.nr - 1), acc);
+  if constexpr (NR > 0) finish_reduction<NR>(acc, G.nr, rb, res);
 }
 
 template <typename R>
 struct OpNorm2 {
   const R* x;
-  __device__ void operator()(const Geom& G, int g, double* acc) const {
+  __device__ void operator()(const Geom& G, int g, int rhs, double* acc) const {
+    const int sp = spad(G);
 #pragma unroll
     for (int j = 0; j < 6; j++) {
-      V4<R> a = ld4(x, G.pad, g, j);
+      V4<R> a = ld4(x, sp, g, j);
       acc[0] += (double)a.x * a.x + (double)a.y * a.y + (double)a.z * a.z + (double)a.w * a.w;
     }
   }
@@ -143,10 +149,11 @@ struct OpNorm2 {
 template <typename R>
 struct OpCdot {
   const R *x, *y;
-  __device__ void operator()(const Geom& G, int g, double* acc) const {
+  __device__ void operator()(const Geom& G, int g, int rhs, double* acc) const {
+    const int sp = spad(G);
 #pragma unroll
     for (int j = 0; j < 6; j++) {
-      V4<R> a = ld4(x, G.pad, g, j), b = ld4(y, G.pad, g, j);
+      V4<R> a = ld4(x, sp, g, j), b = ld4(y, sp, g, j);
       acc[0] += (double)a.x * b.x + (double)a.y * b.y + (double)a.z * b.z + (double)a.w * b.w;
       acc[1] += (double)a.x * b.y - (double)a.y * b.x + (double)a.z * b.w - (double)a.w * b.z;
     }
@@ -156,10 +163,11 @@ struct OpCdot {
 template <typename R>
 struct OpNormCdot {  // |y|^2, <y, x>
   const R *y, *x;
-  __device__ void operator()(const Geom& G, int g, double* acc) const {
+  __device__ void operator()(const Geom& G, int g, int rhs, double* acc) const {
+    const int sp = spad(G);
 #pragma unroll
     for (int j = 0; j < 6; j++) {
-      V4<R> a = ld4(y, G.pad, g, j), b = ld4(x, G.pad, g, j);
+      V4<R> a = ld4(y, sp, g, j), b = ld4(x, sp, g, j);
       acc[0] += (double)a.x * a.x + (double)a.y * a.y + (double)a.z * a.z + (double)a.w * a.w;
       acc[1] += (double)a.x * b.x + (double)a.y * b.y + (double)a.z * b.z + (double)a.w * b.w;
       acc[2] += (double)a.x * b.y - (double)a.y * b.x + (double)a.z * b.w - (double)a.w * b.z;
@@ -172,12 +180,15 @@ template <typename R>
 struct OpBicgUpdate {
   R *x, *r;
   const R *p, *q, *r0;
-  R ar, ai;
-  __device__ void operator()(const Geom& G, int g, double* acc) const {
+  R ar_, ai_;
+  const double* cf;  // per-RHS (ar, ai) when set
+  __device__ void operator()(const Geom& G, int g, int rhs, double* acc) const {
+    const int sp = spad(G);
+    const R ar = coef(cf, rhs, 0, ar_), ai = coef(cf, rhs, 1, ai_);
 #pragma unroll
     for (int j = 0; j < 6; j++) {
-      V4<R> X = ld4<R>(x, G.pad, g, j), Rr = ld4<R>(r, G.pad, g, j);
-      V4<R> P = ld4(p, G.pad, g, j), Q = ld4(q, G.pad, g, j);
+      V4<R> X = ld4<R>(x, sp, g, j), Rr = ld4<R>(r, sp, g, j);
+      V4<R> P = ld4(p, sp, g, j), Q = ld4(q, sp, g, j);
       X.x = X.x + ar * P.x - ai * P.y;
       X.y = X.y + ar * P.y + ai * P.x;
       X.z = X.z + ar * P.z - ai * P.w;
@@ -186,12 +197,12 @@ struct OpBicgUpdate {
       Rr.y = Rr.y - ar * Q.y - ai * Q.x;
       Rr.z = Rr.z - ar * Q.z + ai * Q.w;
       Rr.w = Rr.w - ar * Q.w - ai * Q.z;
-      st4<R>(x, G.pad, g, j, X);
-      st4<R>(r, G.pad, g, j, Rr);
+      st4<R>(x, sp, g, j, X);
+      st4<R>(r, sp, g, j, Rr);
       acc[0] += (double)Rr.x * Rr.x + (double)Rr.y * Rr.y + (double)Rr.z * Rr.z +
                 (double)Rr.w * Rr.w;
       if (r0) {
-        V4<R> A = ld4(r0, G.pad, g, j);
+        V4<R> A = ld4(r0, sp, g, j);
         acc[1] += (double)A.x * Rr.x + (double)A.y * Rr.y + (double)A.z * Rr.z + (double)A.w * Rr.w;
         acc[2] += (double)A.x * Rr.y - (double)A.y * Rr.x + (double)A.z * Rr.w - (double)A.w * Rr.z;
       }
@@ -204,18 +215,22 @@ template <typename R>
 struct OpBicgP {
   R* p;
   const R *r, *q;
-  R br, bi, wr, wi;
-  __device__ void operator()(const Geom& G, int g, double*) const {
+  R br_, bi_, wr_, wi_;
+  const double* cf;  // per-RHS (br, bi, wr, wi) when set
+  __device__ void operator()(const Geom& G, int g, int rhs, double*) const {
+    const int sp = spad(G);
+    const R br = coef(cf, rhs, 0, br_), bi = coef(cf, rhs, 1, bi_);
+    const R wr = coef(cf, rhs, 2, wr_), wi = coef(cf, rhs, 3, wi_);
 #pragma unroll
     for (int j = 0; j < 6; j++) {
-      V4<R> P = ld4<R>(p, G.pad, g, j), Rr = ld4(r, G.pad, g, j), Q = ld4(q, G.pad, g, j);
+      V4<R> P = ld4<R>(p, sp, g, j), Rr = ld4(r, sp, g, j), Q = ld4(q, sp, g, j);
       R c0 = P.x - wr * Q.x + wi * Q.y, c1 = P.y - wr * Q.y - wi * Q.x;
       R c2 = P.z - wr * Q.z + wi * Q.w, c3 = P.w - wr * Q.w - wi * Q.z;
       P.x = br * c0 - bi * c1 + Rr.x;
       P.y = br * c1 + bi * c0 + Rr.y;
       P.z = br * c2 - bi * c3 + Rr.z;
       P.w = br * c3 + bi * c2 + Rr.w;
-      st4<R>(p, G.pad, g, j, P);
+      st4<R>(p, sp, g, j, P);
     }
   }
 };
@@ -225,18 +240,19 @@ template <typename R>
 struct OpBicgInit {
   const R *b, *q;
   R *r, *p, *r0;
-  __device__ void operator()(const Geom& G, int g, double* acc) const {
+  __device__ void operator()(const Geom& G, int g, int rhs, double* acc) const {
+    const int sp = spad(G);
 #pragma unroll
     for (int j = 0; j < 6; j++) {
-      V4<R> B = ld4(b, G.pad, g, j), Q;
+      V4<R> B = ld4(b, sp, g, j), Q;
       if (q)
-        Q = ld4(q, G.pad, g, j);
+        Q = ld4(q, sp, g, j);
       else
         Q = {0, 0, 0, 0};
       V4<R> Rr = {B.x - Q.x, B.y - Q.y, B.z - Q.z, B.w - Q.w};
-      st4<R>(r, G.pad, g, j, Rr);
-      st4<R>(p, G.pad, g, j, Rr);
-      st4<R>(r0, G.pad, g, j, Rr);
+      st4<R>(r, sp, g, j, Rr);
+      st4<R>(p, sp, g, j, Rr);
+      st4<R>(r0, sp, g, j, Rr);
       acc[0] += (double)B.x * B.x + (double)B.y * B.y + (double)B.z * B.z + (double)B.w * B.w;
       acc[1] += (double)Rr.x * Rr.x + (double)Rr.y * Rr.y + (double)Rr.z * Rr.z +
                 (double)Rr.w * Rr.w;
@@ -247,12 +263,15 @@ struct OpBicgInit {
 struct OpD2S {
   float* y;
   const double* x;
-  double s;
-  __device__ void operator()(const Geom& G, int g, double*) const {
+  double s_;
+  const double* cf;  // per-RHS scale when set
+  __device__ void operator()(const Geom& G, int g, int rhs, double*) const {
+    const int sp = spad(G);
+    const double s = coef(cf, rhs, 0, s_);
 #pragma unroll
     for (int j = 0; j < 6; j++) {
-      V4<double> a = ld4(x, G.pad, g, j);
-      st4<float>(y, G.pad, g, j,
+      V4<double> a = ld4(x, sp, g, j);
+      st4<float>(y, sp, g, j,
                  {(float)(a.x * s), (float)(a.y * s), (float)(a.z * s), (float)(a.w * s)});
     }
   }
@@ -261,19 +280,22 @@ struct OpD2S {
 struct OpS2D {
   double* y;
   const float* x;
-  double s;
-  __device__ void operator()(const Geom& G, int g, double*) const {
+  double s_;
+  const double* cf;  // per-RHS scale when set
+  __device__ void operator()(const Geom& G, int g, int rhs, double*) const {
+    const int sp = spad(G);
+    const double s = coef(cf, rhs, 0, s_);
 #pragma unroll
     for (int j = 0; j < 6; j++) {
-      V4<float> a = ld4(x, G.pad, g, j);
-      st4<double>(y, G.pad, g, j,
+      V4<float> a = ld4(x, sp, g, j);
+      st4<double>(y, sp, g, j,
                   {(double)a.x * s, (double)a.y * s, (double)a.z * s, (double)a.w * s});
     }
   }
 };
 
 int grid_for(const Geom& G, const RedBuf* rb) {
-  int b = (G.V + kThreads - 1) / kThreads;
+  int b = ((G.V << G.lgnr) + kThreads - 1) / kThreads;
   int cap = rb ? rb->nblk : 148 * 8;
   return b < cap ? b : cap;
 }
@@ -281,35 +303,45 @@ int grid_for(const Geom& G, const RedBuf* rb) {
 template <typename R, int NR, typename Op>
 void run(const Geom& G, Op op, RedBuf* rb, double* res, cudaStream_t st) {
   RedBuf dummy{nullptr, nullptr, 0};
+  count_launch();
   k_sites<R, NR, Op><<<grid_for(G, rb), kThreads, 0, st>>>(G, op, rb ? *rb : dummy, res);
 }
 
+// entries [e0, e0 + n) (all RHS of the sites [site0, site0 + n/nr))
 template <typename R>
-__global__ void k_copy(Geom G, R* y, const R* x, int site0, int n) {
+__global__ void k_copy(Geom G, R* y, const R* x, int e0, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  int g = site0 + i;
+  const int e = e0 + i, sp = spad(G);
 #pragma unroll
-  for (int j = 0; j < 6; j++) st4<R>(y, G.pad, g, j, ld4<R>(x, G.pad, g, j));
+  for (int j = 0; j < 6; j++) st4<R>(y, sp, e, j, ld4<R>(x, sp, e, j));
 }
 template <typename R>
-__global__ void k_zero(Geom G, R* y, int site0, int n) {
+__global__ void k_zero(Geom G, R* y, int e0, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  int g = site0 + i;
+  const int e = e0 + i, sp = spad(G);
 #pragma unroll
-  for (int j = 0; j < 6; j++) st4<R>(y, G.pad, g, j, {0, 0, 0, 0});
+  for (int j = 0; j < 6; j++) st4<R>(y, sp, e, j, {0, 0, 0, 0});
 }
 
 }  // namespace
 
 template <typename R>
 void blas_copy(const Geom& G, R* y, const R* x, int site0, int n, cudaStream_t st) {
-  if (n > 0) k_copy<R><<<(n + 255) / 256, 256, 0, st>>>(G, y, x, site0, n);
+  const int ne = n << G.lgnr;
+  if (ne > 0) {
+    count_launch();
+    k_copy<R><<<(ne + 255) / 256, 256, 0, st>>>(G, y, x, site0 << G.lgnr, ne);
+  }
 }
 template <typename R>
 void blas_zero(const Geom& G, R* y, int site0, int n, cudaStream_t st) {
-  if (n > 0) k_zero<R><<<(n + 255) / 256, 256, 0, st>>>(G, y, site0, n);
+  const int ne = n << G.lgnr;
+  if (ne > 0) {
+    count_launch();
+    k_zero<R><<<(ne + 255) / 256, 256, 0, st>>>(G, y, site0 << G.lgnr, ne);
+  }
 }
 template <typename R>
 void blas_norm2(const Geom& G, const R* x, double* res, RedBuf& rb, cudaStream_t st) {
@@ -326,8 +358,8 @@ void blas_norm_cdot(const Geom& G, const R* y, const R* x, double* res, RedBuf& 
 }
 template <typename R>
 void blas_bicg_update(const Geom& G, R* x, R* r, const R* p, const R* q, double ar, double ai,
-                      const R* r0, double* res, RedBuf& rb, cudaStream_t st) {
-  OpBicgUpdate<R> op{x, r, p, q, r0, (R)ar, (R)ai};
+                      const R* r0, double* res, RedBuf& rb, cudaStream_t st, const double* cf) {
+  OpBicgUpdate<R> op{x, r, p, q, r0, (R)ar, (R)ai, cf};
   if (r0)
     run<R, 3>(G, op, &rb, res, st);
   else
@@ -335,19 +367,21 @@ void blas_bicg_update(const Geom& G, R* x, R* r, const R* p, const R* q, double 
 }
 template <typename R>
 void blas_bicg_p(const Geom& G, R* p, const R* r, const R* q, double br, double bi, double wr,
-                 double wi, cudaStream_t st) {
-  run<R, 0>(G, OpBicgP<R>{p, r, q, (R)br, (R)bi, (R)wr, (R)wi}, nullptr, nullptr, st);
+                 double wi, cudaStream_t st, const double* cf) {
+  run<R, 0>(G, OpBicgP<R>{p, r, q, (R)br, (R)bi, (R)wr, (R)wi, cf}, nullptr, nullptr, st);
 }
 template <typename R>
 void blas_bicg_init(const Geom& G, const R* b, const R* q, R* r, R* p, R* r0, double* res,
                     RedBuf& rb, cudaStream_t st) {
   run<R, 2>(G, OpBicgInit<R>{b, q, r, p, r0}, &rb, res, st);
 }
-void blas_d2s(const Geom& G, float* y, const double* x, double s, cudaStream_t st) {
-  run<float, 0>(G, OpD2S{y, x, s}, nullptr, nullptr, st);
+void blas_d2s(const Geom& G, float* y, const double* x, double s, cudaStream_t st,
+              const double* cf) {
+  run<float, 0>(G, OpD2S{y, x, s, cf}, nullptr, nullptr, st);
 }
-void blas_s2d(const Geom& G, double* y, const float* x, double s, cudaStream_t st) {
-  run<float, 0>(G, OpS2D{y, x, s}, nullptr, nullptr, st);
+void blas_s2d(const Geom& G, double* y, const float* x, double s, cudaStream_t st,
+              const double* cf) {
+  run<float, 0>(G, OpS2D{y, x, s, cf}, nullptr, nullptr, st);
 }
 
 #define QWSG_INST(R)                                                                         \
@@ -358,9 +392,9 @@ void blas_s2d(const Geom& G, double* y, const float* x, double s, cudaStream_t s
   template void blas_norm_cdot<R>(const Geom&, const R*, const R*, double*, RedBuf&,         \
                                   cudaStream_t);                                             \
   template void blas_bicg_update<R>(const Geom&, R*, R*, const R*, const R*, double, double, \
-                                    const R*, double*, RedBuf&, cudaStream_t);               \
+                                    const R*, double*, RedBuf&, cudaStream_t, const double*); \
   template void blas_bicg_p<R>(const Geom&, R*, const R*, const R*, double, double, double,  \
-                               double, cudaStream_t);                                        \
+                               double, cudaStream_t, const double*);                         \
   template void blas_bicg_init<R>(const Geom&, const R*, const R*, R*, R*, R*, double*,      \
                                   RedBuf&, cudaStream_t);
 QWSG_INST(float)

@@ -8,6 +8,7 @@
 
 namespace qwsg {
 
+std::atomic<long> g_kernel_launches{0};
 static thread_local std::string g_last_error;
 
 void set_error(const std::string& m) { g_last_error = m; }
@@ -41,6 +42,17 @@ static void* staging(Ctx& c, size_t n) {
 
 static void check_ctx(qwsg_lattice* l) {
   if (!l || !l->c) throw Error(4, "lattice handle is NULL");
+  if (l->c->parent) l->c->sync_from_parent(false);
+}
+// operations defined for one right-hand side only
+static void single_rhs(qwsg_lattice* l, const char* what) {
+  if (l->c->G.nr != 1)
+    throw Error(1, std::string(what) + ": not available on a multi-RHS handle");
+}
+// fields live on the parent lattice of a multi-RHS handle
+static void not_batch(qwsg_lattice* l, const char* what) {
+  if (l->c->parent)
+    throw Error(1, std::string(what) + ": load fields on the parent lattice of a multi-RHS handle");
 }
 
 template <typename Rin, typename R>
@@ -62,23 +74,46 @@ static void load_clover_t(Ctx& c, R* dst, const Rin* C) {
   QWSG_CUDA(cudaStreamSynchronize(c.st));
 }
 
+// host: G.nr natural-layout spinors back to back ([nr][V][24])
 template <typename R>
 static void sp_to_dev(Ctx& c, R* dev, const R* host) {
-  size_t n = sizeof(R) * 24 * (size_t)c.G.V;
-  void* d = staging(c, n);
-  QWSG_CUDA(cudaMemcpyAsync(d, host, n, cudaMemcpyHostToDevice, c.st));
-  nat_to_planes_spinor<R>(c.G, dev, (const R*)d, c.st);
+  const size_t n = sizeof(R) * 24 * (size_t)c.G.V;
+  R* d = (R*)staging(c, n * c.G.nr);
+  QWSG_CUDA(cudaMemcpyAsync(d, host, n * c.G.nr, cudaMemcpyHostToDevice, c.st));
+  for (int r = 0; r < c.G.nr; r++)
+    nat_to_planes_spinor<R>(c.G, dev, d + (size_t)r * 24 * c.G.V, c.st, r);
   c.check_launch("spinor_to_device");
   QWSG_CUDA(cudaStreamSynchronize(c.st));
 }
 template <typename R>
 static void sp_to_host(Ctx& c, R* host, const R* dev) {
-  size_t n = sizeof(R) * 24 * (size_t)c.G.V;
-  void* d = staging(c, n);
-  planes_to_nat_spinor<R>(c.G, (R*)d, dev, c.st);
+  const size_t n = sizeof(R) * 24 * (size_t)c.G.V;
+  R* d = (R*)staging(c, n * c.G.nr);
+  for (int r = 0; r < c.G.nr; r++)
+    planes_to_nat_spinor<R>(c.G, d + (size_t)r * 24 * c.G.V, dev, c.st, r);
   c.check_launch("spinor_to_host");
-  QWSG_CUDA(cudaMemcpyAsync(host, d, n, cudaMemcpyDeviceToHost, c.st));
+  QWSG_CUDA(cudaMemcpyAsync(host, d, n * c.G.nr, cudaMemcpyDeviceToHost, c.st));
   QWSG_CUDA(cudaStreamSynchronize(c.st));
+}
+
+static void copy_stats(const SolveStats& s, qwsg_solve_stats* st) {
+  st->outer_iters = s.outer_iters;
+  st->inner_iters = s.inner_iters;
+  st->rel_resid_recursive = s.rel_resid_recursive;
+  st->rel_resid_true = s.rel_resid_true;
+}
+// the summary of a multi-RHS solve: the most outer iterations and the largest
+// residuals over the RHS
+static SolveStats worst(const std::vector<SolveStats>& v) {
+  SolveStats w;
+  for (const auto& s : v) {
+    w.outer_iters = s.outer_iters > w.outer_iters ? s.outer_iters : w.outer_iters;
+    w.inner_iters = s.inner_iters;
+    w.rel_resid_recursive =
+        s.rel_resid_recursive > w.rel_resid_recursive ? s.rel_resid_recursive : w.rel_resid_recursive;
+    w.rel_resid_true = s.rel_resid_true > w.rel_resid_true ? s.rel_resid_true : w.rel_resid_true;
+  }
+  return w;
 }
 
 }  // namespace qwsg
@@ -89,12 +124,78 @@ extern "C" {
 
 const char* qwsg_last_error(void) { return g_last_error.c_str(); }
 const char* qwsg_version(void) { return "qws_b200 0.1 (sm_100a)"; }
+long qwsg_launch_count(void) { return g_kernel_launches.load(); }
 
 int qwsg_create(qwsg_lattice** out, const int L[4], const int NB[4], int tbc) {
   return guarded([&] {
     if (!out || !L || !NB) throw Error(1, "qwsg_create: NULL argument");
     if (tbc != 1 && tbc != -1) throw Error(1, "qwsg_create: tbc must be +1 or -1");
     *out = new qwsg_lattice{new Ctx(L, NB, tbc)};
+  });
+}
+
+int qwsg_create_batch(qwsg_lattice** out, qwsg_lattice* parent, int nrhs) {
+  return guarded([&] {
+    if (!out) throw Error(1, "qwsg_create_batch: NULL argument");
+    check_ctx(parent);
+    if (parent->c->parent) throw Error(1, "qwsg_create_batch: the parent must be a lattice");
+    const Geom& G = parent->c->G;
+    auto* c = new Ctx(G.L, G.NB, G.tbc, nrhs);
+    c->owns_fields = false;
+    c->parent = parent->c;
+    try {
+      c->sync_from_parent(false);
+    } catch (...) {
+      delete c;
+      throw;
+    }
+    *out = new qwsg_lattice{c};
+  });
+}
+
+int qwsg_nrhs(const qwsg_lattice* l, int* nrhs) {
+  return guarded([&] {
+    if (!l || !l->c) throw Error(4, "lattice handle is NULL");
+    if (nrhs) *nrhs = l->c->G.nr;
+  });
+}
+
+int qwsg_batch_stats(qwsg_lattice* l, qwsg_solve_stats* per_rhs, int* iters_per_rhs) {
+  return guarded([&] {
+    if (!l || !l->c) throw Error(4, "lattice handle is NULL");
+    Ctx& c = *l->c;
+    for (int r = 0; r < c.G.nr; r++) {
+      if (per_rhs && r < (int)c.last_stats.size()) copy_stats(c.last_stats[r], per_rhs + r);
+      if (iters_per_rhs && r < (int)c.last_iters.size()) iters_per_rhs[r] = c.last_iters[r];
+    }
+  });
+}
+
+int qwsg_build_clover(qwsg_lattice* l, double csw) {
+  return guarded([&] {
+    check_ctx(l);
+    not_batch(l, "qwsg_build_clover");
+    build_clover(*l->c, csw);
+  });
+}
+
+int qwsg_gen_gauge_device(qwsg_lattice* l, unsigned long long seed, int n_smear, double alpha,
+                          double* plaq) {
+  return guarded([&] {
+    check_ctx(l);
+    not_batch(l, "qwsg_gen_gauge_device");
+    double p = gen_gauge_device(*l->c, seed, n_smear, alpha);
+    if (plaq) *plaq = p;
+  });
+}
+
+int qwsg_set_graphs(qwsg_lattice* l, int enable) {
+  return guarded([&] {
+    check_ctx(l);
+    Ctx& c = *l->c;
+    QWSG_CUDA(cudaStreamSynchronize(c.st));
+    c.use_graphs = enable != 0;
+    if (!c.use_graphs) c.clear_graphs();
   });
 }
 
@@ -120,6 +221,7 @@ int qwsg_set_stream(qwsg_lattice* l, void* stream) {
 int qwsg_set_kappa(qwsg_lattice* l, double kappa) {
   return guarded([&] {
     check_ctx(l);
+    not_batch(l, "qwsg_set_kappa");
     l->c->kappa = kappa;
   });
 }
@@ -142,6 +244,7 @@ int qwsg_sync(qwsg_lattice* l) {
 int qwsg_load_gauge(qwsg_lattice* l, const double* U) {
   return guarded([&] {
     check_ctx(l);
+    not_batch(l, "qwsg_load_gauge");
     Ctx& c = *l->c;
     c.ensure_fields_d();
     c.ensure_fields_s();
@@ -152,6 +255,7 @@ int qwsg_load_gauge(qwsg_lattice* l, const double* U) {
 int qwsg_load_clover(qwsg_lattice* l, const double* C) {
   return guarded([&] {
     check_ctx(l);
+    not_batch(l, "qwsg_load_clover");
     Ctx& c = *l->c;
     c.ensure_fields_d();
     c.ensure_fields_s();
@@ -162,6 +266,7 @@ int qwsg_load_clover(qwsg_lattice* l, const double* C) {
 int qwsg_load_gauge_s(qwsg_lattice* l, const float* U) {
   return guarded([&] {
     check_ctx(l);
+    not_batch(l, "qwsg_load_gauge_s");
     Ctx& c = *l->c;
     c.ensure_fields_s();
     load_gauge_t<float, float>(c, c.Us, U);
@@ -170,6 +275,7 @@ int qwsg_load_gauge_s(qwsg_lattice* l, const float* U) {
 int qwsg_load_clover_s(qwsg_lattice* l, const float* C) {
   return guarded([&] {
     check_ctx(l);
+    not_batch(l, "qwsg_load_clover_s");
     Ctx& c = *l->c;
     c.ensure_fields_s();
     load_clover_t<float, float>(c, c.Cs, C);
@@ -278,7 +384,15 @@ int qwsg_bicgstab_precdd_s(qwsg_lattice* l, float* x, const float* b, double tol
   return guarded([&] {
     check_ctx(l);
     need_fields(*l->c, false);
-    int it = bicgstab_precdd_s(*l->c, x, b, tol, maxiter, nsap, nm, final_rel);
+    Ctx& c = *l->c;
+    int it;
+    if (c.G.nr > 1) {
+      c.last_iters.assign(c.G.nr, 0);
+      it = bicgstab_precdd_s_mrhs(c, x, b, tol, maxiter, nsap, nm, c.last_iters.data());
+      if (final_rel) *final_rel = -1;
+    } else {
+      it = bicgstab_precdd_s(c, x, b, tol, maxiter, nsap, nm, final_rel);
+    }
     if (iters) *iters = it;
   });
 }
@@ -288,14 +402,17 @@ int qwsg_bicgstab_dd_mix(qwsg_lattice* l, double* x, const double* b, double tol
     check_ctx(l);
     need_fields(*l->c, true);
     need_fields(*l->c, false);
+    Ctx& c = *l->c;
     SolveStats s;
-    bicgstab_dd_mix(*l->c, x, b, tol, maxiter, tol_s, maxiter_s, nsap, nm, &s, nullptr, 0);
-    if (st) {
-      st->outer_iters = s.outer_iters;
-      st->inner_iters = s.inner_iters;
-      st->rel_resid_recursive = s.rel_resid_recursive;
-      st->rel_resid_true = s.rel_resid_true;
+    if (c.G.nr > 1) {
+      c.last_stats.assign(c.G.nr, SolveStats{});
+      bicgstab_dd_mix_mrhs(c, x, b, tol, maxiter, tol_s, maxiter_s, nsap, nm,
+                           c.last_stats.data());
+      s = worst(c.last_stats);
+    } else {
+      bicgstab_dd_mix(c, x, b, tol, maxiter, tol_s, maxiter_s, nsap, nm, &s, nullptr, 0);
     }
+    if (st) copy_stats(s, st);
   });
 }
 int qwsg_prec_s_h(qwsg_lattice* l, float* out, const float* in, int nsap, int nm) {
@@ -310,7 +427,15 @@ int qwsg_bicgstab_precdd_s_h(qwsg_lattice* l, float* x, const float* b, double t
   return guarded([&] {
     check_ctx(l);
     need_fields(*l->c, false);
-    int it = bicgstab_precdd_s_h(*l->c, x, b, tol, maxiter, nsap, nm, final_rel);
+    Ctx& c = *l->c;
+    int it;
+    if (c.G.nr > 1) {
+      c.last_iters.assign(c.G.nr, 0);
+      it = bicgstab_precdd_s_h_mrhs(c, x, b, tol, maxiter, nsap, nm, c.last_iters.data());
+      if (final_rel) *final_rel = -1;
+    } else {
+      it = bicgstab_precdd_s_h(c, x, b, tol, maxiter, nsap, nm, final_rel);
+    }
     if (iters) *iters = it;
   });
 }
@@ -321,19 +446,23 @@ int qwsg_bicgstab_dd_mix2_hf(qwsg_lattice* l, double* x, const double* b, double
     check_ctx(l);
     need_fields(*l->c, true);
     need_fields(*l->c, false);
+    Ctx& c = *l->c;
     SolveStats s;
-    bicgstab_dd_mix2_hf(*l->c, x, b, tol, maxiter, tol_s, maxiter_s, nsap, nm, reliable, &s);
-    if (st) {
-      st->outer_iters = s.outer_iters;
-      st->inner_iters = s.inner_iters;
-      st->rel_resid_recursive = s.rel_resid_recursive;
-      st->rel_resid_true = s.rel_resid_true;
+    if (c.G.nr > 1) {
+      c.last_stats.assign(c.G.nr, SolveStats{});
+      bicgstab_dd_mix2_hf_mrhs(c, x, b, tol, maxiter, tol_s, maxiter_s, nsap, nm, reliable,
+                               c.last_stats.data());
+      s = worst(c.last_stats);
+    } else {
+      bicgstab_dd_mix2_hf(c, x, b, tol, maxiter, tol_s, maxiter_s, nsap, nm, reliable, &s);
     }
+    if (st) copy_stats(s, st);
   });
 }
 int qwsg_set_parities(qwsg_lattice* l, int pce, int pco) {
   return guarded([&] {
     check_ctx(l);
+    single_rhs(l, "qwsg_set_parities");
     if (pce < 0 || pce > 1 || pco != 1 - pce) throw Error(1, "parities must be (0,1) or (1,0)");
     l->c->pce = pce;
     l->c->pco = pco;
@@ -343,6 +472,7 @@ int qwsg_deo_d(qwsg_lattice* l, double* out, const double* in, int pe, int which
                int clov, int mode, double factor, const double* in0) {
   return guarded([&] {
     check_ctx(l);
+    single_rhs(l, "qwsg_deo_d");
     deo<double>(*l->c, out, in, pe, which, dag, clov, mode, factor, in0);
   });
 }
@@ -350,24 +480,28 @@ int qwsg_deo_s(qwsg_lattice* l, float* out, const float* in, int pe, int which, 
                int mode, double factor, const float* in0) {
   return guarded([&] {
     check_ctx(l);
+    single_rhs(l, "qwsg_deo_s");
     deo<float>(*l->c, out, in, pe, which, dag, clov, mode, factor, in0);
   });
 }
 int qwsg_clv_d(qwsg_lattice* l, double* out, const double* in, int pe) {
   return guarded([&] {
     check_ctx(l);
+    single_rhs(l, "qwsg_clv_d");
     clv<double>(*l->c, out, in, pe);
   });
 }
 int qwsg_clv_s(qwsg_lattice* l, float* out, const float* in, int pe) {
   return guarded([&] {
     check_ctx(l);
+    single_rhs(l, "qwsg_clv_s");
     clv<float>(*l->c, out, in, pe);
   });
 }
 int qwsg_mtilde_d(qwsg_lattice* l, double* out, const double* in) {
   return guarded([&] {
     check_ctx(l);
+    single_rhs(l, "qwsg_mtilde_d");
     need_fields(*l->c, true);
     mtilde_d(*l->c, out, in);
   });
@@ -375,6 +509,7 @@ int qwsg_mtilde_d(qwsg_lattice* l, double* out, const double* in) {
 int qwsg_mtilde_dag_d(qwsg_lattice* l, double* out, const double* in) {
   return guarded([&] {
     check_ctx(l);
+    single_rhs(l, "qwsg_mtilde_dag_d");
     need_fields(*l->c, true);
     mtilde_dag_d(*l->c, out, in);
   });
@@ -382,6 +517,7 @@ int qwsg_mtilde_dag_d(qwsg_lattice* l, double* out, const double* in) {
 int qwsg_mtilde_s(qwsg_lattice* l, float* out, const float* in) {
   return guarded([&] {
     check_ctx(l);
+    single_rhs(l, "qwsg_mtilde_s");
     need_fields(*l->c, false);
     mtilde_s(*l->c, out, in);
   });
@@ -389,6 +525,7 @@ int qwsg_mtilde_s(qwsg_lattice* l, float* out, const float* in) {
 int qwsg_bicgstab_vm(qwsg_lattice* l, double* x, const double* b, int maxiter, int* iters) {
   return guarded([&] {
     check_ctx(l);
+    single_rhs(l, "qwsg_bicgstab_vm");
     need_fields(*l->c, true);
     int it = bicgstab_vm(*l->c, x, b, maxiter);
     if (iters) *iters = it;
@@ -398,8 +535,14 @@ int qwsg_true_residual(qwsg_lattice* l, const double* x, const double* b, double
   return guarded([&] {
     check_ctx(l);
     need_fields(*l->c, true);
-    double r = true_residual(*l->c, x, b);
-    if (rel) *rel = r;
+    Ctx& c = *l->c;
+    if (c.G.nr > 1) {  // rel holds one value per RHS
+      if (!rel) throw Error(1, "qwsg_true_residual: rel must hold one value per RHS");
+      true_residual_mrhs(c, x, b, rel);
+    } else {
+      double r = true_residual(c, x, b);
+      if (rel) *rel = r;
+    }
   });
 }
 int qwsg_kernel_timing(qwsg_lattice* l, int enable) {

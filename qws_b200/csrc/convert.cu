@@ -195,7 +195,7 @@ __global__ void k_qws2pl_clover(Geom G, R* dst, const R* __restrict__ q, int vle
 }
 
 template <typename R>
-__global__ void k_nat2pl_sp(Geom G, R* dst, const R* __restrict__ nat) {
+__global__ void k_nat2pl_sp(Geom G, R* dst, const R* __restrict__ nat, int rhs) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= G.V) return;
   int x[4];
@@ -204,18 +204,18 @@ __global__ void k_nat2pl_sp(Geom G, R* dst, const R* __restrict__ nat) {
   R v[24];
 #pragma unroll
   for (int r = 0; r < 24; r++) v[r] = nat[n * 24 + r];
-  store_sp(dst, G.pad, g, v);
+  store_sp(dst, spad(G), sentry(G, g, rhs), v);
 }
 
 template <typename R>
-__global__ void k_pl2nat_sp(Geom G, R* nat, const R* __restrict__ src) {
+__global__ void k_pl2nat_sp(Geom G, R* nat, const R* __restrict__ src, int rhs) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= G.V) return;
   int x[4];
   global_coords(G, g, x);
   long n = nat_index(G, x);
   R v[24];
-  IO<R>::load_spinor(src, G.pad, g, v);
+  IO<R>::load_spinor(src, spad(G), sentry(G, g, rhs), v);
 #pragma unroll
   for (int r = 0; r < 24; r++) nat[n * 24 + r] = v[r];
 }
@@ -250,31 +250,34 @@ __global__ void k_nat2pl_clover(Geom G, R* dst, const Rin* __restrict__ nat) {
 
 inline int nb(long n) { return (int)((n + 127) / 128); }
 
+// spinor precision conversions: one thread per (site, rhs) entry
 __global__ void k_s2h(Geom G, __half* dst, const float* __restrict__ src) {
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= G.V) return;
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (G.V << G.lgnr)) return;
+  const int sp = spad(G);
   float v[24];
-  IO<float>::load_spinor(src, G.pad, g, v);
-  IO<H16>::store_spinor(dst, G.pad, g, v);
+  IO<float>::load_spinor(src, sp, e, v);
+  IO<H16>::store_spinor(dst, sp, e, v);
 }
 
 __global__ void k_h2s(Geom G, float* dst, const __half* __restrict__ src) {
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= G.V) return;
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (G.V << G.lgnr)) return;
+  const int sp = spad(G);
   float v[24];
-  IO<H16>::load_spinor(src, G.pad, g, v);
-  IO<float>::store_spinor(dst, G.pad, g, v);
+  IO<H16>::load_spinor(src, sp, e, v);
+  IO<float>::store_spinor(dst, sp, e, v);
 }
 
 __global__ void k_h2h(Geom G, __half* dst, const __half* __restrict__ src) {
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= G.V) return;
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (G.V << G.lgnr)) return;
+  const size_t sp = spad(G);
   const uint2* s = reinterpret_cast<const uint2*>(src);
   uint2* d = reinterpret_cast<uint2*>(dst);
 #pragma unroll
-  for (int j = 0; j < 6; j++) d[(size_t)j * G.pad + g] = s[(size_t)j * G.pad + g];
-  reinterpret_cast<float*>(d + (size_t)6 * G.pad)[g] =
-      reinterpret_cast<const float*>(s + (size_t)6 * G.pad)[g];
+  for (int j = 0; j < 6; j++) d[j * sp + e] = s[j * sp + e];
+  reinterpret_cast<float*>(d + 6 * sp)[e] = reinterpret_cast<const float*>(s + 6 * sp)[e];
 }
 
 __global__ void k_fields_s2h(Geom G, __half* Uh, const float* __restrict__ Us, __half* Ch,
@@ -296,61 +299,79 @@ __global__ void k_fields_s2h(Geom G, __half* Uh, const float* __restrict__ Us, _
 }  // namespace
 
 void spinor_s2h(const Geom& G, __half* dst, const float* src, cudaStream_t st) {
-  k_s2h<<<nb(G.V), 128, 0, st>>>(G, dst, src);
+  count_launch();
+  k_s2h<<<nb(G.V << G.lgnr), 128, 0, st>>>(G, dst, src);
 }
 void spinor_h2s(const Geom& G, float* dst, const __half* src, cudaStream_t st) {
-  k_h2s<<<nb(G.V), 128, 0, st>>>(G, dst, src);
+  count_launch();
+  k_h2s<<<nb(G.V << G.lgnr), 128, 0, st>>>(G, dst, src);
 }
 void spinor_h2h(const Geom& G, __half* dst, const __half* src, cudaStream_t st) {
-  k_h2h<<<nb(G.V), 128, 0, st>>>(G, dst, src);
+  count_launch();
+  k_h2h<<<nb(G.V << G.lgnr), 128, 0, st>>>(G, dst, src);
 }
 void fields_s2h(const Geom& G, __half* Uh, const float* Us, __half* Ch, const float* Cs,
                 cudaStream_t st) {
+  count_launch();
   k_fields_s2h<<<nb(G.V), 128, 0, st>>>(G, Uh, Us, Ch, Cs);
 }
 
 template <typename R>
 void qws_to_planes_spinor(const Geom& G, R* dst, const R* qws, int vlen, int site0, int n,
                           cudaStream_t st) {
-  if (n > 0) k_qws2pl_sp<R><<<nb(n), 128, 0, st>>>(G, dst, qws, vlen, site0, n);
+  if (n > 0) {
+    count_launch();
+    k_qws2pl_sp<R><<<nb(n), 128, 0, st>>>(G, dst, qws, vlen, site0, n);
+  }
 }
 template <typename R>
 void planes_to_qws_spinor(const Geom& G, R* qws, const R* src, int vlen, int site0, int n,
                           cudaStream_t st) {
-  if (n > 0) k_pl2qws_sp<R><<<nb(n), 128, 0, st>>>(G, qws, src, vlen, site0, n);
+  if (n > 0) {
+    count_launch();
+    k_pl2qws_sp<R><<<nb(n), 128, 0, st>>>(G, qws, src, vlen, site0, n);
+  }
 }
 template <typename R>
 void qws_eo_to_planes_spinor(const Geom& G, R* dst, const R* qws_half, int vlen, int p,
                              cudaStream_t st) {
+  count_launch();
   k_qwseo2pl_sp<R><<<nb(G.V), 128, 0, st>>>(G, dst, qws_half, vlen, p);
 }
 template <typename R>
 void planes_to_qws_eo_spinor(const Geom& G, R* qws_half, const R* src, int vlen, int p,
                              cudaStream_t st) {
+  count_launch();
   k_pl2qwseo_sp<R><<<nb(G.V), 128, 0, st>>>(G, qws_half, src, vlen, p);
 }
 template <typename R>
 void qws_to_planes_gauge(const Geom& G, R* dst, const R* qws, int vlen, cudaStream_t st, bool eo) {
+  count_launch();
   k_qws2pl_gauge<R><<<nb(G.V), 128, 0, st>>>(G, dst, qws, vlen, eo ? 1 : 0);
 }
 template <typename R>
 void qws_to_planes_clover(const Geom& G, R* dst, const R* qws, int vlen, cudaStream_t st, bool eo) {
+  count_launch();
   k_qws2pl_clover<R><<<nb(G.V), 128, 0, st>>>(G, dst, qws, vlen, eo ? 1 : 0);
 }
 template <typename R>
-void nat_to_planes_spinor(const Geom& G, R* dst, const R* nat, cudaStream_t st) {
-  k_nat2pl_sp<R><<<nb(G.V), 128, 0, st>>>(G, dst, nat);
+void nat_to_planes_spinor(const Geom& G, R* dst, const R* nat, cudaStream_t st, int rhs) {
+  count_launch();
+  k_nat2pl_sp<R><<<nb(G.V), 128, 0, st>>>(G, dst, nat, rhs);
 }
 template <typename R>
-void planes_to_nat_spinor(const Geom& G, R* nat, const R* src, cudaStream_t st) {
-  k_pl2nat_sp<R><<<nb(G.V), 128, 0, st>>>(G, nat, src);
+void planes_to_nat_spinor(const Geom& G, R* nat, const R* src, cudaStream_t st, int rhs) {
+  count_launch();
+  k_pl2nat_sp<R><<<nb(G.V), 128, 0, st>>>(G, nat, src, rhs);
 }
 template <typename Rin, typename R>
 void nat_to_planes_gauge(const Geom& G, R* dst, const Rin* nat, cudaStream_t st) {
+  count_launch();
   k_nat2pl_gauge<Rin, R><<<nb(G.V), 128, 0, st>>>(G, dst, nat);
 }
 template <typename Rin, typename R>
 void nat_to_planes_clover(const Geom& G, R* dst, const Rin* nat, cudaStream_t st) {
+  count_launch();
   k_nat2pl_clover<Rin, R><<<nb(G.V), 128, 0, st>>>(G, dst, nat);
 }
 
@@ -361,8 +382,8 @@ void nat_to_planes_clover(const Geom& G, R* dst, const Rin* nat, cudaStream_t st
   template void planes_to_qws_eo_spinor<R>(const Geom&, R*, const R*, int, int, cudaStream_t);   \
   template void qws_to_planes_gauge<R>(const Geom&, R*, const R*, int, cudaStream_t, bool);      \
   template void qws_to_planes_clover<R>(const Geom&, R*, const R*, int, cudaStream_t, bool);     \
-  template void nat_to_planes_spinor<R>(const Geom&, R*, const R*, cudaStream_t);                \
-  template void planes_to_nat_spinor<R>(const Geom&, R*, const R*, cudaStream_t);
+  template void nat_to_planes_spinor<R>(const Geom&, R*, const R*, cudaStream_t, int);           \
+  template void planes_to_nat_spinor<R>(const Geom&, R*, const R*, cudaStream_t, int);
 QWSG_INST(float)
 QWSG_INST(double)
 #undef QWSG_INST

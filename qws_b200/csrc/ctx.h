@@ -35,6 +35,14 @@ struct Ctx {
   double kappa = 0;
   cudaStream_t st = nullptr;
   bool own_stream = false;
+  // a multi-RHS context borrows the gauge/clover planes of its parent
+  // lattice (same fields, same geometry) and owns only its spinor buffers
+  bool owns_fields = true;
+  Ctx* parent = nullptr;
+  // refresh the borrowed field pointers and kappa from the parent (the FP16
+  // copies too when `half`), before every batched call
+  void sync_from_parent(bool half);
+  cudaEvent_t parent_ev = nullptr;
   int device = 0;
 
   // resident fields (device planes)
@@ -89,10 +97,15 @@ struct Ctx {
   // counters (calls of each reference-named region)
   long n_prec_ddd = 0, n_prec_s = 0, n_jinv = 0, n_dslash_d = 0, n_inner_iter = 0;
 
-  Ctx(const int L[4], const int NB[4], int tbc);
+  // nrhs: right-hand sides per spinor field (power of two, 1..32)
+  Ctx(const int L[4], const int NB[4], int tbc, int nrhs = 1);
   ~Ctx();
 
-  size_t spinor_elems() const { return (size_t)24 * G.pad; }
+  size_t spinor_elems() const { return (size_t)24 * spad(G); }
+  static constexpr int kMaxRhs = 32;
+  // per-RHS statistics of the last multi-RHS solve
+  std::vector<SolveStats> last_stats;
+  std::vector<int> last_iters;
   template <typename R>
   R* alloc_spinor();
   void ensure_sap();
@@ -101,7 +114,15 @@ struct Ctx {
   void ensure_fields_d();
   void ensure_fields_s();
   // synchronous read of n reduction results
+  // the first n reduction results (res[4*rhs + k]: use 4*nr for all RHS)
   const double* fetch(int n);
+  // per-RHS scalar table (4 doubles per RHS) for the batched BLAS updates:
+  // copied from host `v` to a device slot; returns the device pointer
+  const double* put_coefs(const double* v);
+  double* d_coef = nullptr;  // kCoefSlots x 4*kMaxRhs
+  double* h_coef = nullptr;  // pinned staging of the same size
+  int coef_next = 0;
+  static constexpr int kCoefSlots = 64;
   void check_launch(const char* what);
 
   // FP16-storage SAP (precision form): fields converted from the FP32 ones,
@@ -131,6 +152,31 @@ struct Ctx {
   float* eo_s[2] = {};
   void ensure_eo();
   long n_mtilde = 0;
+
+  // CUDA graphs of the SAP preconditioner's launch sequences (about 40
+  // launches, no host synchronisation inside), captured on first use per
+  // (operator, buffers, nsap, nm, kappa) and replayed afterwards.  Off while
+  // kernel timing is on and on the legacy default stream.
+  struct GraphKey {
+    int op;
+    const void* a;
+    const void* b;
+    int nsap, nm;
+    double kappa;
+    bool operator==(const GraphKey& o) const {
+      return op == o.op && a == o.a && b == o.b && nsap == o.nsap && nm == o.nm &&
+             kappa == o.kappa;
+    }
+  };
+  struct GraphEntry {
+    GraphKey key;
+    cudaGraphExec_t exec;
+    long d_jinv, d_prec_ddd, d_prec_s, d_prec_s_h, d_launches;  // counts one replay stands for
+  };
+  std::vector<GraphEntry> graphs;
+  bool use_graphs = true;
+  long n_graph_launches = 0;
+  void clear_graphs();
 };
 
 // kernel kinds for timing
@@ -182,6 +228,25 @@ void bicgstab_dd_mix(Ctx& c, double* x, const double* b, double tol, int maxiter
                      int maxiter_s, int nsap, int nm, SolveStats* stats, double* hist,
                      int hist_len);
 double true_residual(Ctx& c, const double* x, const double* b);
+
+// multi-RHS forms (solver_mrhs.cu) on a context with G.nr right-hand sides:
+// per-RHS scalars and convergence, one launch per operator for all RHS.
+// iters / st / rel hold G.nr entries.
+int bicgstab_precdd_s_mrhs(Ctx& c, float* x, const float* b, double tol, int maxiter, int nsap,
+                           int nm, int* iters);
+int bicgstab_precdd_s_h_mrhs(Ctx& c, float* x, const float* b, double tol, int maxiter, int nsap,
+                             int nm, int* iters);
+void bicgstab_dd_mix_mrhs(Ctx& c, double* x, const double* b, double tol, int maxiter,
+                          double tol_s, int maxiter_s, int nsap, int nm, SolveStats* st);
+void bicgstab_dd_mix2_hf_mrhs(Ctx& c, double* x, const double* b, double tol, int maxiter,
+                              double tol_s, int maxiter_s, int nsap, int nm, int reliable,
+                              SolveStats* st);
+void true_residual_mrhs(Ctx& c, const double* x, const double* b, double* rel);
+
+// clover term of the resident gauge field on the device (clover_build.cu)
+void build_clover(Ctx& c, double csw);
+// seeded SU(3) + APE gauge field generated on the device (gauge_gen.cu)
+double gen_gauge_device(Ctx& c, unsigned long long seed, int n_smear, double alpha);
 
 void set_error(const std::string& m);
 

@@ -23,7 +23,8 @@
 namespace qwsg {
 
 template <typename T, int SEL, int MU, int DIR, typename R = typename Arith<T>::R>
-__device__ __forceinline__ void do_hop(const HopArgs<T>& a, const Site& s, int g, R acc[24]) {
+__device__ __forceinline__ void do_hop(const HopArgs<T>& a, const Site& s, int g, int rhs,
+                                       R acc[24]) {
   const bool face = DIR > 0 ? (s.lc[MU] == a.G.B[MU] - 1) : (s.lc[MU] == 0);
   if (face) {
     if (!(SEL & HOP_OUTER)) return;
@@ -39,10 +40,11 @@ __device__ __forceinline__ void do_hop(const HopArgs<T>& a, const Site& s, int g
     if (ncol == a.zero_col) return;  // that colour's source is defined as zero
   }
   R v[24];
+  const int sp = spad(a.G), en = sentry(a.G, gn, rhs);
   if (MU == 3)
-    IO<T>::load_half(a.src, a.G.pad, gn, DIR > 0, v);
+    IO<T>::load_half(a.src, sp, en, DIR > 0, v);
   else
-    IO<T>::load_spinor(a.src, a.G.pad, gn, v);
+    IO<T>::load_spinor(a.src, sp, en, v);
   R h[12], r[12], u[18];
   project<R, MU, DIR>(v, h);
   IO<T>::load_link(a.U, a.G.pad, MU, DIR > 0 ? g : gn, u);
@@ -62,8 +64,10 @@ template <typename T, int SEL, int EPI>
 __global__ void __launch_bounds__(128) k_hop(const HopArgs<T> a) {
   using R = typename Arith<T>::R;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.nsites) return;
-  const int g = a.list ? __ldg(a.list + i) : a.site0 + i;
+  if (i >= (a.nsites << a.G.lgnr)) return;
+  // consecutive threads: the right-hand sides of one site, then the next site
+  const int si = i >> a.G.lgnr, rhs = i & (a.G.nr - 1);
+  const int g = a.list ? __ldg(a.list + si) : a.site0 + si;
   Site s;
   decode_site(a.G, g, s);
   if (a.dom >= 0 && (s.bc[0] & 1) != a.dom) return;
@@ -76,44 +80,46 @@ __global__ void __launch_bounds__(128) k_hop(const HopArgs<T> a) {
   R acc[24];
 #pragma unroll
   for (int j = 0; j < 24; j++) acc[j] = 0;
-  do_hop<T, SEL, 0, +1>(a, s, g, acc);
-  do_hop<T, SEL, 0, -1>(a, s, g, acc);
-  do_hop<T, SEL, 1, +1>(a, s, g, acc);
-  do_hop<T, SEL, 1, -1>(a, s, g, acc);
-  do_hop<T, SEL, 2, +1>(a, s, g, acc);
-  do_hop<T, SEL, 2, -1>(a, s, g, acc);
-  do_hop<T, SEL, 3, +1>(a, s, g, acc);
-  do_hop<T, SEL, 3, -1>(a, s, g, acc);
+  do_hop<T, SEL, 0, +1>(a, s, g, rhs, acc);
+  do_hop<T, SEL, 0, -1>(a, s, g, rhs, acc);
+  do_hop<T, SEL, 1, +1>(a, s, g, rhs, acc);
+  do_hop<T, SEL, 1, -1>(a, s, g, rhs, acc);
+  do_hop<T, SEL, 2, +1>(a, s, g, rhs, acc);
+  do_hop<T, SEL, 2, -1>(a, s, g, rhs, acc);
+  do_hop<T, SEL, 3, +1>(a, s, g, rhs, acc);
+  do_hop<T, SEL, 3, -1>(a, s, g, rhs, acc);
   clover_apply<T>(a.C, a.G.pad, g, acc);
+  const int sp = spad(a.G), e = sentry(a.G, g, rhs);
   R o[24];
   if (EPI == EPI_D) {
-    IO<T>::load_spinor(a.src, a.G.pad, g, o);
+    IO<T>::load_spinor(a.src, sp, e, o);
 #pragma unroll
     for (int j = 0; j < 24; j++) o[j] = o[j] + a.coef * acc[j];
   } else if (EPI == EPI_ADD) {
-    IO<T>::load_spinor(a.out, a.G.pad, g, o);
+    IO<T>::load_spinor(a.out, sp, e, o);
 #pragma unroll
     for (int j = 0; j < 24; j++) o[j] = o[j] + a.coef * acc[j];
   } else if (EPI == EPI_JINV) {
-    IO<T>::load_spinor(a.aux, a.G.pad, g, o);
+    IO<T>::load_spinor(a.aux, sp, e, o);
 #pragma unroll
     for (int j = 0; j < 24; j++) o[j] = o[j] + a.coef * acc[j];
   } else {  // EPI_SAPE: coef = -kappa
     R in[24], av[24];
-    IO<T>::load_spinor(a.out, a.G.pad, g, o);
-    IO<T>::load_spinor(a.aux, a.G.pad, g, in);
-    IO<T>::load_spinor(a.src, a.G.pad, g, av);
+    IO<T>::load_spinor(a.out, sp, e, o);
+    IO<T>::load_spinor(a.aux, sp, e, in);
+    IO<T>::load_spinor(a.src, sp, e, av);
 #pragma unroll
     for (int j = 0; j < 24; j++) o[j] = o[j] + (in[j] - (av[j] + a.coef * acc[j]));
   }
-  IO<T>::store_spinor(a.out, a.G.pad, g, o);
+  IO<T>::store_spinor(a.out, sp, e, o);
 }
 
 template <typename T, int SEL, int EPI>
 static void launch(const HopArgs<T>& a, cudaStream_t st) {
   if (a.nsites <= 0) return;
   const int threads = 128;
-  const int blocks = (a.nsites + threads - 1) / threads;
+  const int blocks = ((a.nsites << a.G.lgnr) + threads - 1) / threads;
+  count_launch();
   k_hop<T, SEL, EPI><<<blocks, threads, 0, st>>>(a);
 }
 

@@ -19,19 +19,6 @@
 
 namespace qwsg {
 
-__device__ __forceinline__ int dd_index(const Geom& G, const int x[4]) {
-  int bc[4], lc[4];
-#pragma unroll
-  for (int mu = 0; mu < 4; mu++) {
-    bc[mu] = x[mu] / G.B[mu];
-    lc[mu] = x[mu] - bc[mu] * G.B[mu];
-  }
-  int col = (bc[0] + bc[1] + bc[2] + bc[3]) & 1;
-  int blin = bc[0] + G.NB[0] * (bc[1] + G.NB[1] * (bc[2] + G.NB[2] * bc[3]));
-  int local = lc[0] + G.B[0] * (lc[1] + G.B[1] * (lc[2] + G.B[2] * lc[3]));
-  return col * G.Vh + (blin >> 1) * G.Vb + local;
-}
-
 template <typename T, int WHICH, int DAG, int MU, int DIR, typename R = typename Arith<T>::R>
 __device__ __forceinline__ void eo_hop(const EoArgs<T>& a, const int x[4], int g, R acc[24]) {
   const int L = a.G.L[MU], box = a.box[MU];
@@ -154,6 +141,7 @@ __global__ void k_parity_select(Geom G, typename Store<T>::type* dst,
 template <typename T>
 void parity_select(const Geom& G, typename Store<T>::type* dst, const typename Store<T>::type* src,
                    int pe, cudaStream_t st) {
+  count_launch();
   k_parity_select<T><<<(G.V + 127) / 128, 128, 0, st>>>(G, dst, src, pe);
 }
 template void parity_select<float>(const Geom&, float*, const float*, int, cudaStream_t);
@@ -161,6 +149,7 @@ template void parity_select<double>(const Geom&, double*, const double*, int, cu
 
 template <typename T, int WHICH, int DAG, int CLOV, int MODE>
 static void go(const EoArgs<T>& a, cudaStream_t st) {
+  count_launch();
   k_eo<T, WHICH, DAG, CLOV, MODE><<<(a.G.Vh + 127) / 128, 128, 0, st>>>(a);
 }
 
@@ -183,6 +172,7 @@ void launch_eo(int which, int dag, int clov, int mode, const EoArgs<T>& a, cudaS
 
 template <typename T>
 void launch_clv(const EoArgs<T>& a, cudaStream_t st) {
+  count_launch();
   k_clv<T><<<(a.G.Vh + 127) / 128, 128, 0, st>>>(a);
 }
 

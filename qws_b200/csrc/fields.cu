@@ -21,6 +21,7 @@
 //    the two 6x6 chiral blocks of T^-1 / 2 in QWS's packed format
 //    (clover_def.h:88-284): with X = (s0+s2, s1+s3 | s0-s2, s1-s3) the clover
 //    kernel computes s <- P^T diag(M0, M1) P s, so M_i = (P T P^T / 2)_i^-1 / 2.
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -225,6 +226,47 @@ static bool invert(cd* a, int n) {
 }
 
 }  // namespace fields
+
+// sigma_{mu nu} (mu < nu, planes in the order 01 02 03 12 13 23) in the
+// chiral basis of the packed clover: S[p][i][h][h2] = (Ps sigma Ps^T / 2)
+// restricted to chirality block i, rows h / columns h2 of that block, with
+// Ps rows (s0+s2, s1+s3 | s0-s2, s1-s3).  Returns the largest entry outside
+// the two chirality blocks (zero: sigma is block diagonal there).
+double clover_chiral_tables(double S[6][2][2][2][2]) {
+  using namespace fields;
+  cd g[4][4][4];
+  gamma_matrices(g);
+  const cd I(0, 1);
+  const double Ps[4][4] = {{1, 0, 1, 0}, {0, 1, 0, 1}, {1, 0, -1, 0}, {0, 1, 0, -1}};
+  double off = 0;
+  int p = 0;
+  for (int m = 0; m < 4; m++)
+    for (int n = m + 1; n < 4; n++, p++) {
+      cd sig[4][4];
+      for (int a = 0; a < 4; a++)
+        for (int b = 0; b < 4; b++) {
+          cd c = 0;
+          for (int k = 0; k < 4; k++) c += g[m][a][k] * g[n][k][b] - g[n][a][k] * g[m][k][b];
+          sig[a][b] = 0.5 * I * c;
+        }
+      for (int r = 0; r < 4; r++)
+        for (int q = 0; q < 4; q++) {
+          cd acc = 0;
+          for (int a = 0; a < 4; a++)
+            for (int b = 0; b < 4; b++) acc += Ps[r][a] * sig[a][b] * Ps[q][b];
+          acc *= 0.5;
+          const int i = r / 2, j = q / 2;
+          if (i != j) {
+            off = std::max(off, std::abs(acc));
+            continue;
+          }
+          S[p][i][r % 2][q % 2][0] = acc.real();
+          S[p][i][r % 2][q % 2][1] = acc.imag();
+        }
+    }
+  return off;
+}
+
 }  // namespace qwsg
 
 using namespace qwsg::fields;

@@ -2,9 +2,16 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "lattice.cuh"
 
 namespace qwsg {
+
+// kernels launched by this library in this process (host-side count; a CUDA
+// graph replay adds the launches it captured)
+extern std::atomic<long> g_kernel_launches;
+inline void count_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
 
 enum { HOP_INNER = 1, HOP_OUTER = 2, HOP_ALL = 3 };
 enum { EPI_D = 0, EPI_ADD = 1, EPI_JINV = 2, EPI_SAPE = 3 };
@@ -55,20 +62,21 @@ void parity_select(const Geom& G, typename Store<T>::type* dst, const typename S
 [[noreturn]] void throw_unsupported_eo();
 
 // ---------------------------------------------------------------------------
-// BLAS-1 on spinor planes (complex per-site vectors of 12 components).
-// Reductions are written to `res` (device, double) deterministically.
+// BLAS-1 on spinor planes (complex per-site vectors of 12 components), over
+// every right-hand side of the field.  Reductions are per RHS, written to
+// res[4*rhs + k] (device, double) deterministically.
 // ---------------------------------------------------------------------------
 struct RedBuf {
-  double* partial;    // [nblk_max * 8]
-  unsigned* counter;  // one per concurrent reduction slot
-  int nblk;
+  double* partial;    // [nblk * 32 rhs * 4]
+  unsigned* counter;  // completion counter of the running reduction
+  int nblk;           // most blocks a reduction launch uses
 };
 
 template <typename R>
 void blas_copy(const Geom& G, R* y, const R* x, int site0, int n, cudaStream_t st);
 template <typename R>
 void blas_zero(const Geom& G, R* y, int site0, int n, cudaStream_t st);
-// res[0] = |x|^2
+// res[0] = |x|^2   (res[4*rhs] for each right-hand side, and so on below)
 template <typename R>
 void blas_norm2(const Geom& G, const R* x, double* res, RedBuf& rb, cudaStream_t st);
 // res[0..1] = <x,y> = sum conj(x) y
@@ -79,13 +87,15 @@ template <typename R>
 void blas_norm_cdot(const Geom& G, const R* y, const R* x, double* res, RedBuf& rb,
                     cudaStream_t st);
 // x += a p ; r -= a q ; res[0] = |r|^2 ; optionally res[1..2] = <r0, r>
+// (cf: per-RHS (ar, ai) table on the device, cf[4*rhs + 0..1], else the values)
 template <typename R>
 void blas_bicg_update(const Geom& G, R* x, R* r, const R* p, const R* q, double ar, double ai,
-                      const R* r0, double* res, RedBuf& rb, cudaStream_t st);
-// p = r + b (p - w q)
+                      const R* r0, double* res, RedBuf& rb, cudaStream_t st,
+                      const double* cf = nullptr);
+// p = r + b (p - w q)   (cf: per-RHS (br, bi, wr, wi))
 template <typename R>
 void blas_bicg_p(const Geom& G, R* p, const R* r, const R* q, double br, double bi, double wr,
-                 double wi, cudaStream_t st);
+                 double wi, cudaStream_t st, const double* cf = nullptr);
 // r = b - q ; p = r ; r0 = r ; res[0] = |b|^2 ; res[1] = |r|^2
 template <typename R>
 void blas_bicg_init(const Geom& G, const R* b, const R* q, R* r, R* p, R* r0, double* res,
@@ -97,9 +107,11 @@ void spinor_h2h(const Geom& G, __half* dst, const __half* src, cudaStream_t st);
 // FP16 copies of the FP32 gauge (9 complex planes per mu) and clover planes
 void fields_s2h(const Geom& G, __half* Uh, const float* Us, __half* Ch, const float* Cs,
                 cudaStream_t st);
-// y = (float)(x * s)   /   y = (double)x * s
-void blas_d2s(const Geom& G, float* y, const double* x, double s, cudaStream_t st);
-void blas_s2d(const Geom& G, double* y, const float* x, double s, cudaStream_t st);
+// y = (float)(x * s)   /   y = (double)x * s   (cf: per-RHS s, cf[4*rhs])
+void blas_d2s(const Geom& G, float* y, const double* x, double s, cudaStream_t st,
+              const double* cf = nullptr);
+void blas_s2d(const Geom& G, double* y, const float* x, double s, cudaStream_t st,
+              const double* cf = nullptr);
 
 // ---------------------------------------------------------------------------
 // layout conversion: QWS host layout (lane width vlen) <-> device planes.
@@ -128,11 +140,12 @@ void qws_eo_to_planes_spinor(const Geom& G, R* dst, const R* qws_half, int vlen,
 template <typename R>
 void planes_to_qws_eo_spinor(const Geom& G, R* qws_half, const R* src, int vlen, int p,
                              cudaStream_t st);
-// natural layout (site = x + Lx*(y + Ly*(z + Lz*t))) <-> device planes
+// natural layout (site = x + Lx*(y + Ly*(z + Lz*t))) <-> device planes;
+// rhs selects one right-hand side of a multi-RHS field
 template <typename R>
-void nat_to_planes_spinor(const Geom& G, R* dst, const R* nat, cudaStream_t st);
+void nat_to_planes_spinor(const Geom& G, R* dst, const R* nat, cudaStream_t st, int rhs = 0);
 template <typename R>
-void planes_to_nat_spinor(const Geom& G, R* nat, const R* src, cudaStream_t st);
+void planes_to_nat_spinor(const Geom& G, R* nat, const R* src, cudaStream_t st, int rhs = 0);
 template <typename Rin, typename R>
 void nat_to_planes_gauge(const Geom& G, R* dst, const Rin* nat, cudaStream_t st);
 template <typename Rin, typename R>

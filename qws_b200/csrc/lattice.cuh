@@ -38,7 +38,20 @@ struct Geom {
   int tbc;     // +1 periodic / -1 antiperiodic in t (fbc_f[3], qws.cc:298-310)
   int pad;     // plane stride in elements
   int str[4];  // in-block strides: 1, B0, B0*B1, B0*B1*B2
+  // right-hand sides per spinor field (a power of two, 1..32).  Spinor
+  // fields interleave them RHS-minor: RHS r of site g is entry
+  // (g << lgnr) + r of planes with stride pad << lgnr, so the threads of one
+  // site's RHS sit side by side in a warp and share every link and clover
+  // load.  Gauge and clover fields are per site (stride pad).
+  int nr;
+  int lgnr;
 };
+
+// plane stride of spinor fields and the entry of (site, rhs)
+__host__ __device__ __forceinline__ int spad(const Geom& G) { return G.pad << G.lgnr; }
+__host__ __device__ __forceinline__ int sentry(const Geom& G, int g, int r) {
+  return (g << G.lgnr) + r;
+}
 
 struct Site {
   int col;     // block colour
@@ -64,6 +77,28 @@ __device__ __forceinline__ void decode_site(const Geom& G, int g, Site& s) {
   s.bc[2] = q % G.NB[2];
   s.bc[3] = q / G.NB[2];
   s.bc[0] = 2 * r + ((s.col + s.bc[1] + s.bc[2] + s.bc[3]) & 1);
+}
+
+// DD-order index of the site with global coordinates x
+__host__ __device__ __forceinline__ int dd_index(const Geom& G, const int x[4]) {
+  int bc[4], lc[4];
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++) {
+    bc[mu] = x[mu] / G.B[mu];
+    lc[mu] = x[mu] - bc[mu] * G.B[mu];
+  }
+  int col = (bc[0] + bc[1] + bc[2] + bc[3]) & 1;
+  int blin = bc[0] + G.NB[0] * (bc[1] + G.NB[1] * (bc[2] + G.NB[2] * bc[3]));
+  int local = lc[0] + G.B[0] * (lc[1] + G.B[1] * (lc[2] + G.B[2] * lc[3]));
+  return col * G.Vh + (blin >> 1) * G.Vb + local;
+}
+
+// global coordinates of the site with DD-order index g
+__device__ __forceinline__ void site_coords(const Geom& G, int g, int x[4]) {
+  Site s;
+  decode_site(G, g, s);
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++) x[mu] = s.bc[mu] * G.B[mu] + s.lc[mu];
 }
 
 // index of the neighbour across the block face in direction mu (dir = +1/-1)

@@ -71,6 +71,10 @@ extern "C" int qwsg_jinv_s_noalloc(qwsg_lattice* lat, float* x, const float* b, 
     return 4;
   }
   Ctx& c = *lat->c;
+  if (c.G.nr != 1) {
+    set_error("qwsg_jinv_s_noalloc: not available on a multi-RHS handle");
+    return 1;
+  }
   if (24 * (size_t)c.G.pad > kJinvScratchFloats) {
     set_error("qwsg_jinv_s_noalloc: lattice of " + std::to_string(c.G.V) +
               " sites exceeds the fixed scratch (at most " +

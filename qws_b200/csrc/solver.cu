@@ -29,10 +29,11 @@ HopArgs<T> hop_args(const Geom& G, const typename Store<T>::type* U,
   return a;
 }
 
-// algorithmic bytes moved per handled site
+// algorithmic bytes moved per handled site: each spinor stream once per
+// right-hand side, links and clover once per site
 template <typename T>
-double hop_bytes(int sel, int epi) {
-  const double sp = Bytes<T>::spinor, lc = Bytes<T>::links + Bytes<T>::clover;
+double hop_bytes(int sel, int epi, int nr) {
+  const double sp = Bytes<T>::spinor * nr, lc = Bytes<T>::links + Bytes<T>::clover;
   if (epi == EPI_JINV) return 3 * sp + lc;  // src, b, out
   if (epi == EPI_SAPE) return 4 * sp + lc;  // a, in, s (r+w)
   if (epi == EPI_ADD) return 3 * sp + lc;   // out (r+w), one face neighbour
@@ -72,7 +73,7 @@ void run_hop(Ctx& c, int sel, int epi, const HopArgs<T>& a) {
   long sites = a.nsites;
   if (sel == HOP_OUTER && !a.list) sites = face_sites_per_colour(c.G) * (a.nsites == c.G.V ? 2 : 1);
   if (a.dom >= 0) sites /= 2;
-  c.recs.push_back({kind_of<T>(sel, epi), e0, e1, (double)sites * hop_bytes<T>(sel, epi)});
+  c.recs.push_back({kind_of<T>(sel, epi), e0, e1, (double)sites * hop_bytes<T>(sel, epi, c.G.nr)});
 }
 
 template <typename T>
@@ -134,7 +135,12 @@ void kernel_stats(Ctx& c, long* launches, double* ms, double* bytes) {
   c.ev_next = 0;
 }
 
-Ctx::Ctx(const int L[4], const int NB[4], int tbc) {
+Ctx::Ctx(const int L[4], const int NB[4], int tbc, int nrhs) {
+  if (nrhs < 1 || nrhs > kMaxRhs || (nrhs & (nrhs - 1)))
+    throw Error(1, "number of right-hand sides must be a power of two in 1..32");
+  G.nr = nrhs;
+  G.lgnr = 0;
+  while ((1 << G.lgnr) < nrhs) G.lgnr++;
   for (int mu = 0; mu < 4; mu++) {
     if (L[mu] <= 0 || NB[mu] <= 0 || L[mu] % NB[mu] != 0)
       throw Error(1, "lattice extent not divisible by the block grid");
@@ -148,6 +154,8 @@ Ctx::Ctx(const int L[4], const int NB[4], int tbc) {
       throw Error(1, "block grid NB[1..3] must be 1 or even (red-black block colouring)");
   long V = (long)L[0] * L[1] * L[2] * L[3];
   if (V >= (1L << 30)) throw Error(1, "lattice too large for 32-bit site indices");
+  if (((long)(V + 127) / 128 * 128) * nrhs * 12 >= (1L << 31))
+    throw Error(1, "lattice x right-hand sides too large for 32-bit plane offsets");
   G.V = (int)V;
   G.Vh = G.V / 2;
   G.Vb = G.B[0] * G.B[1] * G.B[2] * G.B[3];
@@ -162,11 +170,26 @@ Ctx::Ctx(const int L[4], const int NB[4], int tbc) {
   QWSG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   own_stream = true;
   rb.nblk = 148 * 8;
-  QWSG_CUDA(cudaMalloc(&rb.partial, sizeof(double) * 8 * rb.nblk));
+  QWSG_CUDA(cudaMalloc(&rb.partial, sizeof(double) * 4 * kMaxRhs * rb.nblk));
   QWSG_CUDA(cudaMalloc(&rb.counter, sizeof(unsigned) * 4));
   QWSG_CUDA(cudaMemset(rb.counter, 0, sizeof(unsigned) * 4));
-  QWSG_CUDA(cudaMalloc(&d_res, sizeof(double) * 8));
-  QWSG_CUDA(cudaMallocHost(&h_res, sizeof(double) * 8));
+  QWSG_CUDA(cudaMalloc(&d_res, sizeof(double) * 4 * kMaxRhs));
+  QWSG_CUDA(cudaMallocHost(&h_res, sizeof(double) * 4 * kMaxRhs));
+  QWSG_CUDA(cudaMalloc(&d_coef, sizeof(double) * 4 * kMaxRhs * kCoefSlots));
+  QWSG_CUDA(cudaMallocHost(&h_coef, sizeof(double) * 4 * kMaxRhs * kCoefSlots));
+}
+
+// Each slot is used once per kCoefSlots calls; the batched solvers read a
+// reduction result (a stream synchronisation) between consecutive uses of
+// one slot, so a slot is never rewritten while its copy is pending.
+const double* Ctx::put_coefs(const double* v) {
+  const int n = 4 * kMaxRhs;
+  double* h = h_coef + (size_t)coef_next * n;
+  double* d = d_coef + (size_t)coef_next * n;
+  coef_next = (coef_next + 1) % kCoefSlots;
+  std::memcpy(h, v, sizeof(double) * 4 * G.nr);
+  QWSG_CUDA(cudaMemcpyAsync(d, h, sizeof(double) * 4 * G.nr, cudaMemcpyHostToDevice, st));
+  return d;
 }
 
 Ctx::~Ctx() {
@@ -174,14 +197,20 @@ Ctx::~Ctx() {
   for (void* p : owned) cudaFree(p);
   if (stage) cudaFree(stage);
   for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
-  cudaFree(Ud);
-  cudaFree(Cd);
-  cudaFree(Us);
-  cudaFree(Cs);
-  cudaFree(Uh);
-  cudaFree(Ch);
+  clear_graphs();
+  if (owns_fields) {
+    cudaFree(Ud);
+    cudaFree(Cd);
+    cudaFree(Us);
+    cudaFree(Cs);
+    cudaFree(Uh);
+    cudaFree(Ch);
+  }
   cudaFree(face_list[0]);
   cudaFree(face_list[1]);
+  cudaFree(d_coef);
+  cudaFreeHost(h_coef);
+  if (parent_ev) cudaEventDestroy(parent_ev);
   cudaFree(rb.partial);
   cudaFree(rb.counter);
   cudaFree(d_res);
@@ -203,7 +232,7 @@ template double* Ctx::alloc_spinor<double>();
 // FP16 spinor: 6 uint2 planes + one float plane of per-site scales
 __half* Ctx::alloc_spinor_h() {
   void* p = nullptr;
-  const size_t bytes = (size_t)(6 * 8 + 4) * G.pad;
+  const size_t bytes = (size_t)(6 * 8 + 4) * spad(G);
   QWSG_CUDA(cudaMalloc(&p, bytes));
   QWSG_CUDA(cudaMemsetAsync(p, 0, bytes, st));
   owned.push_back(p);
@@ -271,7 +300,31 @@ void Ctx::ensure_fields_s() {
 }
 // FP16 copies of the FP32 gauge and clover planes (made on first use after
 // every load)
+void Ctx::sync_from_parent(bool half) {
+  if (!parent) return;
+  if (!parent->Ud || !parent->Us) throw Error(4, "gauge/clover fields not loaded");
+  if (half) parent->ensure_fields_h();
+  Ud = parent->Ud;
+  Cd = parent->Cd;
+  Us = parent->Us;
+  Cs = parent->Cs;
+  Uh = parent->Uh;
+  Ch = parent->Ch;
+  fields_h_valid = parent->fields_h_valid;
+  kappa = parent->kappa;
+  // the parent's field uploads and conversions are on its stream
+  if (parent->st != st) {
+    if (!parent_ev) QWSG_CUDA(cudaEventCreateWithFlags(&parent_ev, cudaEventDisableTiming));
+    QWSG_CUDA(cudaEventRecord(parent_ev, parent->st));
+    QWSG_CUDA(cudaStreamWaitEvent(st, parent_ev, 0));
+  }
+}
+
 void Ctx::ensure_fields_h() {
+  if (parent) {
+    sync_from_parent(true);
+    return;
+  }
   if (!Us) throw Error(4, "gauge/clover fields not loaded");
   if (!Uh) {
     QWSG_CUDA(cudaMalloc(&Uh, sizeof(__half) * 72 * (size_t)G.pad));
@@ -456,28 +509,86 @@ static void sap_final_t(Ctx& c, typename Store<T>::type* out, typename Store<T>:
   jinv_t<T>(c, out, s, 1, nm, tmp);
 }
 
+void Ctx::clear_graphs() {
+  for (auto& e : graphs) cudaGraphExecDestroy(e.exec);
+  graphs.clear();
+}
+
+// Run `body` (launches only) through a cached CUDA graph.  Everything the
+// body allocates or builds must exist before the first capture.
+template <typename F>
+static void graphed(Ctx& c, const Ctx::GraphKey& k, F&& body) {
+  if (c.timing || !c.use_graphs || c.st == nullptr || c.st == cudaStreamLegacy ||
+      c.st == cudaStreamPerThread) {
+    body();
+    return;
+  }
+  for (auto& e : c.graphs)
+    if (e.key == k) {
+      QWSG_CUDA(cudaGraphLaunch(e.exec, c.st));
+      c.n_jinv += e.d_jinv;
+      c.n_prec_ddd += e.d_prec_ddd;
+      c.n_prec_s += e.d_prec_s;
+      c.n_prec_s_h += e.d_prec_s_h;
+      g_kernel_launches.fetch_add(e.d_launches, std::memory_order_relaxed);
+      c.n_graph_launches++;
+      return;
+    }
+  const long j0 = c.n_jinv, p0 = c.n_prec_ddd, s0 = c.n_prec_s, h0 = c.n_prec_s_h;
+  const long l0 = g_kernel_launches.load();
+  QWSG_CUDA(cudaStreamBeginCapture(c.st, cudaStreamCaptureModeThreadLocal));
+  try {
+    body();
+  } catch (...) {
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(c.st, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  cudaGraph_t g = nullptr;
+  QWSG_CUDA(cudaStreamEndCapture(c.st, &g));
+  cudaGraphExec_t exec = nullptr;
+  cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+  cudaGraphDestroy(g);
+  QWSG_CUDA(e);
+  if (c.graphs.size() >= 16) {  // a bounded cache: drop the oldest
+    cudaGraphExecDestroy(c.graphs.front().exec);
+    c.graphs.erase(c.graphs.begin());
+  }
+  c.graphs.push_back({k, exec, c.n_jinv - j0, c.n_prec_ddd - p0, c.n_prec_s - s0,
+                      c.n_prec_s_h - h0, g_kernel_launches.load() - l0});
+  QWSG_CUDA(cudaGraphLaunch(exec, c.st));
+  c.n_graph_launches++;
+}
+
 // prec_ddd_s_ (qws.cc:776-926): out = D M_SAP in.  Both of the reference's
 // final-stage branches compute a_E = J_E(s_E), a_O = J_O(s_O - D_face,O (a_E, 0)),
 // out = D (a_E, a_O); here the last product is one full-lattice D.
 void prec_ddd_s(Ctx& c, float* out, const float* in, int nsap, int nm) {
   if (nsap > 10 || nm > 10) throw Error(2, "prec_ddd_s_: nsap and nm must be <= 10 (qws.cc:798-799)");
   c.ensure_sap();
+  c.ensure_face_lists();
   float *s = c.sap_s, *a = c.sap_a;
-  blas_copy<float>(c.G, s, in, 0, c.G.V, c.st);
-  sap_sweeps_t<float>(c, s, a, c.sap_t, in, nsap, nm);
-  sap_final_t<float>(c, a, s, c.sap_t, nm);
-  dslash_full_s(c, out, a);
-  c.n_prec_ddd++;
+  graphed(c, {0, out, in, nsap, nm, c.kappa}, [&] {
+    blas_copy<float>(c.G, s, in, 0, c.G.V, c.st);
+    sap_sweeps_t<float>(c, s, a, c.sap_t, in, nsap, nm);
+    sap_final_t<float>(c, a, s, c.sap_t, nm);
+    dslash_full_s(c, out, a);
+    c.n_prec_ddd++;
+  });
 }
 
 // prec_s_ (qws.cc:929-975): out = M_SAP in.
 void prec_s(Ctx& c, float* out, const float* in, int nsap, int nm) {
   c.ensure_sap();
+  c.ensure_face_lists();
   float *s = c.sap_s, *a = c.sap_a;
-  blas_copy<float>(c.G, s, in, 0, c.G.V, c.st);
-  sap_sweeps_t<float>(c, s, a, c.sap_t, in, nsap, nm);
-  sap_final_t<float>(c, out, s, c.sap_t, nm);
-  c.n_prec_s++;
+  graphed(c, {1, out, in, nsap, nm, c.kappa}, [&] {
+    blas_copy<float>(c.G, s, in, 0, c.G.V, c.st);
+    sap_sweeps_t<float>(c, s, a, c.sap_t, in, nsap, nm);
+    sap_final_t<float>(c, out, s, c.sap_t, nm);
+    c.n_prec_s++;
+  });
 }
 
 // assign_mult_mSAP_s_h_ (prec_ddd_s_h.h:63-231) with FP16 storage: the input
@@ -488,12 +599,15 @@ void prec_s_h(Ctx& c, float* out, const float* in, int nsap, int nm) {
   if (nsap > 10 || nm > 10)
     throw Error(2, "assign_mult_mSAP_s_h_: nsap and nm must be <= 10 (prec_ddd_s_h.h:100-101)");
   c.ensure_hp();
-  spinor_s2h(c.G, c.h_b, in, c.st);
-  spinor_h2h(c.G, c.h_s, c.h_b, c.st);
-  sap_sweeps_t<H16>(c, c.h_s, c.h_a, c.h_t, c.h_b, nsap - 1, nm);
-  sap_final_t<H16>(c, c.h_a, c.h_s, c.h_t, nm);
-  spinor_h2s(c.G, out, c.h_a, c.st);
-  c.n_prec_s_h++;
+  c.ensure_face_lists();
+  graphed(c, {2, out, in, nsap, nm, c.kappa}, [&] {
+    spinor_s2h(c.G, c.h_b, in, c.st);
+    spinor_h2h(c.G, c.h_s, c.h_b, c.st);
+    sap_sweeps_t<H16>(c, c.h_s, c.h_a, c.h_t, c.h_b, nsap - 1, nm);
+    sap_final_t<H16>(c, c.h_a, c.h_s, c.h_t, nm);
+    spinor_h2s(c.G, out, c.h_a, c.st);
+    c.n_prec_s_h++;
+  });
   c.check_launch("prec_s_h");
 }
 

@@ -10,7 +10,10 @@ spinors read and written once, links and clover once per site).
 
 Kernels: jinv (one Richardson step on one colour), dslash_s / dslash_d (full
 D in FP32 / FP64), block_s (block-interior D on one colour), face_s (face hops
-of one colour), prec (the whole SAP preconditioner prec_ddd_s_).
+of one colour), prec (the whole SAP preconditioner prec_ddd_s_), prec_h (the
+FP16-storage SAP).  --nrhs N runs the launch on a multi-RHS handle (N
+right-hand sides per launch; spinor bytes count N times, links and clover
+once).
 """
 from __future__ import annotations
 
@@ -33,6 +36,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--kappa", type=float, default=0.1365)
     ap.add_argument("--csw", type=float, default=1.7)
+    ap.add_argument("--nrhs", type=int, default=1)
     a = ap.parse_args()
     L = tuple(int(v) for v in a.lattice.split(","))
     NB = tuple(int(v) for v in a.blocks.split(","))
@@ -40,10 +44,15 @@ def main():
     C = qws_b200.gen_clover(U, L, a.csw, a.kappa)
     b = qws_b200.gen_source(L, 12)
     st = torch.cuda.Stream()
-    lat = qws_b200.Lattice(L, NB, tbc=-1, kappa=a.kappa, stream=st)
-    lat.load_fields(U, C)
+    base = qws_b200.Lattice(L, NB, tbc=-1, kappa=a.kappa, stream=st)
+    base.load_fields(U, C)
     del U, C
-    V = lat.V
+    V, nr = base.V, a.nrhs
+    lat = base if nr == 1 else base.batch(nr, stream=st)
+    if nr > 1:
+        b = np.stack([b] * nr)
+    # algorithmic bytes per site: spinor streams per RHS + links + clover
+    sp32, sp64, lc32, lc64 = 96 * nr, 192 * nr, 576, 1152
     with torch.cuda.stream(st):
         bs = lat.to_device(b.astype(np.float32))
         bd = lat.to_device(b)
@@ -51,17 +60,19 @@ def main():
         out_d = lat.empty("f64")
         k = a.kernel
         if k == "jinv":
-            fn, nbytes = (lambda: lat.jinv(bs, 0, 1, out=out_s)), (V // 2) * 216 * 4
+            fn, nbytes = (lambda: lat.jinv(bs, 0, 1, out=out_s)), (V // 2) * (3 * sp32 + lc32)
         elif k == "dslash_s":
-            fn, nbytes = (lambda: lat.ddd(bs, out=out_s)), V * 192 * 4
+            fn, nbytes = (lambda: lat.ddd(bs, out=out_s)), V * (2 * sp32 + lc32)
         elif k == "dslash_d":
-            fn, nbytes = (lambda: lat.ddd(bd, out=out_d)), V * 192 * 8
+            fn, nbytes = (lambda: lat.ddd(bd, out=out_d)), V * (2 * sp64 + lc64)
         elif k == "block_s":
-            fn, nbytes = (lambda: lat.ddd_in(bs, 0, out=out_s)), (V // 2) * 192 * 4
+            fn, nbytes = (lambda: lat.ddd_in(bs, 0, out=out_s)), (V // 2) * (2 * sp32 + lc32)
         elif k == "face_s":
             fn, nbytes = (lambda: lat.ddd_out(bs, 0, 0.1, out=out_s)), None
         elif k == "prec":
             fn, nbytes = (lambda: lat.prec_ddd(bs, 4, 2, out=out_s)), None
+        elif k == "prec_h":
+            fn, nbytes = (lambda: lat.prec_h(bs, 4, 2, out=out_s)), None
         else:
             raise SystemExit(f"unknown kernel {k}")
         for _ in range(a.warmup):
@@ -74,13 +85,15 @@ def main():
         e1.record(st)
         torch.cuda.synchronize()
     us = e0.elapsed_time(e1) * 1e3 / a.iters
-    res = {"kernel": k, "lattice": "x".join(map(str, L)), "blocks": list(NB), "us_per_launch": us,
-           "plaquette": plaq}
+    res = {"kernel": k, "lattice": "x".join(map(str, L)), "blocks": list(NB), "nrhs": nr,
+           "us_per_launch": us, "us_per_rhs": us / nr, "plaquette": plaq}
     if nbytes:
         res["bytes_per_launch"] = nbytes
         res["GBps"] = nbytes / (us * 1e-6) / 1e9
     print(json.dumps(res), flush=True)
     lat.close()
+    if lat is not base:
+        base.close()
 
 
 if __name__ == "__main__":

@@ -1,0 +1,410 @@
+"""Continuous-batching solve service on one GPU.
+
+Requests (gauge field, kappa, csw, source, tolerance) arrive at any time.
+The service keeps gauge fields resident on the device, builds each
+request's clover term there (qwsg_build_clover), admits work against an
+HBM budget, merges compatible pending requests -- same lattice, gauge
+field, kappa, csw and tolerance -- into one multi-RHS solve
+(qwsg_create_batch), and runs several solves at once on separate CUDA
+streams, so requests that arrive while others are on the GPU start as soon
+as a worker slot and memory are free.  Every result carries its own latency
+(completion minus arrival); `summarize` gives p50/p99 and solves/s.
+
+The solver is the precision form (bicgstab_dd_mix2_hf: FP64 outer with
+reliable restarts, flexible FP32 inner, FP16-storage SAP).  A request's
+result does not depend on what it was merged or overlapped with beyond the
+solve tolerance: per-RHS scalars and convergence in the batch, and each
+resident field is held by one job at a time.
+
+    python -m qws_b200.serve --rate 20 --window 10
+"""
+from __future__ import annotations
+
+import argparse
+import itertools
+import json
+import queue
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# bytes per padded site of the pieces a job holds on the device
+_FIELD_BYTES = 72 * (8 + 4 + 2) * 2       # gauge + clover, FP64/FP32/FP16 copies
+_WORK_BYTES_PER_RHS = 9 * 24 * 8 + 12 * 24 * 4 + 4 * 52  # FP64, FP32, FP16 work spinors
+
+
+def _pad(V):
+    return (V + 127) // 128 * 128
+
+
+def field_bytes(L):
+    return _FIELD_BYTES * _pad(int(np.prod(L)))
+
+
+def work_bytes(L, nr):
+    return _WORK_BYTES_PER_RHS * _pad(int(np.prod(L))) * nr
+
+
+@dataclass
+class Request:
+    L: tuple
+    gauge: int
+    kappa: float
+    csw: float
+    tol: float
+    source: np.ndarray            # natural layout [V, 24] FP64
+    rid: int = -1
+    t_arrival: float = 0.0
+    # filled in by the service
+    x: np.ndarray | None = None
+    stats: dict | None = None
+    t_start: float = 0.0
+    t_done: float = 0.0
+    batch: int = 0
+    error: str | None = None
+    done: threading.Event = field(default_factory=threading.Event)
+
+    def key(self):
+        return (self.L, self.gauge, self.kappa, self.csw, self.tol)
+
+    @property
+    def latency(self):
+        return self.t_done - self.t_arrival
+
+
+class _Resident:
+    """One gauge field on the device (a Lattice), with the clover term of the
+    kappa/csw it was last built for.  Held by one job at a time."""
+
+    def __init__(self, L, gauge_id, U, NB):
+        import torch
+
+        import qws_b200
+
+        self.L, self.gid = L, gauge_id
+        self.stream = torch.cuda.Stream()
+        self.lat = qws_b200.Lattice(L, NB, tbc=-1, kappa=0.0, stream=self.stream)
+        if isinstance(U, dict):  # {"seed", "n_smear", "alpha"}: generate on the device
+            self.plaquette = self.lat.gen_gauge_device(U["seed"], U["n_smear"], U["alpha"])
+        else:
+            self.lat.load_gauge(U)
+        self.clover_key = None
+        self.busy = False
+        self.bytes = field_bytes(L)
+        self.work = {}  # nrhs -> BatchLattice on this field
+        self.last_used = time.monotonic()
+
+    def prepare(self, kappa, csw):
+        if self.clover_key != (kappa, csw):
+            self.lat.set_kappa(kappa)
+            self.lat.build_clover(csw)
+            self.clover_key = (kappa, csw)
+
+    def close(self):
+        for w in self.work.values():
+            w.close()
+        self.work.clear()
+        self.lat.close()
+
+
+class _Placeholder:
+    """Reserved slot for a field that a worker is about to make resident."""
+
+    def __init__(self, L, gid):
+        self.L, self.gid = L, gid
+        self.lat = None
+        self.busy = True
+        self.work = {}
+        self.bytes = field_bytes(L)
+        self.last_used = time.monotonic()
+
+    def close(self):
+        pass
+
+
+class Service:
+    """The request loop.  gauge_source(L, gauge_id) -> host gauge field
+    [4, V, 18] FP64, or {"seed", "n_smear", "alpha"} to generate it on the
+    device (called each time the field is made resident)."""
+
+    def __init__(self, gauge_source, budget_bytes=150e9, workers=3, max_batch=16,
+                 block_grid=(2, 1, 1, 1), maxiter=100, tol_s=1e-6, maxiter_s=50, nsap=4, nm=2,
+                 reliable=5):
+        self.gauge_source = gauge_source
+        self.budget = float(budget_bytes)
+        self.max_batch = int(max_batch)
+        self.NB = tuple(block_grid)
+        self.solver = dict(maxiter=maxiter, tol_s=tol_s, maxiter_s=maxiter_s, nsap=nsap, nm=nm,
+                           reliable=reliable)
+        self.pending = []                 # requests not yet started, arrival order
+        self.cv = threading.Condition()
+        self.residents = {}               # (L, gid) -> _Resident or _Placeholder
+        self.used = 0.0                   # bytes held by residents and work handles
+        self.jobs = queue.Queue()
+        self.idle_workers = int(workers)
+        self.ids = itertools.count()
+        self.completed = []
+        self.merged = 0
+        self.stop = False
+        self.workers = [threading.Thread(target=self._worker, daemon=True) for _ in range(workers)]
+        for t in self.workers:
+            t.start()
+        self.sched = threading.Thread(target=self._scheduler, daemon=True)
+        self.sched.start()
+
+    # ---- client side -----------------------------------------------------------
+    def submit(self, req: Request) -> Request:
+        req.rid = next(self.ids)
+        req.t_arrival = time.monotonic()
+        with self.cv:
+            self.pending.append(req)
+            self.cv.notify_all()
+        return req
+
+    def close(self):
+        with self.cv:
+            self.stop = True
+            self.cv.notify_all()
+        self.sched.join()
+        for _ in self.workers:
+            self.jobs.put(None)
+        for t in self.workers:
+            t.join()
+        for r in self.residents.values():
+            r.close()
+        self.residents.clear()
+
+    # ---- scheduling ------------------------------------------------------------
+    def _evict(self, need, keep=None):
+        """Free idle work handles, then idle resident fields (least recently
+        used first; never `keep`) until `need` more bytes fit the budget.
+        Called with cv held."""
+        idle = sorted((r for r in self.residents.values()
+                       if not r.busy and r.lat is not None and r is not keep),
+                      key=lambda r: r.last_used)
+        for r in idle:
+            for nr in list(r.work):
+                if self.used + need <= self.budget:
+                    return True
+                r.work.pop(nr).close()
+                self.used -= work_bytes(r.L, nr)
+        for r in idle:
+            if self.used + need <= self.budget:
+                return True
+            r.close()
+            self.residents.pop((r.L, r.gid))
+            self.used -= r.bytes
+        return self.used + need <= self.budget
+
+    def _pick(self):
+        """The oldest request that can start now, with the compatible pending
+        requests merged into its batch (a power of two, at most max_batch).
+        Called with cv held; reserves the memory and the resident field."""
+        tried = set()
+        for r in self.pending:
+            if r.key() in tried:
+                continue
+            tried.add(r.key())
+            res = self.residents.get((r.L, r.gauge))
+            if res is not None and res.busy:
+                continue
+            group = [q for q in self.pending if q.key() == r.key()]
+            nr = 1
+            while nr * 2 <= min(len(group), self.max_batch, 32):
+                nr *= 2
+            group = group[:nr]
+            need = (field_bytes(r.L) if res is None else 0) + \
+                (work_bytes(r.L, nr) if res is None or nr not in res.work else 0)
+            if self.used + need > self.budget and not self._evict(need, keep=res):
+                continue
+            self.used += need
+            if res is None:
+                res = _Placeholder(r.L, r.gauge)
+                self.residents[(r.L, r.gauge)] = res
+            res.busy = True
+            for q in group:
+                self.pending.remove(q)
+            if nr > 1:
+                self.merged += nr - 1
+            return res, group
+        return None
+
+    def _scheduler(self):
+        with self.cv:
+            while True:
+                if self.stop and not self.pending:
+                    return
+                job = self._pick() if self.idle_workers > 0 and self.pending else None
+                if job is None:
+                    self.cv.wait(0.02)
+                    continue
+                self.idle_workers -= 1
+                self.jobs.put(job)
+
+    # ---- execution -------------------------------------------------------------
+    def _worker(self):
+        while True:
+            job = self.jobs.get()
+            if job is None:
+                return
+            res, group = job
+            try:
+                self._run(res, group)
+            except Exception as e:  # reported on the requests, the service goes on
+                for q in group:
+                    q.error = f"{type(e).__name__}: {e}"
+                    q.t_done = time.monotonic()
+            with self.cv:
+                live = self.residents.get((res.L, res.gid))
+                if live is not None:
+                    live.busy = False
+                    live.last_used = time.monotonic()
+                for q in group:
+                    self.completed.append(q)
+                    q.done.set()
+                self.idle_workers += 1
+                self.cv.notify_all()
+
+    def _run(self, res, group):
+        import torch
+
+        t0 = time.monotonic()
+        for q in group:
+            q.t_start = t0
+        if isinstance(res, _Placeholder):  # first use of this field: make it resident
+            U = self.gauge_source(res.L, res.gid)
+            live = _Resident(res.L, res.gid, U, self.NB)
+            live.busy = True
+            with self.cv:
+                self.residents[(res.L, res.gid)] = live
+            res = live
+        r0 = group[0]
+        nr = len(group)
+        res.prepare(r0.kappa, r0.csw)
+        B = res.work.get(nr)
+        if B is None:  # work buffers of an nr-RHS solve on this field, kept for reuse
+            B = res.lat.batch(nr, stream=res.stream)
+            res.work[nr] = B
+        s = self.solver
+        with torch.cuda.stream(res.stream):
+            S = group[0].source if nr == 1 else np.stack([q.source for q in group])
+            bd = B.to_device(S)
+            xd = B.empty("f64")
+            st = B.bicgstab_dd_mix2_hf(xd, bd, r0.tol, s["maxiter"], s["tol_s"], s["maxiter_s"],
+                                       s["nsap"], s["nm"], reliable=s["reliable"])
+            truer = B.true_residual(xd, bd)
+            X = B.to_host(xd)
+            per = B.batch_stats()[0] if nr > 1 else [st]
+            del bd, xd
+        truer = [truer] if nr == 1 else truer
+        t1 = time.monotonic()
+        for k, q in enumerate(group):
+            q.x = X if nr == 1 else X[k]
+            q.stats = {"outer_iters": per[k]["outer_iters"], "true_rel_resid": truer[k],
+                       "inner_iters": per[k]["inner_iters"]}
+            q.batch = nr
+            q.t_done = t1
+
+
+def summarize(reqs, t_begin=None, t_end=None):
+    """p50/p99 latency (ms), solves/s over the span from the first arrival to
+    the last completion, batch sizes and errors."""
+    ok = [q for q in reqs if q.error is None and q.t_done > 0]
+    if not ok:
+        return {"completed": 0, "errors": len(reqs)}
+    lat = np.array([q.latency for q in ok]) * 1e3
+    t0 = min(q.t_arrival for q in ok) if t_begin is None else t_begin
+    t1 = max(q.t_done for q in ok) if t_end is None else t_end
+    return {"completed": len(ok), "errors": len(reqs) - len(ok),
+            "solves_per_s": len(ok) / max(t1 - t0, 1e-9),
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()), "max_ms": float(lat.max()),
+            "mean_batch": float(np.mean([q.batch for q in ok])),
+            "max_true_rel_resid": max(q.stats["true_rel_resid"] for q in ok),
+            "above_tol": sum(q.stats["true_rel_resid"] >= q.tol for q in ok)}
+
+
+def seeded_gauge(seed0=1000, n_smear=5, alpha=0.36, device=True):
+    """gauge_source for the service: seeded SU(3) + APE fields, one per
+    (lattice, gauge id), generated on the device (or on the host)."""
+    import qws_b200
+
+    def make(L, gid):
+        seed = seed0 + 7919 * gid + sum(L)
+        if device:
+            return {"seed": seed, "n_smear": n_smear, "alpha": alpha}
+        U, _ = qws_b200.gen_gauge(L, seed, n_smear, alpha)
+        return U
+    return make
+
+
+def poisson_workload(service, rate, window, volumes, weights, n_gauges, kappa_range=(0.130, 0.137),
+                     csw=1.7, tols=(1e-8, 1e-10, 1e-12), seed=0, sources_per_volume=2):
+    """Poisson arrivals at `rate` per second for `window` seconds.  Each
+    request draws a volume (with `weights`), a gauge id, kappa uniform in
+    kappa_range, a tolerance and a Gaussian or point source.  Sources come from
+    a small pool made before the window opens, so the feeder keeps up with the
+    arrival times.  Returns the submitted requests (wait on req.done)."""
+    import qws_b200
+
+    rng = np.random.default_rng(seed)
+    pool = {}
+    for L in volumes:
+        pool[L] = [qws_b200.gen_source(L, 5000 + k, "gauss") for k in range(sources_per_volume)]
+        pool[L] += [qws_b200.gen_source(L, 0, "point", k) for k in range(2)]
+    t = 0.0
+    arrivals = []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= window:
+            break
+        arrivals.append(t)
+    p = np.asarray(weights, float) / np.sum(weights)
+    reqs = []
+    t0 = time.monotonic()
+    for ta in arrivals:
+        vi = rng.choice(len(volumes), p=p)
+        L = tuple(volumes[vi])
+        req = Request(L=L, gauge=int(rng.integers(n_gauges)),
+                      kappa=float(rng.uniform(*kappa_range)), csw=csw,
+                      tol=float(rng.choice(tols)), source=pool[L][int(rng.integers(len(pool[L])))])
+        delay = t0 + ta - time.monotonic()
+        if delay > 0:
+            time.sleep(delay)
+        reqs.append(service.submit(req))
+    return reqs
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--rate", type=float, default=20.0)
+    ap.add_argument("--window", type=float, default=10.0)
+    ap.add_argument("--volumes", default="16x16x16x32,24x24x24x48,32x32x32x64,48x48x48x96")
+    ap.add_argument("--weights", default="0.4,0.3,0.2,0.1")
+    ap.add_argument("--gauges", type=int, default=4, help="resident gauge fields per volume")
+    ap.add_argument("--budget-gb", type=float, default=150.0)
+    ap.add_argument("--workers", type=int, default=3)
+    ap.add_argument("--max-batch", type=int, default=16)
+    ap.add_argument("--seed", type=int, default=0)
+    a = ap.parse_args()
+    vols = [tuple(int(v) for v in s.split("x")) for s in a.volumes.split(",")]
+    weights = [float(w) for w in a.weights.split(",")]
+    svc = Service(seeded_gauge(), budget_bytes=a.budget_gb * 1e9, workers=a.workers,
+                  max_batch=a.max_batch)
+    try:
+        reqs = poisson_workload(svc, a.rate, a.window, vols, weights, a.gauges, seed=a.seed)
+        for q in reqs:
+            q.done.wait()
+        out = summarize(reqs)
+        out.update({"rate": a.rate, "window_s": a.window, "requests": len(reqs),
+                    "merged": svc.merged, "workers": a.workers, "budget_gb": a.budget_gb,
+                    "gauges_per_volume": a.gauges})
+        print(json.dumps(out), flush=True)
+    finally:
+        svc.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -77,7 +77,7 @@ def qws():
     b = alloc(2 * HALF_D, np.float64)
     b[:] = nat_to_qws_spinor(S[0], L, VLEND)
     bs = alloc(2 * HALF_S, np.float32)
-    bs[:] = nat_to_qws_spinor(np.asarray(S[1], np.float32), L, VLENS)
+    bs[:] = nat_to_qws_spinor(np.asarray(S[0], np.float32), L, VLENS)  # main.cc: bs = (float)b
     yield lib, b, bs
     lib.qws_finalize_()
 
