@@ -277,13 +277,24 @@ def bench_ours(args, w, name):
         hf_ms = allreduce_max(h0.elapsed_time(h1), world)
         hf_true = lat.true_residual(xd, bd)
     e2e_true = lat.true_residual(xh, bh)
-    batched = bench_batched(args, w, lat, stream, world) if args.batch > 1 else None
+    # sub-results: a failure is reported in the line, it does not lose the line
+    def sub(fn, *a):
+        try:
+            return fn(*a)
+        except Exception as e:  # noqa: BLE001
+            return {"error": f"{type(e).__name__}: {str(e)[-400:]}"}
+
+    batched = sub(bench_batched, args, w, lat, stream, world) if args.batch > 1 else None
     serving = None
-    if args.serve_rate > 0 and world == 1:
-        lat.close()  # the service gets the HBM budget to itself
+    precision_48 = None
+    if world == 1 and (args.serve_rate > 0 or args.config3):
+        lat.close()  # the later parts get the HBM to themselves
         del xd, bd, xh, bh
         torch.cuda.empty_cache()
-        serving = bench_serving(args)
+    if args.serve_rate > 0 and world == 1:
+        serving = sub(bench_serving, args)
+    if args.config3 and world == 1:
+        precision_48 = sub(bench_precision_48, args, world)
 
     per_solve = {k: (c1[k] - c0[k]) / args.steps for k in c1}
     inner_iters = sum(s["inner_iters"] for s in stats) / len(stats)
@@ -354,6 +365,7 @@ def bench_ours(args, w, name):
                       "inner / SAP in FP16 storage with per-site FP32 scales (nsap-1 sweeps)"},
         "batched": batched,
         "serving": serving,
+        "precision_48c96": precision_48,
         "gpu_launches": int(n_launches),
         "roofline": roofline,
         "kernels": kernels,
@@ -361,7 +373,7 @@ def bench_ours(args, w, name):
         "counts_per_solve": counts,
         "field_gen_s": round(t_gen, 2),
     }
-    if batched:
+    if batched and "value" in batched:
         batched["speedup_vs_plain"] = batched["value"] / line["value"]
         batched["speedup_vs_precision_single"] = batched["value"] / line["precision_form"]["value"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -433,6 +445,98 @@ def bench_batched(args, w, lat, stream, world):
                       "all RHS, per-RHS scalars and convergence"}
 
 
+def bench_precision_48(args, world):
+    """SURVEY config 3: 48^3x96, seeded SU(3) + 5 APE steps (generated on the
+    GPU), csw 1.7, kappa 0.1365 and 0.1355, Gaussian source, 1e-10.  Per
+    kappa: the plain solver (FP64 outer / FP32 SAP inner), the precision form
+    on one RHS and on a 2-RHS handle (FP16-storage SAP, FP64 outer with
+    reliable restarts), each with its true residual and its error against a
+    reference solution of the same system solved to 1e-13 in FP64 outer."""
+    import torch
+
+    import qws_b200
+
+    L, NB = (48, 48, 48, 96), (2, 1, 1, 1)
+    stream = torch.cuda.Stream()
+    out = {"lattice": "48x48x48x96", "block_grid": list(NB), "tol": 1e-10, "per_kappa": []}
+    b = qws_b200.gen_source(L, 12, "gauss")
+    b2 = np.stack([b, qws_b200.gen_source(L, 13, "gauss")])
+    lat = qws_b200.Lattice(L, NB, tbc=-1, kappa=0.1365, stream=stream)
+    try:
+        out["plaquette"] = lat.gen_gauge_device(11, 5, 0.36)
+        for kappa in (0.1365, 0.1355):
+            lat.set_kappa(kappa)
+            lat.build_clover(1.7)
+            with torch.cuda.stream(stream):
+                bd = lat.to_device(b)
+                x = lat.empty("f64")
+                xref = lat.empty("f64")
+                lat.bicgstab_dd_mix(xref, bd, 1e-13, 200, 1e-6, 50)
+                nref = torch.linalg.vector_norm(xref).item()
+
+                def timed(fn, reps):
+                    fn()
+                    torch.cuda.synchronize()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    for _ in range(reps):
+                        st = fn()
+                    e1.record(stream)
+                    torch.cuda.synchronize()
+                    return e0.elapsed_time(e1) / reps, st
+
+                def plain():
+                    x.zero_()
+                    return lat.bicgstab_dd_mix(x, bd, 1e-10, 200, 1e-6, 50)
+
+                def prec():
+                    x.zero_()
+                    return lat.bicgstab_dd_mix2_hf(x, bd, 1e-10, 200, 1e-6, 50, reliable=5)
+
+                ms_p, st_p = timed(plain, 2)
+                err_p = (torch.linalg.vector_norm(x - xref) / nref).item()
+                res_p = lat.true_residual(x, bd)
+                ms_h, st_h = timed(prec, 2)
+                err_h = (torch.linalg.vector_norm(x - xref) / nref).item()
+                res_h = lat.true_residual(x, bd)
+                del x
+                B = lat.batch(2, stream=stream)
+                bb = B.to_device(b2)
+                xb = B.empty("f64")
+
+                def batched():
+                    xb.zero_()
+                    return B.bicgstab_dd_mix2_hf(xb, bb, 1e-10, 200, 1e-6, 50, reliable=5)
+
+                ms_b, _ = timed(batched, 2)
+                res_b = max(B.true_residual(xb, bb))
+                xr = lat.to_host(xref)  # RHS 0 of the batch is the single solve's source
+                err_b = float(np.linalg.norm(B.to_host(xb)[0] - xr) / np.linalg.norm(xr))
+                del xr
+                B.close()
+                del xb, bb, bd, xref
+                torch.cuda.empty_cache()
+            plain_sps = 1e3 / ms_p
+            out["per_kappa"].append({
+                "kappa": kappa,
+                "plain": {"solves_per_s": plain_sps, "true_rel_resid": res_p,
+                          "rel_error_vs_reference": err_p, "outer_iters": st_p["outer_iters"],
+                          "inner_iters": st_p["inner_iters"]},
+                "precision_single": {"solves_per_s": 1e3 / ms_h, "true_rel_resid": res_h,
+                                     "rel_error_vs_reference": err_h,
+                                     "outer_iters": st_h["outer_iters"],
+                                     "inner_iters": st_h["inner_iters"],
+                                     "speedup_vs_plain": (1e3 / ms_h) / plain_sps},
+                "precision_batched_2rhs": {"solves_per_s": 2e3 / ms_b,
+                                           "max_true_rel_resid": res_b,
+                                           "rel_error_vs_reference": err_b,
+                                           "speedup_vs_plain": (2e3 / ms_b) / plain_sps}})
+    finally:
+        lat.close()
+        torch.cuda.empty_cache()
+    return out
+
+
 def bench_serving(args):
     """A short window of the serving workload: Poisson arrivals, volumes
     16^3x32 / 24^3x48 / 32^3x64 / 48^3x96 (weights .4/.3/.2/.1), kappa uniform
@@ -501,6 +605,8 @@ def main():
                     help="arrival rate of the serving sub-result (0: skip)")
     ap.add_argument("--serve-window", type=float, default=10.0)
     ap.add_argument("--serve-gauges", type=int, default=4)
+    ap.add_argument("--config3", type=int, default=1,
+                    help="run the 48^3x96 precision-form comparison (0: skip)")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
