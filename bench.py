@@ -55,6 +55,14 @@ REF_COUNTS = {
 }
 
 
+_T0 = time.time()
+
+
+def progress(msg):
+    """Phase markers on stderr (the JSON line alone goes to stdout)."""
+    print(f"[bench {time.time() - _T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -185,6 +193,7 @@ def bench_ours(args, w, name):
     import qws_b200
 
     world, rank, local = dist_setup(args.gpus)
+    progress(f"fields for {name}")
     U, C, b, plaq, t_gen = make_fields(w)
     stream = torch.cuda.Stream()
     lat = qws_b200.Lattice(w["L"], w["NB"], tbc=w["tbc"], kappa=w["kappa"], stream=stream)
@@ -207,6 +216,7 @@ def bench_ours(args, w, name):
         true_rel = lat.true_residual(xd, bd)
         c0 = lat.counters()
 
+        progress("warm-up done; timed plain solves")
         # ---- device-resident timed region (production configuration: the
         #      SAP launch sequences replayed from CUDA graphs) ------------------
         clocks = ClockSampler(local)
@@ -237,6 +247,7 @@ def bench_ours(args, w, name):
         kstats = lat.kernel_stats()
         lat.kernel_timing(False)
 
+        progress("end-to-end solves")
         # ---- end to end through the public API with host buffers --------------
         pinned = torch.from_numpy(b).pin_memory()
         host_b = pinned.numpy()
@@ -284,6 +295,7 @@ def bench_ours(args, w, name):
         except Exception as e:  # noqa: BLE001
             return {"error": f"{type(e).__name__}: {str(e)[-400:]}"}
 
+    progress("batched")
     batched = sub(bench_batched, args, w, lat, stream, world) if args.batch > 1 else None
     serving = None
     precision_48 = None
@@ -292,9 +304,12 @@ def bench_ours(args, w, name):
         del xd, bd, xh, bh
         torch.cuda.empty_cache()
     if args.serve_rate > 0 and world == 1:
+        progress("serving window")
         serving = sub(bench_serving, args)
     if args.config3 and world == 1:
+        progress("48^3x96 precision comparison")
         precision_48 = sub(bench_precision_48, args, world)
+    progress("done with GPU parts")
 
     per_solve = {k: (c1[k] - c0[k]) / args.steps for k in c1}
     inner_iters = sum(s["inner_iters"] for s in stats) / len(stats)

@@ -27,6 +27,30 @@
 
 namespace qwsg {
 
+// n / d for 0 <= n < 2^31 by a multiply-high (Granlund-Montgomery): with
+// s = ceil(log2 d) and m = floor(2^(32+s) / d) + 1 - 2^32 (fits 32 bits),
+// floor(n / d) = (umulhi(n, m) + n) >> s exactly for every n < 2^32; the sum
+// cannot overflow for n < 2^31.  Replaces the integer divisions of the site
+// decoding, which ran in every hop thread.
+struct FastDiv {
+  unsigned m;
+  int s;
+};
+inline FastDiv make_fastdiv(int d) {
+  int s = 0;
+  while ((1u << s) < (unsigned)d) s++;
+  const unsigned long long m = ((1ull << (32 + s)) / (unsigned long long)d) + 1 - (1ull << 32);
+  return {(unsigned)m, s};
+}
+__host__ __device__ __forceinline__ int fdiv(int n, FastDiv f) {
+#ifdef __CUDA_ARCH__
+  const unsigned hi = __umulhi((unsigned)n, f.m);
+#else
+  const unsigned hi = (unsigned)(((unsigned long long)(unsigned)n * f.m) >> 32);
+#endif
+  return (int)((hi + (unsigned)n) >> f.s);
+}
+
 struct Geom {
   int L[4];    // global extents
   int B[4];    // block extents
@@ -45,6 +69,8 @@ struct Geom {
   // load.  Gauge and clover fields are per site (stride pad).
   int nr;
   int lgnr;
+  // multipliers for the divisions of the site decoding
+  FastDiv fB[4], fVb, fnbh0, fNB1, fNB2;
 };
 
 // plane stride of spinor fields and the entry of (site, rhs)
@@ -62,20 +88,22 @@ struct Site {
 __device__ __forceinline__ void decode_site(const Geom& G, int g, Site& s) {
   s.col = g >= G.Vh;
   int rem = g - s.col * G.Vh;
-  int k = rem / G.Vb;
+  int k = fdiv(rem, G.fVb);
   int t = rem - k * G.Vb;
-  s.lc[0] = t % G.B[0];
-  t /= G.B[0];
-  s.lc[1] = t % G.B[1];
-  t /= G.B[1];
-  s.lc[2] = t % G.B[2];
-  s.lc[3] = t / G.B[2];
-  int q = k / G.nbh0;
+  int t1 = fdiv(t, G.fB[0]);
+  s.lc[0] = t - t1 * G.B[0];
+  int t2 = fdiv(t1, G.fB[1]);
+  s.lc[1] = t1 - t2 * G.B[1];
+  int t3 = fdiv(t2, G.fB[2]);
+  s.lc[2] = t2 - t3 * G.B[2];
+  s.lc[3] = t3;
+  int q = fdiv(k, G.fnbh0);
   int r = k - q * G.nbh0;
-  s.bc[1] = q % G.NB[1];
-  q /= G.NB[1];
-  s.bc[2] = q % G.NB[2];
-  s.bc[3] = q / G.NB[2];
+  int q1 = fdiv(q, G.fNB1);
+  s.bc[1] = q - q1 * G.NB[1];
+  int q2 = fdiv(q1, G.fNB2);
+  s.bc[2] = q1 - q2 * G.NB[2];
+  s.bc[3] = q2;
   s.bc[0] = 2 * r + ((s.col + s.bc[1] + s.bc[2] + s.bc[3]) & 1);
 }
 
@@ -84,7 +112,7 @@ __host__ __device__ __forceinline__ int dd_index(const Geom& G, const int x[4]) 
   int bc[4], lc[4];
 #pragma unroll
   for (int mu = 0; mu < 4; mu++) {
-    bc[mu] = x[mu] / G.B[mu];
+    bc[mu] = fdiv(x[mu], G.fB[mu]);
     lc[mu] = x[mu] - bc[mu] * G.B[mu];
   }
   int col = (bc[0] + bc[1] + bc[2] + bc[3]) & 1;
@@ -313,11 +341,17 @@ struct IO<H16> {
     float n = 0;
 #pragma unroll
     for (int j = 0; j < 24; j++) n = fmaxf(n, fabsf(v[j]));
-    const float inv = n > 0 ? 1.0f / n : 0.0f;
+    // A site whose largest component is below 1e-30 is stored as zero: 1/n
+    // overflows FP32 for denormal n (0 * inf would give NaN), and such
+    // entries sit far below what FP16 storage resolves next to the O(1)
+    // entries of the normalised fields the SAP works on (a point source's
+    // solution decays below FP32's normal range across a large lattice).
+    const bool keep = n >= 1e-30f;
+    const float inv = keep ? 1.0f / n : 0.0f;
     uint2* q = reinterpret_cast<uint2*>(p);
 #pragma unroll
     for (int j = 0; j < 6; j++) q[(size_t)j * pad + g] = pack4(v + 4 * j, inv);
-    reinterpret_cast<float*>(q + (size_t)6 * pad)[g] = n;
+    reinterpret_cast<float*>(q + (size_t)6 * pad)[g] = keep ? n : 0.0f;
   }
   __device__ __forceinline__ static void load_link(const __half* __restrict__ U, int pad, int mu,
                                                    int g, float u[18]) {

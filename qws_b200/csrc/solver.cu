@@ -166,6 +166,11 @@ Ctx::Ctx(const int L[4], const int NB[4], int tbc, int nrhs) {
   G.str[1] = G.B[0];
   G.str[2] = G.B[0] * G.B[1];
   G.str[3] = G.B[0] * G.B[1] * G.B[2];
+  for (int mu = 0; mu < 4; mu++) G.fB[mu] = make_fastdiv(G.B[mu]);
+  G.fVb = make_fastdiv(G.Vb);
+  G.fnbh0 = make_fastdiv(G.nbh0);
+  G.fNB1 = make_fastdiv(G.NB[1]);
+  G.fNB2 = make_fastdiv(G.NB[2]);
   QWSG_CUDA(cudaGetDevice(&device));
   QWSG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   own_stream = true;

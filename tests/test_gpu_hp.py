@@ -117,3 +117,27 @@ def test_hp_golden():
                              (np.sum(b * b), np.sum(r * r), np.sum(x * x)), vals):
         assert check_sh_ok(nm_, float(val), ref), (nm_, val, ref)
     lat.close()
+
+
+def test_fp16_storage_of_vanishing_sites():
+    """Sites whose components are FP32 denormals (a point source's solution
+    far from the source on a large lattice) are stored as zero, never as
+    NaN: the FP16 SAP of such a field stays finite and matches the FP32 SAP
+    of the same field (the tiny sites contribute nothing either way)."""
+    import qws_b200
+
+    L = (8, 8, 8, 16)
+    U, _ = qws_b200.gen_gauge(L, 3, 5, 0.36)
+    C = qws_b200.gen_clover(U, L, 1.7, 0.1365)
+    lat = qws_b200.Lattice(L, (2, 2, 2, 2), tbc=-1, kappa=0.1365)
+    try:
+        lat.load_fields(U, C)
+        v = np.full((int(np.prod(L)), 24), 1e-39, np.float32)  # denormal everywhere
+        v[0] = 1.0
+        x = lat.to_device(v)
+        h = lat.to_host(lat.prec_h(x, 4, 2))
+        f = lat.to_host(lat.prec(x, 3, 2))  # the same sweep count: nsap-1 sweeps + final
+        assert np.all(np.isfinite(h))
+        assert rel(h, f) < 1e-2
+    finally:
+        lat.close()
