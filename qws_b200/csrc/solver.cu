@@ -641,6 +641,7 @@ int bicgstab_precdd_s(Ctx& c, float* x, const float* b, double tol, int maxiter,
     blas_bicg_update<float>(G, x, r, p, q, alpha.real(), alpha.imag(), nullptr, c.d_res, c.rb,
                             c.st);
     rnorm = (float)c.fetch(1)[0];
+    if (!std::isfinite(rnorm)) throw Error(3, "solver: non-finite residual norm");
     if (std::sqrt(rnorm / bnorm) < tol) {
       done = iter + 1;
       break;
@@ -654,6 +655,7 @@ int bicgstab_precdd_s(Ctx& c, float* x, const float* b, double tol, int maxiter,
     blas_bicg_update<float>(G, x, r, r, t, omega.real(), omega.imag(), r0, c.d_res, c.rb, c.st);
     h = c.fetch(3);
     rnorm = (float)h[0];
+    if (!std::isfinite(rnorm)) throw Error(3, "solver: non-finite residual norm");
     rho = std::complex<float>((float)h[1], (float)h[2]);
     if (std::sqrt(rnorm / bnorm) < tol) {
       done = iter + 1;
@@ -696,6 +698,7 @@ int bicgstab_precdd_s_h(Ctx& c, float* x, const float* b, double tol, int maxite
     blas_bicg_update<float>(G, x, r, w, q, alpha.real(), alpha.imag(), nullptr, c.d_res, c.rb,
                             c.st);
     rnorm = (float)c.fetch(1)[0];
+    if (!std::isfinite(rnorm)) throw Error(3, "solver: non-finite residual norm");
     if (std::sqrt(rnorm / bnorm) < tol) {
       done = iter + 1;
       break;
@@ -710,6 +713,7 @@ int bicgstab_precdd_s_h(Ctx& c, float* x, const float* b, double tol, int maxite
     blas_bicg_update<float>(G, x, r, w, t, omega.real(), omega.imag(), r0, c.d_res, c.rb, c.st);
     h = c.fetch(3);
     rnorm = (float)h[0];
+    if (!std::isfinite(rnorm)) throw Error(3, "solver: non-finite residual norm");
     rho = std::complex<float>((float)h[1], (float)h[2]);
     if (std::sqrt(rnorm / bnorm) < tol) {
       done = iter + 1;
@@ -773,6 +777,7 @@ static int outer_loop(Ctx& c, double* x, const double* b, double tol, int iter_b
     blas_bicg_update<double>(G, x, r, u, q, alpha.real(), alpha.imag(), nullptr, c.d_res, c.rb,
                              c.st);
     rnorm = c.fetch(1)[0];
+    if (!std::isfinite(rnorm)) throw Error(3, "solver: non-finite residual norm");
     if (hist && nh < hist_len) hist[nh++] = std::sqrt(rnorm / bnorm);
     if (std::sqrt(rnorm / bnorm) < tol) {
       conv = iter;
@@ -787,6 +792,7 @@ static int outer_loop(Ctx& c, double* x, const double* b, double tol, int iter_b
     blas_bicg_update<double>(G, x, r, u, t, omega.real(), omega.imag(), r0, c.d_res, c.rb, c.st);
     h = c.fetch(3);
     rnorm = h[0];
+    if (!std::isfinite(rnorm)) throw Error(3, "solver: non-finite residual norm");
     rho = std::complex<double>(h[1], h[2]);
     if (hist && nh < hist_len) hist[nh++] = std::sqrt(rnorm / bnorm);
     if (std::sqrt(rnorm / bnorm) < tol) {

@@ -78,6 +78,7 @@ int inner_solve(Ctx& c, float* x, const float* b, double tol, int maxiter, int n
     for (int k = 0; k < nr; k++) {
       if (!act[k]) continue;
       rnorm[k] = (float)h[4 * k];
+      if (!std::isfinite(rnorm[k])) throw Error(3, "solver: non-finite residual norm");
       if (std::sqrt(rnorm[k] / bnorm[k]) < tol) {
         iters[k] = iter + 1;
         act[k] = false;
@@ -110,6 +111,7 @@ int inner_solve(Ctx& c, float* x, const float* b, double tol, int maxiter, int n
     for (int k = 0; k < nr; k++) {
       if (!act[k]) continue;  // frozen: p = r (beta = omega = 0), harmless
       rnorm[k] = (float)h[4 * k];
+      if (!std::isfinite(rnorm[k])) throw Error(3, "solver: non-finite residual norm");
       rho[k] = cf((float)h[4 * k + 1], (float)h[4 * k + 2]);
       if (std::sqrt(rnorm[k] / bnorm[k]) < tol) {
         iters[k] = iter + 1;
@@ -208,6 +210,7 @@ void outer_loop(Ctx& c, double* x, const double* b, double tol, int iter_begin, 
     for (int k = 0; k < nr; k++) {
       if (!act[k]) continue;
       rnorm[k] = h[4 * k];
+      if (!std::isfinite(rnorm[k])) throw Error(3, "solver: non-finite residual norm");
       if (std::sqrt(rnorm[k] / bnorm[k]) < tol) {
         conv[k] = iter;
         act[k] = false;
@@ -234,6 +237,7 @@ void outer_loop(Ctx& c, double* x, const double* b, double tol, int iter_begin, 
     for (int k = 0; k < nr; k++) {
       if (!act[k]) continue;
       rnorm[k] = h[4 * k];
+      if (!std::isfinite(rnorm[k])) throw Error(3, "solver: non-finite residual norm");
       rho[k] = cd(h[4 * k + 1], h[4 * k + 2]);
       if (std::sqrt(rnorm[k] / bnorm[k]) < tol) {
         conv[k] = iter;
