@@ -198,7 +198,6 @@ def bench_ours(args, w, name):
     stream = torch.cuda.Stream()
     lat = qws_b200.Lattice(w["L"], w["NB"], tbc=w["tbc"], kappa=w["kappa"], stream=stream)
     lat.load_fields(U, C)
-    del U, C
     with torch.cuda.stream(stream):
         bd = lat.to_device(b)
         xd = lat.empty("f64")
@@ -285,9 +284,13 @@ def bench_ours(args, w, name):
         hstats = [solve_hf() for _ in range(args.steps)]
         h1.record(stream)
         torch.cuda.synchronize()
-        hf_ms = allreduce_max(h0.elapsed_time(h1), world)
-        hf_true = lat.true_residual(xd, bd)
+        hf_ref_ms = allreduce_max(h0.elapsed_time(h1), world)
+        hf_ref_true = lat.true_residual(xd, bd)
+        hf_ref_iters = (sum(s["outer_iters"] for s in hstats) / len(hstats),
+                        sum(s["inner_iters"] for s in hstats) / len(hstats))
     e2e_true = lat.true_residual(xh, bh)
+    del xh, bh
+
     # sub-results: a failure is reported in the line, it does not lose the line
     def sub(fn, *a):
         try:
@@ -295,17 +298,58 @@ def bench_ours(args, w, name):
         except Exception as e:  # noqa: BLE001
             return {"error": f"{type(e).__name__}: {str(e)[-400:]}"}
 
+    # ---- the precision form in its tuned configuration (SAP block grid,
+    #      sweep counts, CTA size chosen by qws_b200.autotune for this
+    #      lattice), on the same fields and source -----------------------------
+    progress("autotune")
+    tuned = sub(tuned_config, args, w["L"], rank)
+    tl = lat
+    if "NB" in tuned and tuple(tuned["NB"]) != tuple(w["NB"]):
+        tl = qws_b200.Lattice(w["L"], tuned["NB"], tbc=w["tbc"], kappa=w["kappa"], stream=stream)
+        tl.load_fields(U, C)
+    del U, C
+    cfg = {k: tuned.get(k, w.get(k, d)) for k, d in
+           (("nsap", 4), ("nm", 2), ("hop_threads", 128))}
+    tl.set_hop_threads(cfg["hop_threads"])
+    with torch.cuda.stream(stream):
+        bt = tl.to_device(b) if tl is not lat else bd
+        xt = tl.empty("f64")
+
+        def solve_tuned():
+            xt.zero_()
+            return tl.bicgstab_dd_mix2_hf(xt, bt, w["tol"], w["maxiter"], w["tol_s"],
+                                          w["maxiter_s"], cfg["nsap"], cfg["nm"], reliable=5)
+
+        progress("precision form, tuned")
+        for _ in range(max(1, args.warmup)):
+            solve_tuned()
+        torch.cuda.synchronize()
+        barrier(world)
+        h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        h0.record(stream)
+        hstats = [solve_tuned() for _ in range(args.steps)]
+        h1.record(stream)
+        torch.cuda.synchronize()
+        hf_ms = allreduce_max(h0.elapsed_time(h1), world)
+        hf_true = tl.true_residual(xt, bt)
+
     progress("batched")
-    batched = sub(bench_batched, args, w, lat, stream, world) if args.batch > 1 else None
+    batched = sub(bench_batched, args, w, tl, stream, world, cfg) if args.batch > 1 else None
     serving = None
     precision_48 = None
-    if world == 1 and (args.serve_rate > 0 or args.config3):
+    uneven = None
+    if world == 1 and (args.serve_rate > 0 or args.config3 or args.uneven_workers > 0):
         lat.close()  # the later parts get the HBM to themselves
-        del xd, bd, xh, bh
+        if tl is not lat:
+            tl.close()
+        del xd, bd, xt, bt
         torch.cuda.empty_cache()
     if args.serve_rate > 0 and world == 1:
         progress("serving window")
         serving = sub(bench_serving, args)
+    if args.uneven_workers > 0 and world == 1:
+        progress("48 solves of uneven volume")
+        uneven = sub(bench_uneven, args)
     if args.config3 and world == 1:
         progress("48^3x96 precision comparison")
         precision_48 = sub(bench_precision_48, args, world)
@@ -376,9 +420,17 @@ def bench_ours(args, w, name):
             "true_rel_resid": hf_true,
             "outer_iters": sum(s["outer_iters"] for s in hstats) / len(hstats),
             "inner_iters": sum(s["inner_iters"] for s in hstats) / len(hstats),
+            "config": {"block_grid": list(tl.NB), **cfg},
+            "tuning": tuned,
+            "at_reference_partition": {
+                "block_grid": list(w["NB"]), "nsap": w["nsap"], "nm": w["nm"],
+                "value": world * args.steps / (hf_ref_ms * 1e-3),
+                "speedup_vs_plain": ms_max / hf_ref_ms, "true_rel_resid": hf_ref_true,
+                "outer_iters": hf_ref_iters[0], "inner_iters": hf_ref_iters[1]},
             "method": "bicgstab_dd_mix2_hf: FP64 outer (reliable restarts) / flexible FP32 "
                       "inner / SAP in FP16 storage with per-site FP32 scales (nsap-1 sweeps)"},
         "batched": batched,
+        "uneven_volumes": uneven,
         "serving": serving,
         "precision_48c96": precision_48,
         "gpu_launches": int(n_launches),
@@ -400,6 +452,8 @@ def bench_ours(args, w, name):
         except Exception as e:  # the baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "unit": "solves/s", "error": str(e)[-300:]}
     lat.close()
+    if tl is not lat:
+        tl.close()
     if world > 1:
         import torch.distributed as dist
 
@@ -408,7 +462,20 @@ def bench_ours(args, w, name):
         print(json.dumps(line), flush=True)
 
 
-def bench_batched(args, w, lat, stream, world):
+def tuned_config(args, L, rank):
+    """The autotuner's choice for the precision form on lattice L (the
+    cached entry for this GPU, else a tuning run; --retune forces one)."""
+    from qws_b200 import autotune
+
+    if args.tune == "off":
+        return {"source": "off"}
+    # every rank reads the cache; only rank 0 writes a new entry
+    entry, _ = autotune.autotune(L, "hf", 1, retune=args.tune == "retune", log=progress,
+                                 write=rank == 0)
+    return entry
+
+
+def bench_batched(args, w, lat, stream, world, cfg):
     """Multi-RHS form on the same gauge field: 12 point sources (one per spin x
     colour at the origin) + 4 Z2-noise sources solved together by the
     precision-form solver on one multi-RHS handle (every operator launch
@@ -432,7 +499,7 @@ def bench_batched(args, w, lat, stream, world):
         def solve():
             xb.zero_()
             return B.bicgstab_dd_mix2_hf(xb, bb, w["tol"], w["maxiter"], w["tol_s"],
-                                         w["maxiter_s"], w["nsap"], w["nm"], reliable=5)
+                                         w["maxiter_s"], cfg["nsap"], cfg["nm"], reliable=5)
 
         for _ in range(max(1, min(args.warmup, 2))):
             solve()
@@ -456,99 +523,189 @@ def bench_batched(args, w, lat, stream, world):
             "inner_iters": st["inner_iters"],
             "sources": f"{min(nr, 12)} point (spin x colour at the origin) + "
                        f"{max(0, nr - 12)} Z2 noise",
+            "config": {"block_grid": list(lat.NB), **cfg},
             "method": "bicgstab_dd_mix2_hf on a multi-RHS handle: one launch per operator for "
                       "all RHS, per-RHS scalars and convergence"}
 
 
 def bench_precision_48(args, world):
-    """SURVEY config 3: 48^3x96, seeded SU(3) + 5 APE steps (generated on the
-    GPU), csw 1.7, kappa 0.1365 and 0.1355, Gaussian source, 1e-10.  Per
-    kappa: the plain solver (FP64 outer / FP32 SAP inner), the precision form
-    on one RHS and on a 2-RHS handle (FP16-storage SAP, FP64 outer with
-    reliable restarts), each with its true residual and its error against a
-    reference solution of the same system solved to 1e-13 in FP64 outer."""
+    """48^3x96, seeded SU(3) + 5 APE steps (generated on the GPU), csw 1.7,
+    kappa 0.1365 and 0.1355, Gaussian source, 1e-10.  Per kappa: the plain
+    solver (FP64 outer / FP32 SAP inner) on the reference's one-rank block
+    partition, and the precision form (FP16-storage SAP, FP64 outer with
+    reliable restarts) on one RHS and on a 2-RHS handle, both at the
+    reference partition and in the autotuner's configuration.  Each result
+    has its true residual and its error against a reference solution of the
+    same system solved to 1e-13 (FP64 outer, plain solver).  The two block
+    grids run one after the other (their work buffers do not fit in HBM
+    together); the fields are generated from the same seeds on both."""
     import torch
 
     import qws_b200
 
     L, NB = (48, 48, 48, 96), (2, 1, 1, 1)
+    kappas = (0.1365, 0.1355)
     stream = torch.cuda.Stream()
-    out = {"lattice": "48x48x48x96", "block_grid": list(NB), "tol": 1e-10, "per_kappa": []}
     b = qws_b200.gen_source(L, 12, "gauss")
     b2 = np.stack([b, qws_b200.gen_source(L, 13, "gauss")])
-    lat = qws_b200.Lattice(L, NB, tbc=-1, kappa=0.1365, stream=stream)
-    try:
-        out["plaquette"] = lat.gen_gauge_device(11, 5, 0.36)
-        for kappa in (0.1365, 0.1355):
-            lat.set_kappa(kappa)
-            lat.build_clover(1.7)
-            with torch.cuda.stream(stream):
-                bd = lat.to_device(b)
-                x = lat.empty("f64")
-                xref = lat.empty("f64")
-                lat.bicgstab_dd_mix(xref, bd, 1e-13, 200, 1e-6, 50)
-                nref = torch.linalg.vector_norm(xref).item()
+    tuned = tuned_config(args, L, 0)
+    cfg = {k: tuned.get(k, d) for k, d in (("nsap", 4), ("nm", 2), ("hop_threads", 128))}
+    NBt = tuple(tuned.get("NB", NB))
+    out = {"lattice": "48x48x48x96", "tol": 1e-10, "reference_partition": list(NB),
+           "tuned": {"block_grid": list(NBt), **cfg, "tuning": tuned}, "per_kappa": []}
 
-                def timed(fn, reps):
-                    fn()
-                    torch.cuda.synchronize()
-                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                    e0.record(stream)
-                    for _ in range(reps):
-                        st = fn()
-                    e1.record(stream)
-                    torch.cuda.synchronize()
-                    return e0.elapsed_time(e1) / reps, st
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            st = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps, st
 
-                def plain():
-                    x.zero_()
-                    return lat.bicgstab_dd_mix(x, bd, 1e-10, 200, 1e-6, 50)
+    def rel_err(xh, xr):
+        return float(np.linalg.norm(xh - xr) / np.linalg.norm(xr))
 
-                def prec():
-                    x.zero_()
-                    return lat.bicgstab_dd_mix2_hf(x, bd, 1e-10, 200, 1e-6, 50, reliable=5)
+    def precision_runs(lat, nsap, nm, xr):
+        """single-RHS and 2-RHS precision form on lat; errors against xr."""
+        with torch.cuda.stream(stream):
+            bd = lat.to_device(b)
+            x = lat.empty("f64")
 
-                ms_p, st_p = timed(plain, 2)
-                err_p = (torch.linalg.vector_norm(x - xref) / nref).item()
-                res_p = lat.true_residual(x, bd)
-                ms_h, st_h = timed(prec, 2)
-                err_h = (torch.linalg.vector_norm(x - xref) / nref).item()
-                res_h = lat.true_residual(x, bd)
-                del x
-                B = lat.batch(2, stream=stream)
+            def prec():
+                x.zero_()
+                return lat.bicgstab_dd_mix2_hf(x, bd, 1e-10, 200, 1e-6, 50, nsap, nm, reliable=5)
+
+            ms_h, st_h = timed(prec, 2)
+            single = {"ms": ms_h, "true_rel_resid": lat.true_residual(x, bd),
+                      "rel_error_vs_reference": rel_err(lat.to_host(x), xr),
+                      "outer_iters": st_h["outer_iters"], "inner_iters": st_h["inner_iters"]}
+            del x, bd
+            torch.cuda.empty_cache()
+            B = lat.batch(2, stream=stream)
+            try:
                 bb = B.to_device(b2)
                 xb = B.empty("f64")
 
                 def batched():
                     xb.zero_()
-                    return B.bicgstab_dd_mix2_hf(xb, bb, 1e-10, 200, 1e-6, 50, reliable=5)
+                    return B.bicgstab_dd_mix2_hf(xb, bb, 1e-10, 200, 1e-6, 50, nsap, nm,
+                                                 reliable=5)
 
                 ms_b, _ = timed(batched, 2)
-                res_b = max(B.true_residual(xb, bb))
-                xr = lat.to_host(xref)  # RHS 0 of the batch is the single solve's source
-                err_b = float(np.linalg.norm(B.to_host(xb)[0] - xr) / np.linalg.norm(xr))
-                del xr
+                pair = {"ms": ms_b, "max_true_rel_resid": max(B.true_residual(xb, bb)),
+                        "rel_error_vs_reference": rel_err(B.to_host(xb)[0], xr)}
+                del xb, bb
+            finally:
                 B.close()
-                del xb, bb, bd, xref
                 torch.cuda.empty_cache()
-            plain_sps = 1e3 / ms_p
-            out["per_kappa"].append({
-                "kappa": kappa,
-                "plain": {"solves_per_s": plain_sps, "true_rel_resid": res_p,
-                          "rel_error_vs_reference": err_p, "outer_iters": st_p["outer_iters"],
-                          "inner_iters": st_p["inner_iters"]},
-                "precision_single": {"solves_per_s": 1e3 / ms_h, "true_rel_resid": res_h,
-                                     "rel_error_vs_reference": err_h,
-                                     "outer_iters": st_h["outer_iters"],
-                                     "inner_iters": st_h["inner_iters"],
-                                     "speedup_vs_plain": (1e3 / ms_h) / plain_sps},
-                "precision_batched_2rhs": {"solves_per_s": 2e3 / ms_b,
-                                           "max_true_rel_resid": res_b,
-                                           "rel_error_vs_reference": err_b,
-                                           "speedup_vs_plain": (2e3 / ms_b) / plain_sps}})
+        return single, pair
+
+    # ---- reference partition: the reference solution, plain, precision form
+    per = {k: {"kappa": k} for k in kappas}
+    xref = {}
+    lat = qws_b200.Lattice(L, NB, tbc=-1, kappa=kappas[0], stream=stream)
+    try:
+        out["plaquette"] = lat.gen_gauge_device(11, 5, 0.36)
+        for kappa in kappas:
+            lat.set_kappa(kappa)
+            lat.build_clover(1.7)
+            with torch.cuda.stream(stream):
+                bd = lat.to_device(b)
+                x = lat.empty("f64")
+                lat.bicgstab_dd_mix(x, bd, 1e-13, 200, 1e-6, 50)
+                xref[kappa] = lat.to_host(x)
+
+                def plain():
+                    x.zero_()
+                    return lat.bicgstab_dd_mix(x, bd, 1e-10, 200, 1e-6, 50)
+
+                ms_p, st_p = timed(plain, 2)
+                per[kappa]["plain"] = {
+                    "solves_per_s": 1e3 / ms_p, "true_rel_resid": lat.true_residual(x, bd),
+                    "rel_error_vs_reference": rel_err(lat.to_host(x), xref[kappa]),
+                    "outer_iters": st_p["outer_iters"], "inner_iters": st_p["inner_iters"]}
+                del x, bd
+                torch.cuda.empty_cache()
+            single, pair = precision_runs(lat, 4, 2, xref[kappa])
+            per[kappa]["precision_reference_partition"] = {
+                "single": dict(single, solves_per_s=1e3 / single.pop("ms")),
+                "batched_2rhs": dict(pair, solves_per_s=2e3 / pair.pop("ms"))}
     finally:
         lat.close()
         torch.cuda.empty_cache()
+
+    # ---- tuned configuration: the precision form ------------------------------
+    lat = qws_b200.Lattice(L, NBt, tbc=-1, kappa=kappas[0], stream=stream)
+    try:
+        lat.gen_gauge_device(11, 5, 0.36)
+        lat.set_hop_threads(cfg["hop_threads"])
+        for kappa in kappas:
+            lat.set_kappa(kappa)
+            lat.build_clover(1.7)
+            single, pair = precision_runs(lat, cfg["nsap"], cfg["nm"], xref[kappa])
+            plain_sps = per[kappa]["plain"]["solves_per_s"]
+            s_sps, p_sps = 1e3 / single.pop("ms"), 2e3 / pair.pop("ms")
+            per[kappa]["precision_single"] = dict(single, solves_per_s=s_sps,
+                                                  speedup_vs_plain=s_sps / plain_sps)
+            per[kappa]["precision_batched_2rhs"] = dict(pair, solves_per_s=p_sps,
+                                                        speedup_vs_plain=p_sps / plain_sps)
+    finally:
+        lat.close()
+        torch.cuda.empty_cache()
+    out["per_kappa"] = [per[k] for k in kappas]
+    return out
+
+
+def bench_uneven(args):
+    """48 independent solves, volumes drawn uniformly from 8^4, 12^3x24,
+    16^3x32 and 24^3x48, each on its own seeded gauge field (generated on the
+    GPU), csw 1.7, kappa 0.1365, Gaussian sources, 1e-10, precision form.
+    All 48 are submitted at once to the solve service, whose workers run
+    them concurrently on separate CUDA streams (the small lattices fill a
+    fraction of the SMs each); a cold pass makes the fields resident, the
+    timed warm pass solves the same requests on resident fields.  The same
+    warm pass with one worker (solves one after another) is the reference
+    point for the overlap."""
+    import qws_b200
+    from qws_b200 import serve
+
+    vols = [(8, 8, 8, 8), (12, 12, 12, 24), (16, 16, 16, 32), (24, 24, 24, 48)]
+    rng = np.random.default_rng(4)
+    picks = [vols[int(rng.integers(len(vols)))] for _ in range(48)]
+    src = {L: qws_b200.gen_source(L, 77, "gauss") for L in vols}
+    out = {"solves": 48, "volumes": {"x".join(map(str, L)): picks.count(L) for L in vols}}
+    for workers in (args.uneven_workers, 1):
+        svc = serve.Service(serve.seeded_gauge(), budget_bytes=150e9, workers=workers,
+                            max_batch=1)
+        try:
+            def run():
+                t0 = time.monotonic()
+                reqs = [svc.submit(serve.Request(L=L, gauge=i, kappa=0.1365, csw=1.7, tol=1e-10,
+                                                 source=src[L])) for i, L in enumerate(picks)]
+                for q in reqs:
+                    q.done.wait()
+                t1 = time.monotonic()
+                st = serve.summarize(reqs, t0, t1)
+                return st, t1 - t0
+
+            cold, cold_s = run()
+            warm, warm_s = run()
+        finally:
+            svc.close()
+        out[f"workers_{workers}"] = {
+            "solves_per_s": warm["solves_per_s"], "wall_s": warm_s, "cold_wall_s": cold_s,
+            "p50_ms": warm["p50_ms"], "max_true_rel_resid": warm["max_true_rel_resid"],
+            "errors": warm["errors"] + cold["errors"], "above_tol": warm["above_tol"]}
+    c, one = out[f"workers_{args.uneven_workers}"], out["workers_1"]
+    out["value"] = c["solves_per_s"]
+    out["unit"] = "solves/s"
+    out["speedup_vs_one_at_a_time"] = c["solves_per_s"] / one["solves_per_s"]
+    out["method"] = ("qws_b200.serve.Service: one resident field per gauge, clover built on the "
+                     "GPU, bicgstab_dd_mix2_hf per request on the worker's stream; the "
+                     "wall-clock span from submission to the last result")
     return out
 
 
@@ -620,6 +777,11 @@ def main():
                     help="arrival rate of the serving sub-result (0: skip)")
     ap.add_argument("--serve-window", type=float, default=10.0)
     ap.add_argument("--serve-gauges", type=int, default=4)
+    ap.add_argument("--uneven-workers", type=int, default=8,
+                    help="workers of the 48 uneven-volume solves sub-result (0: skip)")
+    ap.add_argument("--tune", default="cache", choices=["cache", "retune", "off"],
+                    help="precision-form configuration: the autotuner's cached choice "
+                         "(tuning on a miss), a fresh tuning run, or the reference partition")
     ap.add_argument("--config3", type=int, default=1,
                     help="run the 48^3x96 precision-form comparison (0: skip)")
     args = ap.parse_args()

@@ -152,6 +152,11 @@ void mtilde_dag_vm_(scd_t* out, scd_t* in);
 void mtdagmt_vm_(scd_t* out, scd_t* in);
 /* bicgstab.cc:68 ; x: initial guess in, solution out; conviter = iterations */
 void bicgstab_vm_(scd_t* x, scd_t* b, int* conviter, int* maxiter);
+/* cg.cc:65 (conviter: written here with the last iteration; the reference
+ * leaves it unset) and mcg.cc:65 (xx: *n half arrays of vold scd_t back to
+ * back, zeroed and solved for shifts sigma[0..*n-1], *n <= 32) */
+void cg_vm_(scd_t* x, scd_t* b, int* conviter, int* maxiter);
+void mcg_vm_(scd_t* xx, scd_t* b, int* n, double* sigma, int* maxiter);
 void deo_in_s_(int* pe, int* po, scs_t* out, scs_t* in);
 void dee_deo_in_s_(int* pe, int* po, scs_t* out, scs_t* in);
 void one_minus_dee_deo_in_s_(int* pe, int* po, scs_t* out, scs_t* in, scs_t* in0, float factor);

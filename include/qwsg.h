@@ -195,11 +195,26 @@ int qwsg_mtilde_s(qwsg_lattice* lat, float* out, const float* in);
 /* bicgstab_vm_ (bicgstab.cc:68): BiCGStab on mtilde, x = initial guess in,
  * solution out; iters = the reference's conviter */
 int qwsg_bicgstab_vm(qwsg_lattice* lat, double* x, const double* b, int maxiter, int* iters);
+/* mtdagmt_vm_ (qws.cc:566): mtilde_dag(mtilde(in)) on parity pce */
+int qwsg_mtdagmt_d(qwsg_lattice* lat, double* out, const double* in);
+/* cg_vm_ (cg.cc:65): CG on mtdagmt, x = initial guess in, solution out,
+ * stopping at sqrt(|r|^2/|b|^2) < 1e-14 or iteration maxiter-1; iters = the
+ * last iteration (the reference does not return it) */
+int qwsg_cg_vm(qwsg_lattice* lat, double* x, const double* b, int maxiter, int* iters);
+/* mcg_vm_ (mcg.cc:65): multi-shift CG, (mtdagmt + sigma[k]) x_k = b for
+ * k < nshift (1..32), x_k from zero; x holds the nshift solutions back to
+ * back (24*pad reals each, qwsg_geometry); sigma is a host array */
+int qwsg_mcg_vm(qwsg_lattice* lat, double* x, const double* b, int nshift, const double* sigma,
+                int maxiter, int* iters);
 
 /* CUDA graphs for the SAP preconditioner's launch sequences (default on):
  * captured on first use per buffers/nsap/nm/kappa, replayed afterwards; not
  * used while kernel timing is on or on the legacy default stream */
 int qwsg_set_graphs(qwsg_lattice* lat, int enable);
+/* threads per CTA of the Dirac-operator kernels on this handle (64, 128
+ * (default) or 256); a batch handle starts with its parent's value.  No
+ * counterpart in the reference (its loops are OpenMP threads over sites). */
+int qwsg_set_hop_threads(qwsg_lattice* lat, int threads);
 /* per-kernel CUDA-event timing on the handle's stream: enable (clears the
  * records) or disable; stats fills, per kernel kind k < *nkind, the number
  * of launches, the summed device milliseconds and the summed algorithmic

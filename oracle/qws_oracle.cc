@@ -1088,4 +1088,127 @@ int orc_bicgstab_vm(orc_lat* l, double* x, const double* b, int maxiter) {
   return iter;
 }
 
+// mtdagmt_vm_ (qws.cc:566-571)
+void orc_mtdagmt_d(orc_lat* l, double* out, const double* in) {
+  std::vector<double> t(24 * l->V, 0.0);
+  orc_mtilde_d(l, t.data(), in);
+  orc_mtilde_dag_d(l, out, t.data());
+}
+
+namespace {
+// real inner products over the even sites (the parity the eo solvers use)
+struct EvenSites {
+  std::vector<long> idx;
+  explicit EvenSites(const orc_lat* l) {
+    for (long s = 0; s < l->V; s++) {
+      int c[4];
+      coords(l, s, c);
+      if (((c[0] + c[1] + c[2] + c[3]) & 1) == 0) idx.push_back(s);
+    }
+  }
+  double dot(const double* a, const double* b) const {  // Re <a, b>
+    double acc = 0;
+    for (long s : idx)
+      for (int k = 0; k < 24; k++) acc += a[24 * s + k] * b[24 * s + k];
+    return acc;
+  }
+};
+}  // namespace
+
+// cg_vm_ (cg.cc:65-172): CG on mtdagmt_vm_ for the even parity, x = initial
+// guess in / solution out, iter = 1..maxiter-1, stops when
+// sqrt(|r|^2/|b|^2) < 1e-14 after the x/r update; returns the last iter
+int orc_cg_vm(orc_lat* l, double* x, const double* b, int maxiter) {
+  const long n = 24 * l->V;
+  EvenSites ev(l);
+  std::vector<double> q(n, 0.0), r(n, 0.0), p(n, 0.0);
+  orc_mtdagmt_d(l, q.data(), x);
+  for (long s : ev.idx)
+    for (int k = 0; k < 24; k++) {
+      long i = 24 * s + k;
+      r[i] = b[i] - q[i];
+      p[i] = r[i];
+    }
+  const double bnorm = ev.dot(b, b);
+  double rho0 = ev.dot(r.data(), r.data());
+  int iter;
+  for (iter = 1; iter < maxiter; iter++) {
+    orc_mtdagmt_d(l, q.data(), p.data());
+    const double alpha = rho0 / ev.dot(p.data(), q.data());
+    for (long s : ev.idx)
+      for (int k = 0; k < 24; k++) {
+        long i = 24 * s + k;
+        x[i] += alpha * p[i];
+        r[i] -= alpha * q[i];
+      }
+    const double rnorm = ev.dot(r.data(), r.data());
+    if (std::sqrt(rnorm / bnorm) < 1e-14) break;
+    const double beta = rnorm / rho0;
+    rho0 = rnorm;
+    for (long s : ev.idx)
+      for (int k = 0; k < 24; k++) {
+        long i = 24 * s + k;
+        p[i] = r[i] + beta * p[i];
+      }
+  }
+  return iter;
+}
+
+// mcg_vm_ (mcg.cc:65-219): multi-shift CG, (mtdagmt + sigma_k) x_k = b,
+// x_k from zero (X: n natural-layout fields back to back); the shifted
+// coefficients follow mcg.cc:141-147 and 196-200; returns the last iter.
+// One deliberate difference: a shift whose residual |zeta_k| |r| / |b| is
+// below 1e-14 stops being updated.  The reference updates it to the end,
+// and once zeta_k underflows to zero its next ratio is 0/0 and the
+// solution turns into NaN; before that point the two agree.
+int orc_mcg_vm(orc_lat* l, double* X, const double* b, int n, const double* sigma, int maxiter) {
+  const long N = 24 * l->V;
+  EvenSites ev(l);
+  std::vector<double> q(N, 0.0), r(N, 0.0), p(N, 0.0), pp((size_t)N * n, 0.0);
+  for (long s : ev.idx)
+    for (int k = 0; k < 24; k++) r[24 * s + k] = p[24 * s + k] = b[24 * s + k];
+  for (long i = 0; i < N * n; i++) X[i] = 0.0;
+  for (int k = 0; k < n; k++)
+    for (long i = 0; i < N; i++) pp[(size_t)k * N + i] = r[i];
+  const double bnorm = ev.dot(b, b);
+  double rho0 = bnorm, alpha0 = 1.0, beta = 0.0;
+  std::vector<double> z0(n, 1.0), z1(n, 1.0), z2(n);
+  std::vector<char> active(n, 1);
+  int iter;
+  for (iter = 1; iter < maxiter; iter++) {
+    orc_mtdagmt_d(l, q.data(), p.data());
+    const double alpha = -rho0 / ev.dot(p.data(), q.data());
+    for (long s : ev.idx)
+      for (int k = 0; k < 24; k++) r[24 * s + k] += alpha * q[24 * s + k];
+    const double rnorm = ev.dot(r.data(), r.data());
+    for (int k = 0; k < n; k++) {
+      if (!active[k]) continue;
+      z2[k] = z1[k] * z0[k] * alpha0 /
+              (alpha * beta * (z0[k] - z1[k]) + z0[k] * alpha0 * (1.0 - sigma[k] * alpha));
+      const double c = alpha * z2[k] / z1[k];
+      double* xk = X + (size_t)k * N;
+      const double* pk = pp.data() + (size_t)k * N;
+      for (long s : ev.idx)
+        for (int j = 0; j < 24; j++) xk[24 * s + j] -= c * pk[24 * s + j];
+      if (std::fabs(z2[k]) * std::sqrt(rnorm / bnorm) < 1e-14) active[k] = 0;
+    }
+    if (std::sqrt(rnorm / bnorm) < 1e-14) break;
+    beta = rnorm / rho0;
+    rho0 = rnorm;
+    for (long s : ev.idx)
+      for (int k = 0; k < 24; k++) p[24 * s + k] = r[24 * s + k] + beta * p[24 * s + k];
+    for (int k = 0; k < n; k++) {
+      if (!active[k]) continue;
+      const double d = beta * (z2[k] / z1[k]) * (z2[k] / z1[k]);
+      double* pk = pp.data() + (size_t)k * N;
+      for (long s : ev.idx)
+        for (int j = 0; j < 24; j++) pk[24 * s + j] = d * pk[24 * s + j] + z2[k] * r[24 * s + j];
+      z0[k] = z1[k];
+      z1[k] = z2[k];
+    }
+    alpha0 = alpha;
+  }
+  return iter;
+}
+
 }  // extern "C"

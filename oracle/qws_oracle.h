@@ -92,6 +92,16 @@ int orc_bicgstab_precdd_s_h(orc_lat*, float* x, const float* b, double tol, int 
 void orc_bicgstab_dd_mix2_hf(orc_lat*, double* x, const double* b, double tol, int maxiter,
                              double tol_s, int maxiter_s, int nsap, int nm, double* stats);
 
+/* ---- even-odd (site parity) family, natural layout, parity 0 = pce ------ */
+void orc_mtilde_d(orc_lat*, double* out, const double* in);      /* qws.cc:551 */
+void orc_mtilde_dag_d(orc_lat*, double* out, const double* in);  /* qws.cc:557 */
+void orc_mtdagmt_d(orc_lat*, double* out, const double* in);     /* qws.cc:566 */
+int orc_bicgstab_vm(orc_lat*, double* x, const double* b, int maxiter);  /* bicgstab.cc:68 */
+/* cg_vm_ (cg.cc:65): x = initial guess in, solution out, returns the last
+ * iteration; mcg_vm_ (mcg.cc:65): X holds n solutions back to back, zeroed first */
+int orc_cg_vm(orc_lat*, double* x, const double* b, int maxiter);
+int orc_mcg_vm(orc_lat*, double* X, const double* b, int n, const double* sigma, int maxiter);
+
 /* ---- norms -------------------------------------------------------------- */
 double orc_norm2_d(const double* v, long n);
 double orc_norm2_s(const float* v, long n);

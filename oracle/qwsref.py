@@ -105,6 +105,11 @@ def load_oracle():
     lib.orc_mtilde_dag_d.argtypes = [vp, _dp, _dp]
     lib.orc_bicgstab_vm.restype = ctypes.c_int
     lib.orc_bicgstab_vm.argtypes = [vp, _dp, _dp, ctypes.c_int]
+    lib.orc_mtdagmt_d.argtypes = [vp, _dp, _dp]
+    lib.orc_cg_vm.restype = ctypes.c_int
+    lib.orc_cg_vm.argtypes = [vp, _dp, _dp, ctypes.c_int]
+    lib.orc_mcg_vm.restype = ctypes.c_int
+    lib.orc_mcg_vm.argtypes = [vp, _dp, _dp, ctypes.c_int, _dp, ctypes.c_int]
     lib.orc_norm2_d.restype = ctypes.c_double
     lib.orc_norm2_d.argtypes = [_dp, ctypes.c_long]
     lib.orc_norm2_s.restype = ctypes.c_double
@@ -259,6 +264,23 @@ class Oracle:
         x = np.array(x0, np.float64, copy=True)
         it = self.lib.orc_bicgstab_vm(self.h, dptr(x), dptr(np.ascontiguousarray(b)), maxiter)
         return x, it
+
+    def mtdagmt(self, x):
+        out = self.spinor_d()
+        self.lib.orc_mtdagmt_d(self.h, dptr(out), dptr(np.ascontiguousarray(x)))
+        return out
+
+    def cg_vm(self, b, x0, maxiter):
+        x = np.array(x0, np.float64, copy=True)
+        it = self.lib.orc_cg_vm(self.h, dptr(x), dptr(np.ascontiguousarray(b)), maxiter)
+        return x, it
+
+    def mcg_vm(self, b, sigma, maxiter):
+        sigma = np.ascontiguousarray(sigma, np.float64)
+        X = np.zeros((len(sigma),) + np.shape(b), np.float64)
+        it = self.lib.orc_mcg_vm(self.h, dptr(X), dptr(np.ascontiguousarray(b)), len(sigma),
+                                 dptr(sigma), maxiter)
+        return X, it
 
     def bicgstab_dd_mix(self, b, x0, tol, maxiter, tol_s, maxiter_s, nsap, nm):
         x = np.array(x0, np.float64, copy=True)

@@ -61,6 +61,10 @@ def load_library(path: str | os.PathLike | None = None):
         "qwsg_batch_stats": [vp, ctypes.POINTER(SolveStats), ip],
         "qwsg_build_clover": [vp, c_double],
         "qwsg_set_graphs": [vp, c_int],
+        "qwsg_set_hop_threads": [vp, c_int],
+        "qwsg_mtdagmt_d": [vp, vp, vp],
+        "qwsg_cg_vm": [vp, vp, vp, c_int, ip],
+        "qwsg_mcg_vm": [vp, vp, vp, c_int, dp, c_int, ip],
         "qwsg_gen_gauge_device": [vp, ctypes.c_ulonglong, c_int, c_double,
                                   ctypes.POINTER(c_double)],
         "qwsg_load_gauge": [vp, dp],
@@ -388,6 +392,29 @@ class Lattice:
         _check(self.lib.qwsg_bicgstab_vm(self.h, _ptr(x), _ptr(b), int(maxiter), ctypes.byref(it)))
         return it.value
 
+    def mtdagmt(self, x, out=None):
+        out = self._out(x, out)
+        _check(self.lib.qwsg_mtdagmt_d(self.h, _ptr(out), _ptr(x)))
+        return out
+
+    def cg_vm(self, x, b, maxiter=1000):
+        """CG on mtilde^dag mtilde (parity pce), x = initial guess in, solution out."""
+        it = ctypes.c_int()
+        _check(self.lib.qwsg_cg_vm(self.h, _ptr(x), _ptr(b), int(maxiter), ctypes.byref(it)))
+        return it.value
+
+    def mcg_vm(self, b, sigma, maxiter=1000):
+        """Multi-shift CG: (mtilde^dag mtilde + sigma_k) x_k = b; returns
+        ([x_k device tensors], iterations)."""
+        sigma = np.ascontiguousarray(sigma, np.float64)
+        n = len(sigma)
+        X = self.torch.zeros(n * 24 * self.pad, dtype=self.torch.float64, device="cuda")
+        it = ctypes.c_int()
+        _check(self.lib.qwsg_mcg_vm(self.h, _ptr(X), _ptr(b), n,
+                                    ctypes.c_void_p(sigma.ctypes.data),
+                                    int(maxiter), ctypes.byref(it)))
+        return [X[k * 24 * self.pad:(k + 1) * 24 * self.pad] for k in range(n)], it.value
+
     # ---- precision form (FP16-storage SAP) ----------------------------------
     def prec_h(self, x, nsap=4, nm=2, out=None):
         """M_SAP in FP16 storage (nsap-1 sweeps + final stage); FP32 in/out."""
@@ -420,6 +447,10 @@ class Lattice:
 
     def set_graphs(self, enable=True):
         _check(self.lib.qwsg_set_graphs(self.h, 1 if enable else 0))
+
+    def set_hop_threads(self, threads):
+        """Threads per CTA of the Dirac-operator kernels (64, 128 or 256)."""
+        _check(self.lib.qwsg_set_hop_threads(self.h, int(threads)))
 
     def kernel_timing(self, enable=True):
         _check(self.lib.qwsg_kernel_timing(self.h, 1 if enable else 0))

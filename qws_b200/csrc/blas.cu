@@ -260,6 +260,68 @@ struct OpBicgInit {
   }
 };
 
+// r += a q ; |r|^2
+template <typename R>
+struct OpAxpyNorm {
+  R* r;
+  const R* q;
+  R a;
+  __device__ void operator()(const Geom& G, int g, int, double* acc) const {
+    const int sp = spad(G);
+#pragma unroll
+    for (int j = 0; j < 6; j++) {
+      V4<R> Rr = ld4<R>(r, sp, g, j), Q = ld4(q, sp, g, j);
+      Rr.x += a * Q.x;
+      Rr.y += a * Q.y;
+      Rr.z += a * Q.z;
+      Rr.w += a * Q.w;
+      st4<R>(r, sp, g, j, Rr);
+      acc[0] += (double)Rr.x * Rr.x + (double)Rr.y * Rr.y + (double)Rr.z * Rr.z +
+                (double)Rr.w * Rr.w;
+    }
+  }
+};
+
+// the shift updates of one multi-shift CG iteration, all shifts in one pass
+// over the sites: r and p are read once per site, each shift's x_k and pp_k
+// once (single RHS: g is the site)
+struct OpMshift {
+  double *x, *pp, *p;
+  const double* r;
+  const double* cf;
+  size_t stride;
+  int n;
+  double beta;
+  bool update;
+  __device__ void operator()(const Geom& G, int g, int, double*) const {
+    const int sp = spad(G);
+    for (int j = 0; j < 6; j++) {
+      const V4<double> Rr = ld4<double>(r, sp, g, j);
+      for (int k = 0; k < n; k++) {
+        if (__ldg(cf + 4 * k + 3) == 0.0) continue;  // converged shift
+        const double c = __ldg(cf + 4 * k), z = __ldg(cf + 4 * k + 1), d = __ldg(cf + 4 * k + 2);
+        double* xk = x + k * stride;
+        double* pk = pp + k * stride;
+        V4<double> X = ld4<double>(xk, sp, g, j), P = ld4<double>(pk, sp, g, j);
+        X.x -= c * P.x;
+        X.y -= c * P.y;
+        X.z -= c * P.z;
+        X.w -= c * P.w;
+        st4<double>(xk, sp, g, j, X);
+        if (update)
+          st4<double>(pk, sp, g, j,
+                      {z * Rr.x + d * P.x, z * Rr.y + d * P.y, z * Rr.z + d * P.z,
+                       z * Rr.w + d * P.w});
+      }
+      if (update) {
+        V4<double> P = ld4<double>(p, sp, g, j);
+        st4<double>(p, sp, g, j,
+                    {Rr.x + beta * P.x, Rr.y + beta * P.y, Rr.z + beta * P.z, Rr.w + beta * P.w});
+      }
+    }
+  }
+};
+
 struct OpD2S {
   float* y;
   const double* x;
@@ -375,6 +437,16 @@ void blas_bicg_init(const Geom& G, const R* b, const R* q, R* r, R* p, R* r0, do
                     RedBuf& rb, cudaStream_t st) {
   run<R, 2>(G, OpBicgInit<R>{b, q, r, p, r0}, &rb, res, st);
 }
+template <typename R>
+void blas_axpy_norm(const Geom& G, R* r, const R* q, double a, double* res, RedBuf& rb,
+                    cudaStream_t st) {
+  run<R, 1>(G, OpAxpyNorm<R>{r, q, (R)a}, &rb, res, st);
+}
+void blas_mshift(const Geom& G, double* x, double* pp, int n, const double* r, double* p,
+                 double beta, const double* cf, bool update, cudaStream_t st) {
+  OpMshift op{x, pp, p, r, cf, (size_t)24 * spad(G), n, beta, update};
+  run<double, 0>(G, op, nullptr, nullptr, st);
+}
 void blas_d2s(const Geom& G, float* y, const double* x, double s, cudaStream_t st,
               const double* cf) {
   run<float, 0>(G, OpD2S{y, x, s, cf}, nullptr, nullptr, st);
@@ -396,7 +468,9 @@ void blas_s2d(const Geom& G, double* y, const float* x, double s, cudaStream_t s
   template void blas_bicg_p<R>(const Geom&, R*, const R*, const R*, double, double, double,  \
                                double, cudaStream_t, const double*);                         \
   template void blas_bicg_init<R>(const Geom&, const R*, const R*, R*, R*, R*, double*,      \
-                                  RedBuf&, cudaStream_t);
+                                  RedBuf&, cudaStream_t);                                    \
+  template void blas_axpy_norm<R>(const Geom&, R*, const R*, double, double*, RedBuf&,        \
+                                  cudaStream_t);
 QWSG_INST(float)
 QWSG_INST(double)
 #undef QWSG_INST

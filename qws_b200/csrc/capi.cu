@@ -141,6 +141,7 @@ int qwsg_create_batch(qwsg_lattice** out, qwsg_lattice* parent, int nrhs) {
     if (parent->c->parent) throw Error(1, "qwsg_create_batch: the parent must be a lattice");
     const Geom& G = parent->c->G;
     auto* c = new Ctx(G.L, G.NB, G.tbc, nrhs);
+    c->G.hop_threads = G.hop_threads;
     c->owns_fields = false;
     c->parent = parent->c;
     try {
@@ -196,6 +197,18 @@ int qwsg_set_graphs(qwsg_lattice* l, int enable) {
     QWSG_CUDA(cudaStreamSynchronize(c.st));
     c.use_graphs = enable != 0;
     if (!c.use_graphs) c.clear_graphs();
+  });
+}
+
+int qwsg_set_hop_threads(qwsg_lattice* l, int threads) {
+  return guarded([&] {
+    check_ctx(l);
+    if (threads != 64 && threads != 128 && threads != 256)
+      throw Error(1, "qwsg_set_hop_threads: threads must be 64, 128 or 256");
+    Ctx& c = *l->c;
+    QWSG_CUDA(cudaStreamSynchronize(c.st));
+    c.clear_graphs();  // captured launches carry the old shape
+    c.G.hop_threads = threads;
   });
 }
 
@@ -528,6 +541,34 @@ int qwsg_bicgstab_vm(qwsg_lattice* l, double* x, const double* b, int maxiter, i
     single_rhs(l, "qwsg_bicgstab_vm");
     need_fields(*l->c, true);
     int it = bicgstab_vm(*l->c, x, b, maxiter);
+    if (iters) *iters = it;
+  });
+}
+int qwsg_mtdagmt_d(qwsg_lattice* l, double* out, const double* in) {
+  return guarded([&] {
+    check_ctx(l);
+    single_rhs(l, "qwsg_mtdagmt_d");
+    need_fields(*l->c, true);
+    mtdagmt_d(*l->c, out, in);
+  });
+}
+int qwsg_cg_vm(qwsg_lattice* l, double* x, const double* b, int maxiter, int* iters) {
+  return guarded([&] {
+    check_ctx(l);
+    single_rhs(l, "qwsg_cg_vm");
+    need_fields(*l->c, true);
+    int it = cg_vm(*l->c, x, b, maxiter);
+    if (iters) *iters = it;
+  });
+}
+int qwsg_mcg_vm(qwsg_lattice* l, double* x, const double* b, int nshift, const double* sigma,
+                int maxiter, int* iters) {
+  return guarded([&] {
+    check_ctx(l);
+    single_rhs(l, "qwsg_mcg_vm");
+    if (!x || !b || !sigma) throw Error(1, "qwsg_mcg_vm: NULL argument");
+    need_fields(*l->c, true);
+    int it = mcg_vm(*l->c, x, b, nshift, sigma, maxiter);
     if (iters) *iters = it;
   });
 }

@@ -119,6 +119,8 @@ struct Ctx {
   // per-RHS scalar table (4 doubles per RHS) for the batched BLAS updates:
   // copied from host `v` to a device slot; returns the device pointer
   const double* put_coefs(const double* v);
+  // the same for n doubles (n <= 4 * kMaxRhs)
+  const double* put_coefs(const double* v, int n);
   double* d_coef = nullptr;  // kCoefSlots x 4*kMaxRhs
   double* h_coef = nullptr;  // pinned staging of the same size
   int coef_next = 0;
@@ -149,6 +151,9 @@ struct Ctx {
   const float* eoCs = nullptr;
   int pce = 0, pco = 1;
   double* eo_d[6] = {};
+  // multi-shift CG: the shifts' search vectors (ms_n fields back to back)
+  double* ms_p = nullptr;
+  int ms_n = 0;
   float* eo_s[2] = {};
   void ensure_eo();
   long n_mtilde = 0;
@@ -260,6 +265,11 @@ void mtilde_d(Ctx& c, double* out, const double* in);      // qws.cc:551-556
 void mtilde_dag_d(Ctx& c, double* out, const double* in);  // qws.cc:557-565
 void mtilde_s(Ctx& c, float* out, const float* in);        // qws.cc:598-604
 int bicgstab_vm(Ctx& c, double* x, const double* b, int maxiter);  // bicgstab.cc:68
+void mtdagmt_d(Ctx& c, double* out, const double* in);              // qws.cc:566-571
+int cg_vm(Ctx& c, double* x, const double* b, int maxiter);        // cg.cc:65
+// X: n solution fields back to back (spinor_elems() doubles each)
+int mcg_vm(Ctx& c, double* X, const double* b, int n, const double* sigma,
+           int maxiter);                                            // mcg.cc:65
 
 }  // namespace qwsg
 

@@ -907,6 +907,44 @@ void bicgstab_vm_(scd_t* x, scd_t* b, int* conviter, int* maxiter) {
   });
 }
 
+// cg.cc:65-172: x (initial guess in, solution out) and b are parity-pce half arrays
+void cg_vm_(scd_t* x, scd_t* b, int* conviter, int* maxiter) {
+  guard("cg_vm_", [&] {
+    Ctx& c = ctx();
+    sync_eo(c);
+    double** P = g.ed;
+    up_eo<double>(c, P[0], x, g.pce, g.vlend);
+    up_eo<double>(c, P[1], b, g.pce, g.vlend);
+    const int it = cg_vm(c, P[0], P[1], *maxiter);
+    if (conviter) *conviter = it;
+    down_eo<double>(c, x, P[0], g.pce, g.vlend);
+  });
+}
+// mcg.cc:65-219: *n solutions, each a parity-pce half array, back to back in xx
+void mcg_vm_(scd_t* xx, scd_t* b, int* n, double* sigma, int* maxiter) {
+  guard("mcg_vm_", [&] {
+    Ctx& c = ctx();
+    sync_eo(c);
+    if (*n < 1 || *n > Ctx::kMaxRhs) throw Error(1, "mcg_vm_: number of shifts must be 1..32");
+    double** P = g.ed;
+    up_eo<double>(c, P[1], b, g.pce, g.vlend);
+    double* X = nullptr;
+    QWSG_CUDA(cudaMalloc(&X, sizeof(double) * c.spinor_elems() * *n));
+    try {
+      mcg_vm(c, X, P[1], *n, sigma, *maxiter);
+      const size_t half = (size_t)c.G.Vh * 24;  // reals of one half array
+      for (int k = 0; k < *n; k++)
+        down_eo<double>(c, (double*)xx + k * half, X + k * c.spinor_elems(), g.pce, g.vlend);
+      QWSG_CUDA(cudaStreamSynchronize(c.st));
+    } catch (...) {
+      cudaStreamSynchronize(c.st);
+      cudaFree(X);
+      throw;
+    }
+    QWSG_CUDA(cudaFree(X));
+  });
+}
+
 void deo_in_s_(int* pe, int* po, scs_t* out, scs_t* in) {
   eo_apply<float>("deo_in_s_", pe, po, out, in, nullptr, kIn, 0);
 }

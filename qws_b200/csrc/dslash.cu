@@ -61,7 +61,7 @@ __device__ __forceinline__ void do_hop(const HopArgs<T>& a, const Site& s, int g
 }
 
 template <typename T, int SEL, int EPI>
-__global__ void __launch_bounds__(128) k_hop(const HopArgs<T> a) {
+__global__ void __launch_bounds__(256) k_hop(const HopArgs<T> a) {
   using R = typename Arith<T>::R;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (a.nsites << a.G.lgnr)) return;
@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(128) k_hop(const HopArgs<T> a) {
 template <typename T, int SEL, int EPI>
 static void launch(const HopArgs<T>& a, cudaStream_t st) {
   if (a.nsites <= 0) return;
-  const int threads = 128;
+  const int threads = a.G.hop_threads;
   const int blocks = ((a.nsites << a.G.lgnr) + threads - 1) / threads;
   count_launch();
   k_hop<T, SEL, EPI><<<blocks, threads, 0, st>>>(a);

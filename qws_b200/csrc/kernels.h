@@ -100,6 +100,17 @@ void blas_bicg_p(const Geom& G, R* p, const R* r, const R* q, double br, double 
 template <typename R>
 void blas_bicg_init(const Geom& G, const R* b, const R* q, R* r, R* p, R* r0, double* res,
                     RedBuf& rb, cudaStream_t st);
+// r += a q ; res[0] = |r|^2   (real a; the residual step of mcg.cc:118-138)
+template <typename R>
+void blas_axpy_norm(const Geom& G, R* r, const R* q, double a, double* res, RedBuf& rb,
+                    cudaStream_t st);
+// one multi-shift CG step for n shifts (mcg.cc:141-205), single RHS:
+// x_k -= c_k pp_k for every shift k; then, when `update`,
+// pp_k = z_k r + d_k pp_k and p = r + beta p.  x and pp hold the n shift
+// fields back to back (24 * spad(G) doubles each); cf[4k + 0..3] = (c_k, z_k,
+// d_k, active_k): shifts with active_k == 0 are left as they are
+void blas_mshift(const Geom& G, double* x, double* pp, int n, const double* r, double* p,
+                 double beta, const double* cf, bool update, cudaStream_t st);
 // FP32 planes <-> FP16 planes with per-site scales (IO<H16> format)
 void spinor_s2h(const Geom& G, __half* dst, const float* src, cudaStream_t st);
 void spinor_h2s(const Geom& G, float* dst, const __half* src, cudaStream_t st);

@@ -69,6 +69,9 @@ struct Geom {
   // load.  Gauge and clover fields are per site (stride pad).
   int nr;
   int lgnr;
+  // threads per CTA of the hop kernels (a launch shape: 64, 128 or 256;
+  // host-side only, chosen per lattice)
+  int hop_threads;
   // multipliers for the divisions of the site decoding
   FastDiv fB[4], fVb, fnbh0, fNB1, fNB2;
 };

@@ -139,6 +139,7 @@ Ctx::Ctx(const int L[4], const int NB[4], int tbc, int nrhs) {
   if (nrhs < 1 || nrhs > kMaxRhs || (nrhs & (nrhs - 1)))
     throw Error(1, "number of right-hand sides must be a power of two in 1..32");
   G.nr = nrhs;
+  G.hop_threads = 128;
   G.lgnr = 0;
   while ((1 << G.lgnr) < nrhs) G.lgnr++;
   for (int mu = 0; mu < 4; mu++) {
@@ -187,13 +188,16 @@ Ctx::Ctx(const int L[4], const int NB[4], int tbc, int nrhs) {
 // Each slot is used once per kCoefSlots calls; the batched solvers read a
 // reduction result (a stream synchronisation) between consecutive uses of
 // one slot, so a slot is never rewritten while its copy is pending.
-const double* Ctx::put_coefs(const double* v) {
-  const int n = 4 * kMaxRhs;
-  double* h = h_coef + (size_t)coef_next * n;
-  double* d = d_coef + (size_t)coef_next * n;
+const double* Ctx::put_coefs(const double* v) { return put_coefs(v, 4 * G.nr); }
+
+const double* Ctx::put_coefs(const double* v, int n) {
+  const int slot = 4 * kMaxRhs;
+  if (n < 0 || n > slot) throw Error(1, "coefficient table too large");
+  double* h = h_coef + (size_t)coef_next * slot;
+  double* d = d_coef + (size_t)coef_next * slot;
   coef_next = (coef_next + 1) % kCoefSlots;
-  std::memcpy(h, v, sizeof(double) * 4 * G.nr);
-  QWSG_CUDA(cudaMemcpyAsync(d, h, sizeof(double) * 4 * G.nr, cudaMemcpyHostToDevice, st));
+  std::memcpy(h, v, sizeof(double) * n);
+  QWSG_CUDA(cudaMemcpyAsync(d, h, sizeof(double) * n, cudaMemcpyHostToDevice, st));
   return d;
 }
 

@@ -78,7 +78,7 @@ class _Resident:
     """One gauge field on the device (a Lattice), with the clover term of the
     kappa/csw it was last built for.  Held by one job at a time."""
 
-    def __init__(self, L, gauge_id, U, NB):
+    def __init__(self, L, gauge_id, U, NB, hop_threads=128):
         import torch
 
         import qws_b200
@@ -86,6 +86,7 @@ class _Resident:
         self.L, self.gid = L, gauge_id
         self.stream = torch.cuda.Stream()
         self.lat = qws_b200.Lattice(L, NB, tbc=-1, kappa=0.0, stream=self.stream)
+        self.lat.set_hop_threads(hop_threads)
         if isinstance(U, dict):  # {"seed", "n_smear", "alpha"}: generate on the device
             self.plaquette = self.lat.gen_gauge_device(U["seed"], U["n_smear"], U["alpha"])
         else:
@@ -130,14 +131,17 @@ class Service:
     device (called each time the field is made resident)."""
 
     def __init__(self, gauge_source, budget_bytes=150e9, workers=3, max_batch=16,
-                 block_grid=(2, 1, 1, 1), maxiter=100, tol_s=1e-6, maxiter_s=50, nsap=4, nm=2,
+                 block_grid=None, maxiter=100, tol_s=1e-6, maxiter_s=50, nsap=None, nm=None,
                  reliable=5):
         self.gauge_source = gauge_source
         self.budget = float(budget_bytes)
         self.max_batch = int(max_batch)
-        self.NB = tuple(block_grid)
-        self.solver = dict(maxiter=maxiter, tol_s=tol_s, maxiter_s=maxiter_s, nsap=nsap, nm=nm,
-                           reliable=reliable)
+        # SAP block grid / sweep counts / CTA size per volume: as given, else
+        # the autotuner's cached choice for this GPU, else the reference's
+        # one-rank partition with (nsap, nm) = (4, 2)
+        self.fixed = {"NB": block_grid, "nsap": nsap, "nm": nm}
+        self.configs = {}
+        self.solver = dict(maxiter=maxiter, tol_s=tol_s, maxiter_s=maxiter_s, reliable=reliable)
         self.pending = []                 # requests not yet started, arrival order
         self.cv = threading.Condition()
         self.residents = {}               # (L, gid) -> _Resident or _Placeholder
@@ -153,6 +157,22 @@ class Service:
             t.start()
         self.sched = threading.Thread(target=self._scheduler, daemon=True)
         self.sched.start()
+
+    def config(self, L):
+        """Launch configuration of volume L (block grid, nsap, nm, hop threads)."""
+        c = self.configs.get(L)
+        if c is None:
+            from . import autotune
+
+            hit = autotune.lookup(L, "hf", 1) or {}
+            c = {"NB": tuple(hit.get("NB", autotune.REFERENCE_NB)), "nsap": hit.get("nsap", 4),
+                 "nm": hit.get("nm", 2), "hop_threads": hit.get("hop_threads", 128),
+                 "tuned": bool(hit)}
+            for k, v in self.fixed.items():
+                if v is not None:
+                    c[k] = tuple(v) if k == "NB" else v
+            self.configs[L] = c
+        return c
 
     # ---- client side -----------------------------------------------------------
     def submit(self, req: Request) -> Request:
@@ -273,9 +293,10 @@ class Service:
         t0 = time.monotonic()
         for q in group:
             q.t_start = t0
+        cfg = self.config(res.L)
         if isinstance(res, _Placeholder):  # first use of this field: make it resident
             U = self.gauge_source(res.L, res.gid)
-            live = _Resident(res.L, res.gid, U, self.NB)
+            live = _Resident(res.L, res.gid, U, cfg["NB"], cfg["hop_threads"])
             live.busy = True
             with self.cv:
                 self.residents[(res.L, res.gid)] = live
@@ -293,7 +314,7 @@ class Service:
             bd = B.to_device(S)
             xd = B.empty("f64")
             st = B.bicgstab_dd_mix2_hf(xd, bd, r0.tol, s["maxiter"], s["tol_s"], s["maxiter_s"],
-                                       s["nsap"], s["nm"], reliable=s["reliable"])
+                                       cfg["nsap"], cfg["nm"], reliable=s["reliable"])
             truer = B.true_residual(xd, bd)
             X = B.to_host(xd)
             per = B.batch_stats()[0] if nr > 1 else [st]

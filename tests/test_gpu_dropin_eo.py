@@ -179,6 +179,43 @@ def test_bicgstab_vm(qws):
         assert check_sh_ok(k, v, rv), (k, v, rv)
 
 
+def test_cg_vm_and_mcg_vm(qws):
+    """cg.cc:65 and mcg.cc:65 through the drop-in entry points on main.cc's
+    arrays (source: the first half array read as a parity-0 field), against
+    the oracle's restatements on the even-odd reading (eo_perm) of the same
+    fields.  CG on mtilde^dag mtilde needs about 1100 iterations here (the
+    links of main.cc are not unitary)."""
+    from qwsref import Oracle, eo_perm, parity_mask, qws_to_nat_spinor
+
+    lib, b, _ = qws
+    U, C, S = gen_main_fields(L, (1, 1, 1, 1), 2)
+    perm, m0 = eo_perm(L), parity_mask(L, 0)
+    oe = Oracle(L, (2, 1, 1, 1), tbc=-1, kappa=KAPPA)
+    oe.set_fields(U[:, perm], C[perm])
+    be = S[0][perm] * m0[:, None]
+
+    def eo_field(h):
+        q = np.zeros(2 * HALF_D)
+        q[:HALF_D] = h
+        return qws_to_nat_spinor(q, L, VLEND)[perm][m0]
+
+    def rel(a, r):
+        return float(np.linalg.norm((a - r).ravel()) / np.linalg.norm(r.ravel()))
+
+    x = alloc(2 * HALF_D, np.float64)
+    it = ctypes.c_int(0)
+    lib.cg_vm_(P(x), P(b), ctypes.byref(it), I(2000))
+    xo, it_o = oe.cg_vm(be, np.zeros_like(be), 2000)
+    assert it_o < 1999 and abs(it.value - it_o) <= 1
+    assert rel(eo_field(x[:HALF_D]), xo[m0]) < 1e-11
+    sigma = np.array([0.0, 0.01, 0.2, 1.5])
+    xx = alloc(len(sigma) * HALF_D, np.float64)
+    lib.mcg_vm_(P(xx), P(b), I(len(sigma)), P(sigma), I(2000))
+    Xo, _ = oe.mcg_vm(be, sigma, 2000)
+    for k in range(len(sigma)):
+        assert rel(eo_field(xx[k * HALF_D:(k + 1) * HALF_D]), Xo[k][m0]) < 1e-11, k
+
+
 def test_bqcd_loaders_roundtrip(qws):
     """qws_{load,store}f{d,s}_bqcd_ move the even sites of one half array
     and invert each other (FP32 through one rounding)."""

@@ -89,3 +89,30 @@ def test_mtilde_and_solver(setup):
         for nm_, val, ref in zip(("bnorm^2", "rnorm^2", "xnorm^2"),
                                  (n2(be), n2(r), n2(lat.to_host(x))), vals):
             assert check_sh_ok(nm_, val, ref), (nm_, val, ref)
+
+
+def test_cg_solvers(setup):
+    """cg_vm_ (cg.cc:65) and mcg_vm_ (mcg.cc:65) on mtilde^dag mtilde against
+    the oracle's restatements (which tests/test_oracle_vs_ref.py pins to the
+    reference's own solvers): iteration counts within 1, solutions to 1e-11
+    relative, and every shifted system solved to 1e-10."""
+    name, L, o, lat, b = setup
+    m0 = parity_mask(L, 0)
+    be = b * m0[:, None]
+    bd = lat.to_device(be)
+    xo, it_o = o.cg_vm(be, np.zeros_like(b), 3000)
+    assert it_o < 2999
+    x = lat.empty("f64")
+    it = lat.cg_vm(x, bd, 3000)
+    assert abs(it - it_o) <= 1
+    assert rel(lat.to_host(x), xo, m0) < 1e-11
+    sigma = [0.0, 0.05, 0.5, 2.0]
+    Xo, it_o = o.mcg_vm(be, sigma, 3000)
+    X, it = lat.mcg_vm(bd, sigma, 3000)
+    assert abs(it - it_o) <= 1
+    for k, s in enumerate(sigma):
+        xk = lat.to_host(X[k])
+        assert np.isfinite(xk).all(), k
+        assert rel(xk, Xo[k], m0) < 1e-11, k
+        ax = lat.to_host(lat.mtdagmt(X[k])) + s * xk
+        assert rel(ax, be, m0) < 1e-10, k

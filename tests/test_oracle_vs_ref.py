@@ -138,3 +138,55 @@ def test_bqcd_loaders_match_reference(setup):
     finally:
         r.set_kappa(KAPPA)
         r.set_fields(U, C)
+
+
+def test_cg_solvers_match_reference(setup):
+    """cg_vm_ (cg.cc:65) and mcg_vm_ (mcg.cc:65) of the reference against
+    the oracle's restatements, driven as main.cc drives the even-odd family:
+    the DD arrays are read with the parity split (eo_perm), the source is the
+    first half array read as a parity-0 field.  Solutions agree to 1e-11
+    relative on the even sites (both stop at |r|/|b| < 1e-14)."""
+    from qwsref import eo_perm, parity_mask
+
+    o, r, _ = setup
+    U, C, S = gen_main_fields(L, (1, 1, 1, 1), 2)
+    P, m0 = eo_perm(L), parity_mask(L, 0)
+    oe = Oracle(L, (2, 1, 1, 1), tbc=-1, kappa=KAPPA)
+    oe.set_fields(U[:, P], C[P])
+    V = int(np.prod(L))
+    half = 12 * V  # reals of one half array
+    bfull = r.to_d(S[0])
+    be = S[0][P] * m0[:, None]
+
+    def eo_field(h):
+        q = aligned_empty(24 * V, np.float64)
+        q[:] = 0
+        q[:half] = h
+        return r.from_d(q)[P] * m0[:, None]
+
+    x = aligned_empty(half, np.float64)
+    x[:] = 0
+    # main.cc's links are not unitary: CG on mtdagmt needs about 1100 iterations
+    r.call("cg_vm_", x, bfull, ctypes.byref(ctypes.c_int(0)), ctypes.byref(ctypes.c_int(2000)))
+    xo, it = oe.cg_vm(be, np.zeros_like(be), 2000)
+    assert 1 < it < 1999
+    assert rel(eo_field(x)[m0], xo[m0]) < 1e-11
+
+    sigma = np.array([0.0, 0.01, 0.2, 1.5])
+    xx = aligned_empty(len(sigma) * half, np.float64)
+    xx[:] = 0
+    r.call("mcg_vm_", xx, bfull, ctypes.byref(ctypes.c_int(len(sigma))),
+           sigma.ctypes.data_as(ctypes.c_void_p), ctypes.byref(ctypes.c_int(2000)))
+    Xo, it = oe.mcg_vm(be, sigma, 2000)
+    assert 1 < it < 1999
+    # shifts 0 and 0.01 run to the end in the reference too; the larger ones
+    # converge early, after which the reference's zeta underflows (0/0 = NaN)
+    # while the oracle has stopped updating them
+    finite = [bool(np.isfinite(xx[k * half:(k + 1) * half]).all()) for k in range(len(sigma))]
+    assert finite[0] and finite[1]
+    for k in range(len(sigma)):
+        if finite[k]:
+            assert rel(eo_field(xx[k * half:(k + 1) * half])[m0], Xo[k][m0]) < 1e-11, k
+    # the shifted systems are solved: (mtdagmt + sigma) x_k = b on the even sites
+    for k, s in enumerate(sigma):
+        assert rel((oe.mtdagmt(Xo[k]) + s * Xo[k])[m0], be[m0]) < 1e-10, k
