@@ -207,6 +207,27 @@ int qwsg_cg_vm(qwsg_lattice* lat, double* x, const double* b, int maxiter, int* 
 int qwsg_mcg_vm(qwsg_lattice* lat, double* x, const double* b, int nshift, const double* sigma,
                 int maxiter, int* iters);
 
+/* BQCD-format arrays converted on the device (the reference's loaders,
+ * qws_bqcd.cc:66-642, reorder on the host into QWS's layout instead).
+ * Links u[ri + 2*row + 6*col + 18*slot + 18*V*mu], clover
+ * c[perm[k] + 36*ud + 72*slot] (qws_bqcd.cc:125-377), spinors as an even and
+ * an odd array of V/2 sites, element 2*s + 8*c + ri + 24*(i-1)
+ * (qws_bqcd.cc:500-642; nrhs arrays back to back on a batch handle).
+ * slot = (i-1) + V/2*eo for the site's 1-based index i within its parity
+ * eo.  site_map: host array, site_map[n] = slot of natural site
+ * n = x + Lx*(y + Ly*(z + Lz*t)); NULL = i-1 = n/2 (the numbering the
+ * drop-in uses when the host program has no std_xyzt2i_). */
+int qwsg_load_gauge_bqcd(qwsg_lattice* lat, const double* u, const int* site_map);
+int qwsg_load_clover_bqcd(qwsg_lattice* lat, const double* c, const int* site_map);
+int qwsg_spinor_from_bqcd_d(qwsg_lattice* lat, double* dev, const double* even,
+                            const double* odd, const int* site_map);
+int qwsg_spinor_from_bqcd_s(qwsg_lattice* lat, float* dev, const double* even, const double* odd,
+                            const int* site_map);
+int qwsg_spinor_to_bqcd_d(qwsg_lattice* lat, double* even, double* odd, const double* dev,
+                          const int* site_map);
+int qwsg_spinor_to_bqcd_s(qwsg_lattice* lat, double* even, double* odd, const float* dev,
+                          const int* site_map);
+
 /* CUDA graphs for the SAP preconditioner's launch sequences (default on):
  * captured on first use per buffers/nsap/nm/kappa, replayed afterwards; not
  * used while kernel timing is on or on the legacy default stream */

@@ -63,6 +63,12 @@ def load_library(path: str | os.PathLike | None = None):
         "qwsg_set_graphs": [vp, c_int],
         "qwsg_set_hop_threads": [vp, c_int],
         "qwsg_mtdagmt_d": [vp, vp, vp],
+        "qwsg_load_gauge_bqcd": [vp, vp, vp],
+        "qwsg_load_clover_bqcd": [vp, vp, vp],
+        "qwsg_spinor_from_bqcd_d": [vp, vp, vp, vp, vp],
+        "qwsg_spinor_from_bqcd_s": [vp, vp, vp, vp, vp],
+        "qwsg_spinor_to_bqcd_d": [vp, vp, vp, vp, vp],
+        "qwsg_spinor_to_bqcd_s": [vp, vp, vp, vp, vp],
         "qwsg_cg_vm": [vp, vp, vp, c_int, ip],
         "qwsg_mcg_vm": [vp, vp, vp, c_int, dp, c_int, ip],
         "qwsg_gen_gauge_device": [vp, ctypes.c_ulonglong, c_int, c_double,
@@ -259,6 +265,46 @@ class Lattice:
         U, pu = _host(U, np.float64)
         assert U.size == 72 * self.V
         _check(self.lib.qwsg_load_gauge(self.h, pu))
+
+    # ---- BQCD-format arrays (reordered on the device) ------------------------
+    @staticmethod
+    def _map(site_map):
+        if site_map is None:
+            return None, None
+        m = np.ascontiguousarray(site_map, np.int32)
+        return m, ctypes.c_void_p(m.ctypes.data)
+
+    def load_fields_bqcd(self, u, c, site_map=None):
+        """BQCD gauge u (4*V*18 reals) and clover c (V*72 reals), FP64."""
+        u, pu = _host(u, np.float64)
+        c, pc = _host(c, np.float64)
+        assert u.size == 72 * self.V and c.size == 72 * self.V
+        m, pm = self._map(site_map)
+        _check(self.lib.qwsg_load_gauge_bqcd(self.h, pu, pm))
+        _check(self.lib.qwsg_load_clover_bqcd(self.h, pc, pm))
+
+    def from_bqcd(self, even, odd, dtype="f64", site_map=None, out=None):
+        """BQCD even/odd spinor arrays (FP64, V/2*24 reals each per RHS) -> device."""
+        e, pe_ = _host(even, np.float64)
+        o, po = _host(odd, np.float64)
+        assert e.size == o.size == 12 * self.V * self.nr
+        out = self.empty(dtype) if out is None else out
+        m, pm = self._map(site_map)
+        fn = self.lib.qwsg_spinor_from_bqcd_d if out.dtype == self.torch.float64 else \
+            self.lib.qwsg_spinor_from_bqcd_s
+        _check(fn(self.h, _ptr(out), pe_, po, pm))
+        return out
+
+    def to_bqcd(self, t, site_map=None):
+        """device spinor -> (even, odd) BQCD arrays, FP64."""
+        even = np.empty(12 * self.V * self.nr, np.float64)
+        odd = np.empty_like(even)
+        m, pm = self._map(site_map)
+        fn = self.lib.qwsg_spinor_to_bqcd_d if t.dtype == self.torch.float64 else \
+            self.lib.qwsg_spinor_to_bqcd_s
+        _check(fn(self.h, ctypes.c_void_p(even.ctypes.data), ctypes.c_void_p(odd.ctypes.data),
+                  _ptr(t), pm))
+        return even, odd
 
     def gen_gauge_device(self, seed, n_smear=5, alpha=0.36):
         """Seeded SU(3) + APE gauge field generated on the GPU; returns the plaquette."""

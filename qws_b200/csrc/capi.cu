@@ -2,8 +2,10 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/qwsg.h"
+
 #include "ctx.h"
 
 namespace qwsg {
@@ -120,6 +122,81 @@ static SolveStats worst(const std::vector<SolveStats>& v) {
 
 using namespace qwsg;
 
+// ---- BQCD-format arrays, reordered on the device (bqcd.cu) --------------------
+// staging: the raw array (n reals) and, if given, the site map after it
+static const int* bqcd_stage(Ctx& c, const double* const* parts, const size_t* sizes, int nparts,
+                             const int* site_map, double** data) {
+  size_t n = 0;
+  for (int k = 0; k < nparts; k++) n += sizes[k];
+  const size_t map_off = (sizeof(double) * n + 255) / 256 * 256;
+  char* d = (char*)staging(c, map_off + (site_map ? sizeof(int) * (size_t)c.G.V : 0));
+  size_t off = 0;
+  for (int k = 0; k < nparts; k++) {
+    if (parts[k])
+      QWSG_CUDA(cudaMemcpyAsync(d + sizeof(double) * off, parts[k], sizeof(double) * sizes[k],
+                                cudaMemcpyHostToDevice, c.st));
+    off += sizes[k];
+  }
+  *data = (double*)d;
+  if (!site_map) return nullptr;
+  QWSG_CUDA(cudaMemcpyAsync(d + map_off, site_map, sizeof(int) * (size_t)c.G.V,
+                            cudaMemcpyHostToDevice, c.st));
+  return (const int*)(d + map_off);
+}
+
+// a site map must send the sites of parity eo to slots [eo*V/2, (eo+1)*V/2),
+// each slot once (std_xyzt2i_ numbers the sites of each parity 1..V/2)
+static void check_site_map(const Ctx& c, const int* site_map) {
+  if (!site_map) return;
+  const int* L = c.G.L;
+  const int V = c.G.V, Vh = V / 2;
+  std::vector<char> seen(V, 0);
+  for (int n = 0; n < V; n++) {
+    const int x = n % L[0], y = (n / L[0]) % L[1], z = (n / (L[0] * L[1])) % L[2],
+              t = n / (L[0] * L[1] * L[2]);
+    const int eo = (x + y + z + t) & 1, s = site_map[n];
+    if (s < eo * Vh || s >= (eo + 1) * Vh || seen[s])
+      throw Error(1, "BQCD site map: not a per-parity permutation of the slots");
+    seen[s] = 1;
+  }
+}
+
+template <typename R>
+static void spinor_from_bqcd(Ctx& c, R* dev, const double* even, const double* odd,
+                             const int* site_map) {
+  if (!dev || !even || !odd) throw Error(1, "spinor_from_bqcd: NULL argument");
+  check_site_map(c, site_map);
+  const size_t half = (size_t)12 * c.G.V;  // reals of one parity array
+  const double* parts[2] = {even, odd};
+  const size_t sizes[2] = {half, half};
+  for (int r = 0; r < c.G.nr; r++) {
+    double* d;
+    const double* pr[2] = {parts[0] + r * half, parts[1] + r * half};
+    const int* map = bqcd_stage(c, pr, sizes, 2, site_map, &d);
+    bqcd_to_planes_spinor<R>(c.G, dev, d, map, r, c.st);
+    c.check_launch("spinor_from_bqcd");
+    QWSG_CUDA(cudaStreamSynchronize(c.st));
+  }
+}
+template <typename R>
+static void spinor_to_bqcd(Ctx& c, double* even, double* odd, const R* dev, const int* site_map) {
+  if (!dev || !even || !odd) throw Error(1, "spinor_to_bqcd: NULL argument");
+  check_site_map(c, site_map);
+  const size_t half = (size_t)12 * c.G.V;
+  const double* none[2] = {nullptr, nullptr};
+  const size_t sizes[2] = {half, half};
+  for (int r = 0; r < c.G.nr; r++) {
+    double* d;
+    const int* map = bqcd_stage(c, none, sizes, 2, site_map, &d);
+    planes_to_bqcd_spinor<R>(c.G, d, dev, map, r, c.st);
+    c.check_launch("spinor_to_bqcd");
+    QWSG_CUDA(cudaMemcpyAsync(even + r * half, d, sizeof(double) * half, cudaMemcpyDeviceToHost,
+                              c.st));
+    QWSG_CUDA(cudaMemcpyAsync(odd + r * half, d + half, sizeof(double) * half,
+                              cudaMemcpyDeviceToHost, c.st));
+    QWSG_CUDA(cudaStreamSynchronize(c.st));
+  }
+}
 extern "C" {
 
 const char* qwsg_last_error(void) { return g_last_error.c_str(); }
@@ -292,6 +369,71 @@ int qwsg_load_clover_s(qwsg_lattice* l, const float* C) {
     Ctx& c = *l->c;
     c.ensure_fields_s();
     load_clover_t<float, float>(c, c.Cs, C);
+  });
+}
+
+int qwsg_load_gauge_bqcd(qwsg_lattice* l, const double* u, const int* site_map) {
+  return guarded([&] {
+    check_ctx(l);
+    not_batch(l, "qwsg_load_gauge_bqcd");
+    if (!u) throw Error(1, "qwsg_load_gauge_bqcd: NULL argument");
+    Ctx& c = *l->c;
+    check_site_map(c, site_map);
+    c.ensure_fields_d();
+    c.ensure_fields_s();
+    const size_t n = (size_t)72 * c.G.V;
+    double* d;
+    const int* map = bqcd_stage(c, &u, &n, 1, site_map, &d);
+    bqcd_to_planes_gauge<double>(c.G, c.Ud, d, map, c.st);
+    bqcd_to_planes_gauge<float>(c.G, c.Us, d, map, c.st);
+    c.check_launch("load_gauge_bqcd");
+    QWSG_CUDA(cudaStreamSynchronize(c.st));
+  });
+}
+int qwsg_load_clover_bqcd(qwsg_lattice* l, const double* cl, const int* site_map) {
+  return guarded([&] {
+    check_ctx(l);
+    not_batch(l, "qwsg_load_clover_bqcd");
+    if (!cl) throw Error(1, "qwsg_load_clover_bqcd: NULL argument");
+    Ctx& c = *l->c;
+    check_site_map(c, site_map);
+    c.ensure_fields_d();
+    c.ensure_fields_s();
+    const size_t n = (size_t)72 * c.G.V;
+    double* d;
+    const int* map = bqcd_stage(c, &cl, &n, 1, site_map, &d);
+    bqcd_to_planes_clover<double>(c.G, c.Cd, d, map, c.st);
+    bqcd_to_planes_clover<float>(c.G, c.Cs, d, map, c.st);
+    c.check_launch("load_clover_bqcd");
+    QWSG_CUDA(cudaStreamSynchronize(c.st));
+  });
+}
+int qwsg_spinor_from_bqcd_d(qwsg_lattice* l, double* dev, const double* even, const double* odd,
+                            const int* site_map) {
+  return guarded([&] {
+    check_ctx(l);
+    spinor_from_bqcd<double>(*l->c, dev, even, odd, site_map);
+  });
+}
+int qwsg_spinor_from_bqcd_s(qwsg_lattice* l, float* dev, const double* even, const double* odd,
+                            const int* site_map) {
+  return guarded([&] {
+    check_ctx(l);
+    spinor_from_bqcd<float>(*l->c, dev, even, odd, site_map);
+  });
+}
+int qwsg_spinor_to_bqcd_d(qwsg_lattice* l, double* even, double* odd, const double* dev,
+                          const int* site_map) {
+  return guarded([&] {
+    check_ctx(l);
+    spinor_to_bqcd<double>(*l->c, even, odd, dev, site_map);
+  });
+}
+int qwsg_spinor_to_bqcd_s(qwsg_lattice* l, double* even, double* odd, const float* dev,
+                          const int* site_map) {
+  return guarded([&] {
+    check_ctx(l);
+    spinor_to_bqcd<float>(*l->c, even, odd, dev, site_map);
   });
 }
 

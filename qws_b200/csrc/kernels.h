@@ -111,6 +111,20 @@ void blas_axpy_norm(const Geom& G, R* r, const R* q, double a, double* res, RedB
 // d_k, active_k): shifts with active_k == 0 are left as they are
 void blas_mshift(const Geom& G, double* x, double* pp, int n, const double* r, double* p,
                  double beta, const double* cf, bool update, cudaStream_t st);
+// BQCD-format arrays (already on the device) <-> planes, bqcd.cu.  map:
+// device array of each natural site's BQCD slot (i-1 + volh*eo), or null for
+// the default numbering; spinors: the even array followed by the odd one
+template <typename R>
+void bqcd_to_planes_gauge(const Geom& G, R* dst, const double* u, const int* map, cudaStream_t st);
+template <typename R>
+void bqcd_to_planes_clover(const Geom& G, R* dst, const double* c, const int* map,
+                           cudaStream_t st);
+template <typename R>
+void bqcd_to_planes_spinor(const Geom& G, R* dst, const double* both, const int* map, int rhs,
+                           cudaStream_t st);
+template <typename R>
+void planes_to_bqcd_spinor(const Geom& G, double* both, const R* src, const int* map, int rhs,
+                           cudaStream_t st);
 // FP32 planes <-> FP16 planes with per-site scales (IO<H16> format)
 void spinor_s2h(const Geom& G, __half* dst, const float* src, cudaStream_t st);
 void spinor_h2s(const Geom& G, float* dst, const __half* src, cudaStream_t st);

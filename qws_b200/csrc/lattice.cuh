@@ -551,4 +551,40 @@ __device__ __forceinline__ void clover_apply(const typename Store<T>::type* __re
   }
 }
 
+// writers of one site's link (9 complex, row-major U_mu) and clover (72
+// reals, QWS packing) into the device planes
+template <typename R>
+__device__ __forceinline__ void store_link(R* p, int pad, int mu, int g, const R u[18]);
+template <>
+__device__ __forceinline__ void store_link<float>(float* p, int pad, int mu, int g,
+                                                  const float u[18]) {
+  float2* q = reinterpret_cast<float2*>(p);
+#pragma unroll
+  for (int e = 0; e < 9; e++) q[(size_t)(mu * 9 + e) * pad + g] = make_float2(u[2 * e], u[2 * e + 1]);
+}
+template <>
+__device__ __forceinline__ void store_link<double>(double* p, int pad, int mu, int g,
+                                                   const double u[18]) {
+  double2* q = reinterpret_cast<double2*>(p);
+#pragma unroll
+  for (int e = 0; e < 9; e++)
+    q[(size_t)(mu * 9 + e) * pad + g] = make_double2(u[2 * e], u[2 * e + 1]);
+}
+
+template <typename R>
+__device__ __forceinline__ void store_clover(R* p, int pad, int g, const R a[72]);
+template <>
+__device__ __forceinline__ void store_clover<float>(float* p, int pad, int g, const float a[72]) {
+  float4* q = reinterpret_cast<float4*>(p);
+#pragma unroll
+  for (int j = 0; j < 18; j++)
+    q[(size_t)j * pad + g] = make_float4(a[4 * j], a[4 * j + 1], a[4 * j + 2], a[4 * j + 3]);
+}
+template <>
+__device__ __forceinline__ void store_clover<double>(double* p, int pad, int g, const double a[72]) {
+  double2* q = reinterpret_cast<double2*>(p);
+#pragma unroll
+  for (int j = 0; j < 36; j++) q[(size_t)j * pad + g] = make_double2(a[2 * j], a[2 * j + 1]);
+}
+
 }  // namespace qwsg
