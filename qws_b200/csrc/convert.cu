@@ -239,27 +239,34 @@ __global__ void k_h2h(Geom G, __half* dst, const __half* __restrict__ src) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= (G.V << G.lgnr)) return;
   const size_t sp = spad(G);
-  const uint2* s = reinterpret_cast<const uint2*>(src);
-  uint2* d = reinterpret_cast<uint2*>(dst);
+  // the IO<H16> spinor layout: three 16-byte planes, then the scale plane
+  const uint4* s = reinterpret_cast<const uint4*>(src);
+  uint4* d = reinterpret_cast<uint4*>(dst);
 #pragma unroll
-  for (int j = 0; j < 6; j++) d[j * sp + e] = s[j * sp + e];
-  reinterpret_cast<float*>(d + 6 * sp)[e] = reinterpret_cast<const float*>(s + 6 * sp)[e];
+  for (int j = 0; j < 3; j++) d[j * sp + e] = s[j * sp + e];
+  reinterpret_cast<float*>(d + 3 * sp)[e] = reinterpret_cast<const float*>(s + 3 * sp)[e];
 }
 
 __global__ void k_fields_s2h(Geom G, __half* Uh, const float* __restrict__ Us, __half* Ch,
                              const float* __restrict__ Cs) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= G.V) return;
-  const float2* u = reinterpret_cast<const float2*>(Us);
-  __half2* uh = reinterpret_cast<__half2*>(Uh);
-  for (int p = 0; p < 36; p++) uh[(size_t)p * G.pad + g] = __float22half2_rn(u[(size_t)p * G.pad + g]);
-  const float4* c = reinterpret_cast<const float4*>(Cs);
-  uint2* ch = reinterpret_cast<uint2*>(Ch);
-  for (int j = 0; j < 18; j++) {
-    float4 t = c[(size_t)j * G.pad + g];
-    float v[4] = {t.x, t.y, t.z, t.w};
-    ch[(size_t)j * G.pad + g] = IO<H16>::pack4(v, 1.0f);
+  for (int mu = 0; mu < 4; mu++) {
+    float u[18];
+    IO<float>::load_link(Us, G.pad, mu, g, u);
+    IO<H16>::store_link(Uh, G.pad, mu, g, u);
   }
+  const float4* c = reinterpret_cast<const float4*>(Cs);
+  float a[72];
+#pragma unroll
+  for (int j = 0; j < 18; j++) {
+    const float4 t = c[(size_t)j * G.pad + g];
+    a[4 * j] = t.x;
+    a[4 * j + 1] = t.y;
+    a[4 * j + 2] = t.z;
+    a[4 * j + 3] = t.w;
+  }
+  IO<H16>::store_clover(Ch, G.pad, g, a);
 }
 
 }  // namespace

@@ -157,12 +157,13 @@ __device__ __forceinline__ int nbr_across(const Geom& G, const Site& s, int mu, 
 // plane I/O.  A storage tag T selects the in-memory format; arithmetic is in
 // Arith<T>::R.  float / double store what they compute; H16 stores FP16 and
 // computes in FP32:
-//   spinor  6 uint2 planes of 4 halves (plane j = colour j/2, spins
-//           2(j%2), 2(j%2)+1 -- the grouping of the FP32 float4 planes) holding
-//           v / n, followed by one float plane of per-site scales
-//           n = max |v_i| over the 24 reals (QUDA-style per-site norm);
-//   gauge   9 half2 planes per direction (entries of SU(3) are <= 1);
-//   clover  18 uint2 planes (block i = planes 9i .. 9i+8).
+//   spinor  three 16-byte planes of 8 halves holding v / n (grouped so that
+//           a t-hop's half spinor is one 16- and one 8-byte load, see
+//           IO<H16>), followed by one float plane of per-site scales
+//           n = max |v_i| over the 24 reals (a per-site norm);
+//   gauge   per direction two 16-byte planes and one 4-byte plane (the 9
+//           complex entries, which are <= 1 for SU(3));
+//   clover  nine 16-byte planes (the 72 reals; block 0 = reals 0-35).
 // ---------------------------------------------------------------------------
 struct H16 {};
 
@@ -300,19 +301,30 @@ struct IO<double> {
 
 template <>
 struct IO<H16> {
-  __device__ __forceinline__ static float scale(const __half* p, int pad, int g) {
-    return __ldg(reinterpret_cast<const float*>(reinterpret_cast<const uint2*>(p) + (size_t)6 * pad) +
-                 g);
+  // Spinor fields: three 16-byte planes and a float plane of per-site scales.
+  //   P0 = spins 0-1 of colours 0-1   (reals 0-3, 8-11 of [c][s][ri])
+  //   P1 = spins 2-3 of colours 0-1   (reals 4-7, 12-15)
+  //   P2 = colour 2, spins 0-1 then 2-3 (reals 16-23)
+  // A full spinor is three 16-byte loads; the half spinor a t-hop projects
+  // (spins 0-1 or 2-3) is one 16-byte and one 8-byte load.
+  __device__ __forceinline__ static const float* scale_plane(const __half* p, int pad) {
+    return reinterpret_cast<const float*>(reinterpret_cast<const uint4*>(p) + (size_t)3 * pad);
   }
-  __device__ __forceinline__ static void unpack4(uint2 t, float s, float* o) {
+  __device__ __forceinline__ static float scale(const __half* p, int pad, int g) {
+    return __ldg(scale_plane(p, pad) + g);
+  }
+  __device__ __forceinline__ static void unpack4(unsigned x, unsigned y, float s, float* o) {
     __half2 a, b;
-    memcpy(&a, &t.x, 4);
-    memcpy(&b, &t.y, 4);
+    memcpy(&a, &x, 4);
+    memcpy(&b, &y, 4);
     float2 fa = __half22float2(a), fb = __half22float2(b);
     o[0] = fa.x * s;
     o[1] = fa.y * s;
     o[2] = fb.x * s;
     o[3] = fb.y * s;
+  }
+  __device__ __forceinline__ static void unpack4(uint2 t, float s, float* o) {
+    unpack4(t.x, t.y, s, o);
   }
   __device__ __forceinline__ static uint2 pack4(const float* v, float inv) {
     __half2 a = __floats2half2_rn(v[0] * inv, v[1] * inv);
@@ -324,20 +336,27 @@ struct IO<H16> {
   }
   __device__ __forceinline__ static void load_spinor(const __half* __restrict__ p, int pad, int g,
                                                      float v[24]) {
-    const uint2* q = reinterpret_cast<const uint2*>(p);
+    const uint4* q = reinterpret_cast<const uint4*>(p);
     const float s = scale(p, pad, g);
-#pragma unroll
-    for (int j = 0; j < 6; j++) unpack4(__ldg(q + (size_t)j * pad + g), s, v + 4 * j);
+    const uint4 a = __ldg(q + g), b = __ldg(q + (size_t)pad + g), c = __ldg(q + (size_t)2 * pad + g);
+    unpack4(a.x, a.y, s, v + 0);
+    unpack4(a.z, a.w, s, v + 8);
+    unpack4(b.x, b.y, s, v + 4);
+    unpack4(b.z, b.w, s, v + 12);
+    unpack4(c.x, c.y, s, v + 16);
+    unpack4(c.z, c.w, s, v + 20);
   }
+  // upper = 0: spins 0-1 (reals 0-3, 8-11, 16-19); 1: spins 2-3 (+4)
   __device__ __forceinline__ static void load_half(const __half* __restrict__ p, int pad, int g,
                                                    int upper, float v[24]) {
-    const uint2* q = reinterpret_cast<const uint2*>(p);
+    const uint4* q = reinterpret_cast<const uint4*>(p);
     const float s = scale(p, pad, g);
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-      int j = 2 * c + (upper ? 1 : 0);
-      unpack4(__ldg(q + (size_t)j * pad + g), s, v + 4 * j);
-    }
+    const int o = upper ? 4 : 0;
+    const uint4 a = __ldg(q + (size_t)(upper ? pad : 0) + g);
+    const uint2 c = __ldg(reinterpret_cast<const uint2*>(q + (size_t)2 * pad) + 2 * (size_t)g + (upper ? 1 : 0));
+    unpack4(a.x, a.y, s, v + o);
+    unpack4(a.z, a.w, s, v + 8 + o);
+    unpack4(c, s, v + 16 + o);
   }
   __device__ __forceinline__ static void store_spinor(__half* __restrict__ p, int pad, int g,
                                                       const float v[24]) {
@@ -351,26 +370,71 @@ struct IO<H16> {
     // solution decays below FP32's normal range across a large lattice).
     const bool keep = n >= 1e-30f;
     const float inv = keep ? 1.0f / n : 0.0f;
-    uint2* q = reinterpret_cast<uint2*>(p);
-#pragma unroll
-    for (int j = 0; j < 6; j++) q[(size_t)j * pad + g] = pack4(v + 4 * j, inv);
-    reinterpret_cast<float*>(q + (size_t)6 * pad)[g] = keep ? n : 0.0f;
+    uint4* q = reinterpret_cast<uint4*>(p);
+    const uint2 a0 = pack4(v + 0, inv), a1 = pack4(v + 8, inv);
+    const uint2 b0 = pack4(v + 4, inv), b1 = pack4(v + 12, inv);
+    const uint2 c0 = pack4(v + 16, inv), c1 = pack4(v + 20, inv);
+    q[g] = make_uint4(a0.x, a0.y, a1.x, a1.y);
+    q[(size_t)pad + g] = make_uint4(b0.x, b0.y, b1.x, b1.y);
+    q[(size_t)2 * pad + g] = make_uint4(c0.x, c0.y, c1.x, c1.y);
+    reinterpret_cast<float*>(q + (size_t)3 * pad)[g] = keep ? n : 0.0f;
   }
+  // Links: per direction 36 bytes a site, as two 16-byte planes (complex
+  // elements 0-3 and 4-7 of the row-major matrix) and one 4-byte plane
+  // (element 8): three loads per link.
   __device__ __forceinline__ static void load_link(const __half* __restrict__ U, int pad, int mu,
                                                    int g, float u[18]) {
-    const __half2* q = reinterpret_cast<const __half2*>(U);
+    const char* base = reinterpret_cast<const char*>(U) + (size_t)mu * 36 * pad;
+    const uint4 a = __ldg(reinterpret_cast<const uint4*>(base) + g);
+    const uint4 b = __ldg(reinterpret_cast<const uint4*>(base + (size_t)16 * pad) + g);
+    const unsigned c = __ldg(reinterpret_cast<const unsigned*>(base + (size_t)32 * pad) + g);
+    const unsigned w[9] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c};
 #pragma unroll
     for (int e = 0; e < 9; e++) {
-      float2 f = __half22float2(__ldg(q + (size_t)(mu * 9 + e) * pad + g));
+      __half2 h;
+      memcpy(&h, &w[e], 4);
+      const float2 f = __half22float2(h);
       u[2 * e] = f.x;
       u[2 * e + 1] = f.y;
     }
   }
+  __device__ __forceinline__ static void store_link(__half* U, int pad, int mu, int g,
+                                                    const float u[18]) {
+    char* base = reinterpret_cast<char*>(U) + (size_t)mu * 36 * pad;
+    unsigned w[9];
+#pragma unroll
+    for (int e = 0; e < 9; e++) {
+      const __half2 h = __floats2half2_rn(u[2 * e], u[2 * e + 1]);
+      memcpy(&w[e], &h, 4);
+    }
+    reinterpret_cast<uint4*>(base)[g] = make_uint4(w[0], w[1], w[2], w[3]);
+    reinterpret_cast<uint4*>(base + (size_t)16 * pad)[g] = make_uint4(w[4], w[5], w[6], w[7]);
+    reinterpret_cast<unsigned*>(base + (size_t)32 * pad)[g] = w[8];
+  }
+  // Clover: the 72 reals (two chiral blocks of 36) as nine 16-byte planes;
+  // block 0 is planes 0-3 and the first half of plane 4, block 1 the second
+  // half of plane 4 and planes 5-8.
   __device__ __forceinline__ static void load_clover_block(const __half* __restrict__ C, int pad,
                                                            int g, int blk, float a[36]) {
-    const uint2* q = reinterpret_cast<const uint2*>(C);
+    const uint4* q = reinterpret_cast<const uint4*>(C);
+    const uint2 mid = __ldg(reinterpret_cast<const uint2*>(q + (size_t)4 * pad) + 2 * (size_t)g + blk);
+    const int first = blk ? 5 : 0, o = blk ? 4 : 0;
+    if (blk) unpack4(mid, 1.0f, a);
 #pragma unroll
-    for (int j = 0; j < 9; j++) unpack4(__ldg(q + (size_t)(9 * blk + j) * pad + g), 1.0f, a + 4 * j);
+    for (int j = 0; j < 4; j++) {
+      const uint4 t = __ldg(q + (size_t)(first + j) * pad + g);
+      unpack4(t.x, t.y, 1.0f, a + o + 8 * j);
+      unpack4(t.z, t.w, 1.0f, a + o + 8 * j + 4);
+    }
+    if (!blk) unpack4(mid, 1.0f, a + 32);
+  }
+  __device__ __forceinline__ static void store_clover(__half* C, int pad, int g, const float a[72]) {
+    uint4* q = reinterpret_cast<uint4*>(C);
+#pragma unroll
+    for (int j = 0; j < 9; j++) {
+      const uint2 x = pack4(a + 8 * j, 1.0f), y = pack4(a + 8 * j + 4, 1.0f);
+      q[(size_t)j * pad + g] = make_uint4(x.x, x.y, y.x, y.y);
+    }
   }
 };
 

@@ -238,7 +238,7 @@ R* Ctx::alloc_spinor() {
 template float* Ctx::alloc_spinor<float>();
 template double* Ctx::alloc_spinor<double>();
 
-// FP16 spinor: 6 uint2 planes + one float plane of per-site scales
+// FP16 spinor: three 16-byte planes + one float plane of per-site scales (IO<H16>)
 __half* Ctx::alloc_spinor_h() {
   void* p = nullptr;
   const size_t bytes = (size_t)(6 * 8 + 4) * spad(G);
