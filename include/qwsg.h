@@ -232,6 +232,13 @@ int qwsg_spinor_to_bqcd_s(qwsg_lattice* lat, double* even, double* odd, const fl
  * captured on first use per buffers/nsap/nm/kappa, replayed afterwards; not
  * used while kernel timing is on or on the legacy default stream */
 int qwsg_set_graphs(qwsg_lattice* lat, int enable);
+/* FP32 links in 12-real form (no counterpart in the reference): with mode
+ * 1 (default) the FP32 Dirac kernels read the first two rows of each link
+ * and rebuild the third when every loaded link is SU(3) to 1e-5 (checked
+ * on the device once per load); mode 0 always reads all 18 reals.
+ * qwsg_link_compression reports whether the 12-real form is in use. */
+int qwsg_set_link_compression(qwsg_lattice* lat, int mode);
+int qwsg_link_compression(qwsg_lattice* lat, int* active);
 /* threads per CTA of the Dirac-operator kernels on this handle (64, 128
  * (default) or 256); a batch handle starts with its parent's value.  No
  * counterpart in the reference (its loops are OpenMP threads over sites). */

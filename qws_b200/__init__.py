@@ -62,6 +62,8 @@ def load_library(path: str | os.PathLike | None = None):
         "qwsg_build_clover": [vp, c_double],
         "qwsg_set_graphs": [vp, c_int],
         "qwsg_set_hop_threads": [vp, c_int],
+        "qwsg_set_link_compression": [vp, c_int],
+        "qwsg_link_compression": [vp, ip],
         "qwsg_mtdagmt_d": [vp, vp, vp],
         "qwsg_load_gauge_bqcd": [vp, vp, vp],
         "qwsg_load_clover_bqcd": [vp, vp, vp],
@@ -493,6 +495,16 @@ class Lattice:
 
     def set_graphs(self, enable=True):
         _check(self.lib.qwsg_set_graphs(self.h, 1 if enable else 0))
+
+    def set_link_compression(self, mode=1):
+        """1: FP32 kernels read 12-real links when the links are SU(3); 0: never."""
+        _check(self.lib.qwsg_set_link_compression(self.h, int(mode)))
+
+    def link_compression(self):
+        """True when the FP32 kernels read the 12-real links."""
+        v = ctypes.c_int()
+        _check(self.lib.qwsg_link_compression(self.h, ctypes.byref(v)))
+        return bool(v.value)
 
     def set_hop_threads(self, threads):
         """Threads per CTA of the Dirac-operator kernels (64, 128 or 256)."""

@@ -277,6 +277,27 @@ int qwsg_set_graphs(qwsg_lattice* l, int enable) {
   });
 }
 
+int qwsg_set_link_compression(qwsg_lattice* l, int mode) {
+  return guarded([&] {
+    check_ctx(l);
+    not_batch(l, "qwsg_set_link_compression");
+    if (mode != 0 && mode != 1) throw Error(1, "qwsg_set_link_compression: mode must be 0 or 1");
+    Ctx& c = *l->c;
+    QWSG_CUDA(cudaStreamSynchronize(c.st));
+    c.link_compress = mode;
+    c.links12_valid = false;
+    c.ensure_links12();
+  });
+}
+int qwsg_link_compression(qwsg_lattice* l, int* active) {
+  return guarded([&] {
+    check_ctx(l);
+    Ctx& c = *l->c;
+    c.ensure_links12();
+    if (active) *active = c.links12_on ? 1 : 0;
+  });
+}
+
 int qwsg_set_hop_threads(qwsg_lattice* l, int threads) {
   return guarded([&] {
     check_ctx(l);

@@ -269,7 +269,69 @@ __global__ void k_fields_s2h(Geom G, __half* Uh, const float* __restrict__ Us, _
   IO<H16>::store_clover(Ch, G.pad, g, a);
 }
 
+// largest deviation from SU(3) of the FP32 link of one (site, direction)
+__global__ void k_su3_dev(Geom G, const float* __restrict__ Us, unsigned* dev) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  float worst = 0;
+  if (g < G.V) {
+    for (int mu = 0; mu < 4; mu++) {
+      float u[18];
+      IO<float>::load_link(Us, G.pad, mu, g, u);
+      double d = 0;
+      for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {  // (U U^+)_ab - delta_ab
+          double re = 0, im = 0;
+          for (int k = 0; k < 3; k++) {
+            const double xr = u[2 * (3 * a + k)], xi = u[2 * (3 * a + k) + 1];
+            const double yr = u[2 * (3 * b + k)], yi = -u[2 * (3 * b + k) + 1];
+            re += xr * yr - xi * yi;
+            im += xr * yi + xi * yr;
+          }
+          d = fmax(d, fabs(re - (a == b)) + fabs(im));
+        }
+      // det U by the first row's cofactors
+      double dr = 0, di = 0;
+      for (int b = 0; b < 3; b++) {
+        const int b1 = (b + 1) % 3, b2 = (b + 2) % 3;
+        const double pr = (double)u[6 + 2 * b1] * u[12 + 2 * b2] - (double)u[7 + 2 * b1] * u[13 + 2 * b2] -
+                          ((double)u[6 + 2 * b2] * u[12 + 2 * b1] - (double)u[7 + 2 * b2] * u[13 + 2 * b1]);
+        const double pi = (double)u[6 + 2 * b1] * u[13 + 2 * b2] + (double)u[7 + 2 * b1] * u[12 + 2 * b2] -
+                          ((double)u[6 + 2 * b2] * u[13 + 2 * b1] + (double)u[7 + 2 * b2] * u[12 + 2 * b1]);
+        dr += u[2 * b] * pr - u[2 * b + 1] * pi;
+        di += u[2 * b] * pi + u[2 * b + 1] * pr;
+      }
+      d = fmax(d, fabs(dr - 1) + fabs(di));
+      worst = fmaxf(worst, isfinite(d) ? (float)d : 3.0e38f);
+    }
+  }
+  // non-negative floats order like their bit patterns
+  for (int o = 16; o > 0; o >>= 1) worst = fmaxf(worst, __shfl_xor_sync(0xffffffffu, worst, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(dev, __float_as_uint(worst));
+}
+
+__global__ void k_compress12(Geom G, float* __restrict__ U12, const float* __restrict__ Us) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G.V) return;
+  float4* q = reinterpret_cast<float4*>(U12);
+  for (int mu = 0; mu < 4; mu++) {
+    float u[18];
+    IO<float>::load_link(Us, G.pad, mu, g, u);
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+      q[(size_t)(3 * mu + k) * G.pad + g] = make_float4(u[4 * k], u[4 * k + 1], u[4 * k + 2], u[4 * k + 3]);
+  }
+}
+
 }  // namespace
+
+void links_su3_deviation(const Geom& G, const float* Us, unsigned* dev, cudaStream_t st) {
+  count_launch();
+  k_su3_dev<<<nb(G.V), 128, 0, st>>>(G, Us, dev);
+}
+void links_compress12(const Geom& G, float* U12, const float* Us, cudaStream_t st) {
+  count_launch();
+  k_compress12<<<nb(G.V), 128, 0, st>>>(G, U12, Us);
+}
 
 void spinor_s2h(const Geom& G, __half* dst, const float* src, cudaStream_t st) {
   count_launch();

@@ -49,6 +49,13 @@ struct Ctx {
   double* Ud = nullptr;
   double* Cd = nullptr;
   float* Us = nullptr;
+  // FP32 links in 12-real form, used by the FP32 Dirac kernels when the
+  // links are SU(3) to FP32 accuracy (link_compress: 1 = automatic, 0 = off)
+  float* Us12 = nullptr;
+  bool links12_valid = false;  // the check / copy reflects the current Us
+  bool links12_on = false;
+  int link_compress = 1;
+  void ensure_links12();
   float* Cs = nullptr;
 
   // reductions

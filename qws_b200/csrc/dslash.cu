@@ -17,6 +17,8 @@
 //   T    storage format (float, double, H16); arithmetic in Arith<T>::R.
 // Faces are not packed: a face hop reads the neighbouring block's site of
 // the source field directly from HBM (the whole lattice is resident).
+#include <type_traits>
+
 #include "kernels.h"
 #include "lattice.cuh"
 
@@ -39,23 +41,32 @@ __device__ __forceinline__ void do_hop(const HopArgs<T>& a, const Site& s, int g
     gn = nbr_across(a.G, s, MU, DIR, &ncol);
     if (ncol == a.zero_col) return;  // that colour's source is defined as zero
   }
-  R v[24];
+  R v[24], sc;
   const int sp = spad(a.G), en = sentry(a.G, gn, rhs);
+  // the projection and the link product are linear: the source's scale
+  // (FP16 storage) is applied once, in the reconstruction
   if (MU == 3)
-    IO<T>::load_half(a.src, sp, en, DIR > 0, v);
+    IO<T>::load_half_raw(a.src, sp, en, DIR > 0, v, sc);
   else
-    IO<T>::load_spinor(a.src, sp, en, v);
+    IO<T>::load_spinor_raw(a.src, sp, en, v, sc);
   R h[12], r[12], u[18];
   project<R, MU, DIR>(v, h);
-  IO<T>::load_link(a.U, a.G.pad, MU, DIR > 0 ? g : gn, u);
+  if constexpr (std::is_same<T, float>::value) {
+    if (a.U12)
+      load_link12(a.U12, a.G.pad, MU, DIR > 0 ? g : gn, u);
+    else
+      IO<T>::load_link(a.U, a.G.pad, MU, DIR > 0 ? g : gn, u);
+  } else {
+    IO<T>::load_link(a.U, a.G.pad, MU, DIR > 0 ? g : gn, u);
+  }
   if (DIR > 0)
     link_mul<R, false>(u, h, r);
   else
     link_mul<R, true>(u, h, r);
-  R f = 1;
+  R f = sc;
   if (MU == 3) {
-    f = 2;
-    if (face && (DIR > 0 ? s.bc[3] == a.G.NB[3] - 1 : s.bc[3] == 0)) f = (R)(2 * a.G.tbc);
+    f = 2 * sc;
+    if (face && (DIR > 0 ? s.bc[3] == a.G.NB[3] - 1 : s.bc[3] == 0)) f = (R)(2 * a.G.tbc) * sc;
   }
   reconstruct<R, MU, DIR>(r, acc, f);
 }

@@ -25,6 +25,7 @@ struct HopArgs {
   const S* aux;   // b (EPI_JINV) or the SAP right-hand side `in` (EPI_SAPE)
   S* out;
   const S* U;     // gauge planes
+  const S* U12;   // FP32 only: links in 12-real form (null: use U)
   const S* C;     // clover planes
   typename Arith<T>::R coef;
   const int* list;  // if set: thread i handles site list[i], else site0 + i
@@ -125,6 +126,11 @@ void bqcd_to_planes_spinor(const Geom& G, R* dst, const double* both, const int*
 template <typename R>
 void planes_to_bqcd_spinor(const Geom& G, double* both, const R* src, const int* map, int rhs,
                            cudaStream_t st);
+// 12-real FP32 links: worst deviation of the FP32 links from SU(3)
+// (max over sites and directions of |U U^+ - 1| and |det U - 1|, into *dev
+// as float bits) and the compressed copy (first two rows)
+void links_su3_deviation(const Geom& G, const float* Us, unsigned* dev, cudaStream_t st);
+void links_compress12(const Geom& G, float* U12, const float* Us, cudaStream_t st);
 // FP32 planes <-> FP16 planes with per-site scales (IO<H16> format)
 void spinor_s2h(const Geom& G, __half* dst, const float* src, cudaStream_t st);
 void spinor_h2s(const Geom& G, float* dst, const __half* src, cudaStream_t st);

@@ -201,6 +201,17 @@ struct IO<float> {
       v[4 * j + 3] = t.w;
     }
   }
+  // the *_raw loads return the stored values and the site's scale (1 here)
+  __device__ __forceinline__ static void load_spinor_raw(const float* __restrict__ p, int pad,
+                                                         int g, float v[24], float& s) {
+    load_spinor(p, pad, g, v);
+    s = 1.0f;
+  }
+  __device__ __forceinline__ static void load_half_raw(const float* __restrict__ p, int pad, int g,
+                                                       int upper, float v[24], float& s) {
+    load_half(p, pad, g, upper, v);
+    s = 1.0f;
+  }
   // spins {s0, s0+1} only (t-direction projections need half the spinor)
   __device__ __forceinline__ static void load_half(const float* __restrict__ p, int pad, int g,
                                                    int upper, float v[24]) {
@@ -257,6 +268,16 @@ struct IO<double> {
       v[2 * j] = t.x;
       v[2 * j + 1] = t.y;
     }
+  }
+  __device__ __forceinline__ static void load_spinor_raw(const double* __restrict__ p, int pad,
+                                                         int g, double v[24], double& s) {
+    load_spinor(p, pad, g, v);
+    s = 1.0;
+  }
+  __device__ __forceinline__ static void load_half_raw(const double* __restrict__ p, int pad,
+                                                       int g, int upper, double v[24], double& s) {
+    load_half(p, pad, g, upper, v);
+    s = 1.0;
   }
   __device__ __forceinline__ static void load_half(const double* __restrict__ p, int pad, int g,
                                                    int upper, double v[24]) {
@@ -334,29 +355,47 @@ struct IO<H16> {
     memcpy(&t.y, &b, 4);
     return t;
   }
+  // the stored (normalised) values; the site's scale in s
+  __device__ __forceinline__ static void load_spinor_raw(const __half* __restrict__ p, int pad,
+                                                         int g, float v[24], float& s) {
+    const uint4* q = reinterpret_cast<const uint4*>(p);
+    s = scale(p, pad, g);
+    const uint4 a = __ldg(q + g), b = __ldg(q + (size_t)pad + g), c = __ldg(q + (size_t)2 * pad + g);
+    unpack4(a.x, a.y, 1.0f, v + 0);
+    unpack4(a.z, a.w, 1.0f, v + 8);
+    unpack4(b.x, b.y, 1.0f, v + 4);
+    unpack4(b.z, b.w, 1.0f, v + 12);
+    unpack4(c.x, c.y, 1.0f, v + 16);
+    unpack4(c.z, c.w, 1.0f, v + 20);
+  }
   __device__ __forceinline__ static void load_spinor(const __half* __restrict__ p, int pad, int g,
                                                      float v[24]) {
-    const uint4* q = reinterpret_cast<const uint4*>(p);
-    const float s = scale(p, pad, g);
-    const uint4 a = __ldg(q + g), b = __ldg(q + (size_t)pad + g), c = __ldg(q + (size_t)2 * pad + g);
-    unpack4(a.x, a.y, s, v + 0);
-    unpack4(a.z, a.w, s, v + 8);
-    unpack4(b.x, b.y, s, v + 4);
-    unpack4(b.z, b.w, s, v + 12);
-    unpack4(c.x, c.y, s, v + 16);
-    unpack4(c.z, c.w, s, v + 20);
+    float s;
+    load_spinor_raw(p, pad, g, v, s);
+#pragma unroll
+    for (int j = 0; j < 24; j++) v[j] *= s;
   }
   // upper = 0: spins 0-1 (reals 0-3, 8-11, 16-19); 1: spins 2-3 (+4)
-  __device__ __forceinline__ static void load_half(const __half* __restrict__ p, int pad, int g,
-                                                   int upper, float v[24]) {
+  __device__ __forceinline__ static void load_half_raw(const __half* __restrict__ p, int pad,
+                                                       int g, int upper, float v[24], float& s) {
     const uint4* q = reinterpret_cast<const uint4*>(p);
-    const float s = scale(p, pad, g);
+    s = scale(p, pad, g);
     const int o = upper ? 4 : 0;
     const uint4 a = __ldg(q + (size_t)(upper ? pad : 0) + g);
     const uint2 c = __ldg(reinterpret_cast<const uint2*>(q + (size_t)2 * pad) + 2 * (size_t)g + (upper ? 1 : 0));
-    unpack4(a.x, a.y, s, v + o);
-    unpack4(a.z, a.w, s, v + 8 + o);
-    unpack4(c, s, v + 16 + o);
+    unpack4(a.x, a.y, 1.0f, v + o);
+    unpack4(a.z, a.w, 1.0f, v + 8 + o);
+    unpack4(c, 1.0f, v + 16 + o);
+  }
+  __device__ __forceinline__ static void load_half(const __half* __restrict__ p, int pad, int g,
+                                                   int upper, float v[24]) {
+    float s;
+    load_half_raw(p, pad, g, upper, v, s);
+    const int o = upper ? 4 : 0;
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+      for (int k = 0; k < 4; k++) v[8 * c + o + k] *= s;
   }
   __device__ __forceinline__ static void store_spinor(__half* __restrict__ p, int pad, int g,
                                                       const float v[24]) {
@@ -544,19 +583,20 @@ __device__ __forceinline__ void reconstruct(const R r[12], R acc[24], R f) {
       }
       continue;
     }
-    AR(c, 0) += r0; AI(c, 0) += i0; AR(c, 1) += r1; AI(c, 1) += i1;
+    // f: the source's scale (FP16 storage; 1 otherwise, folded at compile time)
+    AR(c, 0) += f * r0; AI(c, 0) += f * i0; AR(c, 1) += f * r1; AI(c, 1) += f * i1;
     if (MU == 0 && DIR > 0) {
-      AR(c, 2) -= i1; AI(c, 2) += r1; AR(c, 3) -= i0; AI(c, 3) += r0;
+      AR(c, 2) -= f * i1; AI(c, 2) += f * r1; AR(c, 3) -= f * i0; AI(c, 3) += f * r0;
     } else if (MU == 0) {
-      AR(c, 2) += i1; AI(c, 2) -= r1; AR(c, 3) += i0; AI(c, 3) -= r0;
+      AR(c, 2) += f * i1; AI(c, 2) -= f * r1; AR(c, 3) += f * i0; AI(c, 3) -= f * r0;
     } else if (MU == 1 && DIR > 0) {
-      AR(c, 2) += r1; AI(c, 2) += i1; AR(c, 3) -= r0; AI(c, 3) -= i0;
+      AR(c, 2) += f * r1; AI(c, 2) += f * i1; AR(c, 3) -= f * r0; AI(c, 3) -= f * i0;
     } else if (MU == 1) {
-      AR(c, 2) -= r1; AI(c, 2) -= i1; AR(c, 3) += r0; AI(c, 3) += i0;
+      AR(c, 2) -= f * r1; AI(c, 2) -= f * i1; AR(c, 3) += f * r0; AI(c, 3) += f * i0;
     } else if (MU == 2 && DIR > 0) {
-      AR(c, 2) -= i0; AI(c, 2) += r0; AR(c, 3) += i1; AI(c, 3) -= r1;
+      AR(c, 2) -= f * i0; AI(c, 2) += f * r0; AR(c, 3) += f * i1; AI(c, 3) -= f * r1;
     } else {
-      AR(c, 2) += i0; AI(c, 2) -= r0; AR(c, 3) -= i1; AI(c, 3) += r1;
+      AR(c, 2) += f * i0; AI(c, 2) -= f * r0; AR(c, 3) -= f * i1; AI(c, 3) += f * r1;
     }
   }
 }
@@ -612,6 +652,33 @@ __device__ __forceinline__ void clover_apply(const typename Store<T>::type* __re
     v[8 * c + 3] = yi[0][3 + c] + yi[1][3 + c];
     v[8 * c + 6] = yr[0][3 + c] - yr[1][3 + c];
     v[8 * c + 7] = yi[0][3 + c] - yi[1][3 + c];
+  }
+}
+
+// FP32 links in 12-real form: the first two rows of U_mu (6 complex) as three
+// float4 planes per direction; the third row of an SU(3) matrix is the
+// complex conjugate of the cross product of the first two,
+//   u_2b = conj(u_0,b+1 u_1,b+2 - u_0,b+2 u_1,b+1)   (indices mod 3).
+__device__ __forceinline__ void load_link12(const float* __restrict__ U12, int pad, int mu, int g,
+                                            float u[18]) {
+  const float4* q = reinterpret_cast<const float4*>(U12);
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const float4 t = __ldg(q + (size_t)(3 * mu + k) * pad + g);
+    u[4 * k] = t.x;
+    u[4 * k + 1] = t.y;
+    u[4 * k + 2] = t.z;
+    u[4 * k + 3] = t.w;
+  }
+#pragma unroll
+  for (int b = 0; b < 3; b++) {
+    const int b1 = (b + 1) % 3, b2 = (b + 2) % 3;
+    const float ar = u[2 * b1], ai = u[2 * b1 + 1], br = u[6 + 2 * b2], bi = u[6 + 2 * b2 + 1];
+    const float cr = u[2 * b2], ci = u[2 * b2 + 1], dr = u[6 + 2 * b1], di = u[6 + 2 * b1 + 1];
+    const float re = (ar * br - ai * bi) - (cr * dr - ci * di);
+    const float im = (ar * bi + ai * br) - (cr * di + ci * dr);
+    u[12 + 2 * b] = re;
+    u[12 + 2 * b + 1] = -im;
   }
 }
 

@@ -29,11 +29,33 @@ HopArgs<T> hop_args(const Geom& G, const typename Store<T>::type* U,
   return a;
 }
 
-// algorithmic bytes moved per handled site: each spinor stream once per
-// right-hand side, links and clover once per site
+// the resident fields of the handle; FP32 launches read the 12-real links
+// when they are on
 template <typename T>
-double hop_bytes(int sel, int epi, int nr) {
-  const double sp = Bytes<T>::spinor * nr, lc = Bytes<T>::links + Bytes<T>::clover;
+HopArgs<T> hop_args_c(Ctx& c);
+template <>
+HopArgs<float> hop_args_c<float>(Ctx& c) {
+  c.ensure_links12();
+  auto a = hop_args<float>(c.G, c.Us, c.Cs);
+  a.U12 = c.links12_on ? c.Us12 : nullptr;
+  return a;
+}
+template <>
+HopArgs<double> hop_args_c<double>(Ctx& c) {
+  return hop_args<double>(c.G, c.Ud, c.Cd);
+}
+template <>
+HopArgs<H16> hop_args_c<H16>(Ctx& c) {
+  return hop_args<H16>(c.G, c.Uh, c.Ch);
+}
+
+// algorithmic bytes moved per handled site: each spinor stream once per
+// right-hand side, links and clover once per site (48 B less per link
+// direction pair for 12-real FP32 links)
+template <typename T>
+double hop_bytes(int sel, int epi, int nr, bool links12 = false) {
+  const double sp = Bytes<T>::spinor * nr,
+               lc = (links12 ? Bytes<T>::links * 2 / 3 : Bytes<T>::links) + Bytes<T>::clover;
   if (epi == EPI_JINV) return 3 * sp + lc;  // src, b, out
   if (epi == EPI_SAPE) return 4 * sp + lc;  // a, in, s (r+w)
   if (epi == EPI_ADD) return 3 * sp + lc;   // out (r+w), one face neighbour
@@ -73,7 +95,8 @@ void run_hop(Ctx& c, int sel, int epi, const HopArgs<T>& a) {
   long sites = a.nsites;
   if (sel == HOP_OUTER && !a.list) sites = face_sites_per_colour(c.G) * (a.nsites == c.G.V ? 2 : 1);
   if (a.dom >= 0) sites /= 2;
-  c.recs.push_back({kind_of<T>(sel, epi), e0, e1, (double)sites * hop_bytes<T>(sel, epi, c.G.nr)});
+  c.recs.push_back({kind_of<T>(sel, epi), e0, e1,
+                    (double)sites * hop_bytes<T>(sel, epi, c.G.nr, a.U12 != nullptr)});
 }
 
 template <typename T>
@@ -306,6 +329,53 @@ void Ctx::ensure_fields_s() {
     QWSG_CUDA(cudaMemsetAsync(Cs, 0, sizeof(float) * 72 * (size_t)G.pad, st));
   }
   fields_h_valid = false;  // the FP16 copies follow the FP32 fields
+  links12_valid = false;   // so does the 12-real link copy
+}
+
+// The FP32 links are checked once per load: if every link is SU(3) to 1e-5
+// (|U U^+ - 1| and |det U - 1|), the Dirac kernels read the 12-real copy and
+// rebuild the third row (a third fewer link bytes).  Fields that are not
+// SU(3), e.g. the reference's own test fields, keep the 18-real links.
+void Ctx::ensure_links12() {
+  if (parent) {
+    parent->ensure_links12();
+    Us12 = parent->Us12;
+    if (links12_on != parent->links12_on) {
+      QWSG_CUDA(cudaStreamSynchronize(st));
+      clear_graphs();
+    }
+    links12_on = parent->links12_on;
+    links12_valid = true;
+    return;
+  }
+  if (links12_valid || !Us) return;
+  bool on = false;
+  if (link_compress) {
+    unsigned* dev = rb.counter + 2;
+    QWSG_CUDA(cudaMemsetAsync(dev, 0, sizeof(unsigned), st));
+    links_su3_deviation(G, Us, dev, st);
+    check_launch("links_su3_deviation");
+    unsigned h = 0;
+    QWSG_CUDA(cudaMemcpyAsync(&h, dev, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    QWSG_CUDA(cudaStreamSynchronize(st));
+    float worst;
+    std::memcpy(&worst, &h, sizeof(float));
+    on = worst < 1e-5f;
+    if (on) {
+      if (!Us12) {
+        QWSG_CUDA(cudaMalloc(&Us12, sizeof(float) * 48 * (size_t)G.pad));
+        owned.push_back(Us12);
+      }
+      links_compress12(G, Us12, Us, st);
+      check_launch("links_compress12");
+    }
+  }
+  if (on != links12_on) {  // captured launches carry the link form
+    QWSG_CUDA(cudaStreamSynchronize(st));
+    clear_graphs();
+  }
+  links12_on = on;
+  links12_valid = true;
 }
 // FP16 copies of the FP32 gauge and clover planes (made on first use after
 // every load)
@@ -320,6 +390,7 @@ void Ctx::sync_from_parent(bool half) {
   Uh = parent->Uh;
   Ch = parent->Ch;
   fields_h_valid = parent->fields_h_valid;
+  links12_valid = false;  // taken from the parent at the next FP32 launch
   kappa = parent->kappa;
   // the parent's field uploads and conversions are on its stream
   if (parent->st != st) {
@@ -361,7 +432,7 @@ void Ctx::check_launch(const char* what) {
 // operators
 // ---------------------------------------------------------------------------
 void dslash_full_d(Ctx& c, double* out, const double* in) {
-  auto a = hop_args<double>(c.G, c.Ud, c.Cd);
+  auto a = hop_args_c<double>(c);
   a.src = in;
   a.out = out;
   a.coef = -c.kappa;
@@ -373,7 +444,7 @@ void dslash_full_d(Ctx& c, double* out, const double* in) {
 }
 
 void dslash_full_s(Ctx& c, float* out, const float* in) {
-  auto a = hop_args<float>(c.G, c.Us, c.Cs);
+  auto a = hop_args_c<float>(c);
   a.src = in;
   a.out = out;
   a.coef = -(float)c.kappa;
@@ -385,7 +456,7 @@ void dslash_full_s(Ctx& c, float* out, const float* in) {
 
 template <typename R>
 void dslash_inner(Ctx& c, R* out, const R* in, int col, int dom) {
-  auto a = hop_args<R>(c.G, gauge_of<R>(c), clover_of<R>(c));
+  auto a = hop_args_c<R>(c);
   a.src = in;
   a.out = out;
   a.coef = (R)(-c.kappa);
@@ -402,7 +473,7 @@ template void dslash_inner<double>(Ctx&, double*, const double*, int, int);
 template <typename T>
 static void outer_t(Ctx& c, typename Store<T>::type* out, const typename Store<T>::type* in,
                     int col, int dom, double factor, int zero_col) {
-  auto a = hop_args<T>(c.G, gauge_of<T>(c), clover_of<T>(c));
+  auto a = hop_args_c<T>(c);
   a.src = in;
   a.out = out;
   a.coef = (typename Arith<T>::R)factor;
@@ -459,7 +530,7 @@ template <typename T>
 static void jinv_t(Ctx& c, typename Store<T>::type* x, const typename Store<T>::type* b, int col,
                    int nm, typename Store<T>::type* tmp) {
   const int steps = nm < 1 ? 1 : nm;
-  auto a = hop_args<T>(c.G, gauge_of<T>(c), clover_of<T>(c));
+  auto a = hop_args_c<T>(c);
   a.aux = b;
   a.coef = (typename Arith<T>::R)c.kappa;
   site_range(c, col, a.site0, a.nsites);
@@ -495,7 +566,7 @@ static void sap_sweeps_t(Ctx& c, typename Store<T>::type* s, typename Store<T>::
     for (int e = 0; e < 2; e++) {
       const int o = 1 - e;
       jinv_t<T>(c, a, s, e, nm, tmp);
-      auto h = hop_args<T>(c.G, gauge_of<T>(c), clover_of<T>(c));
+      auto h = hop_args_c<T>(c);
       h.src = a;
       h.aux = in;
       h.out = s;
@@ -527,6 +598,9 @@ void Ctx::clear_graphs() {
 // body allocates or builds must exist before the first capture.
 template <typename F>
 static void graphed(Ctx& c, const Ctx::GraphKey& k, F&& body) {
+  // the link form is settled before a capture (its check reads back a result)
+  // and a change of form drops the graphs captured with the other one
+  c.ensure_links12();
   if (c.timing || !c.use_graphs || c.st == nullptr || c.st == cudaStreamLegacy ||
       c.st == cudaStreamPerThread) {
     body();

@@ -37,6 +37,8 @@ def main():
     ap.add_argument("--kappa", type=float, default=0.1365)
     ap.add_argument("--csw", type=float, default=1.7)
     ap.add_argument("--nrhs", type=int, default=1)
+    ap.add_argument("--links18", action="store_true",
+                    help="FP32 kernels read 18-real links even for SU(3) fields")
     a = ap.parse_args()
     L = tuple(int(v) for v in a.lattice.split(","))
     NB = tuple(int(v) for v in a.blocks.split(","))
@@ -45,14 +47,18 @@ def main():
     b = qws_b200.gen_source(L, 12)
     st = torch.cuda.Stream()
     base = qws_b200.Lattice(L, NB, tbc=-1, kappa=a.kappa, stream=st)
+    if a.links18:
+        base.set_link_compression(0)
     base.load_fields(U, C)
+    links12 = base.link_compression()
     del U, C
     V, nr = base.V, a.nrhs
     lat = base if nr == 1 else base.batch(nr, stream=st)
     if nr > 1:
         b = np.stack([b] * nr)
     # algorithmic bytes per site: spinor streams per RHS + links + clover
-    sp32, sp64, lc32, lc64 = 96 * nr, 192 * nr, 576, 1152
+    # (FP32 links: 48 instead of 72 B per direction in 12-real form)
+    sp32, sp64, lc32, lc64 = 96 * nr, 192 * nr, (192 if links12 else 288) + 288, 1152
     with torch.cuda.stream(st):
         bs = lat.to_device(b.astype(np.float32))
         bd = lat.to_device(b)
@@ -86,6 +92,7 @@ def main():
         torch.cuda.synchronize()
     us = e0.elapsed_time(e1) * 1e3 / a.iters
     res = {"kernel": k, "lattice": "x".join(map(str, L)), "blocks": list(NB), "nrhs": nr,
+           "fp32_links": 12 if links12 else 18,
            "us_per_launch": us, "us_per_rhs": us / nr, "plaquette": plaq}
     if nbytes:
         res["bytes_per_launch"] = nbytes
