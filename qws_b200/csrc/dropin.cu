@@ -77,12 +77,20 @@ Ctx& ctx() {
   std::exit(1);
 }
 
+// QWS ends the program on errors (exit(1)); with QWSG_NO_EXIT set in the
+// environment the entry point returns instead, leaving the message in
+// qwsg_last_error() and its outputs unspecified
 template <typename F>
 void guard(const char* name, F&& f) {
   try {
     f();
   } catch (const std::exception& e) {
-    set_error(e.what());
+    set_error(std::string(name) + ": " + e.what());
+    static const bool no_exit = std::getenv("QWSG_NO_EXIT") != nullptr;
+    if (no_exit) {
+      fprintf(stderr, "qws_b200: %s: %s\n", name, e.what());
+      return;
+    }
     die(std::string(name) + ": " + e.what());
   }
 }
