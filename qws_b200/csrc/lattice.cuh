@@ -61,7 +61,7 @@ struct Geom {
   int nbh0;    // NB[0] / 2
   int tbc;     // +1 periodic / -1 antiperiodic in t (fbc_f[3], qws.cc:298-310)
   int pad;     // plane stride in elements
-  int str[4];  // in-block strides: 1, B0, B0*B1, B0*B1*B2
+  int str[4];  // in-block strides of x, y, z, t (block_local)
   // right-hand sides per spinor field (a power of two, 1..32).  Spinor
   // fields interleave them RHS-minor: RHS r of site g is entry
   // (g << lgnr) + r of planes with stride pad << lgnr, so the threads of one
@@ -73,7 +73,7 @@ struct Geom {
   // host-side only, chosen per lattice)
   int hop_threads;
   // multipliers for the divisions of the site decoding
-  FastDiv fB[4], fVb, fnbh0, fNB1, fNB2;
+  FastDiv fB[4], fVb, fnbh0, fNB1, fNB2, fstr[4];
 };
 
 // plane stride of spinor fields and the entry of (site, rhs)
@@ -88,18 +88,26 @@ struct Site {
   int bc[4];   // block coordinates
 };
 
+// Inside a block, sites are lexicographic in an order of the four
+// directions chosen per block shape (G.str, set in the Ctx constructor):
+// the largest extent is slowest, so the far neighbours of a site are the
+// nearest they can be and stay in L2 between the launches' reads; the
+// second largest is fastest, so every block face but that direction's is a
+// run of whole rows and the face kernels read whole sectors.
+__host__ __device__ __forceinline__ int block_local(const Geom& G, const int lc[4]) {
+  return lc[0] * G.str[0] + lc[1] * G.str[1] + lc[2] * G.str[2] + lc[3] * G.str[3];
+}
+
 __device__ __forceinline__ void decode_site(const Geom& G, int g, Site& s) {
   s.col = g >= G.Vh;
   int rem = g - s.col * G.Vh;
   int k = fdiv(rem, G.fVb);
   int t = rem - k * G.Vb;
-  int t1 = fdiv(t, G.fB[0]);
-  s.lc[0] = t - t1 * G.B[0];
-  int t2 = fdiv(t1, G.fB[1]);
-  s.lc[1] = t1 - t2 * G.B[1];
-  int t3 = fdiv(t2, G.fB[2]);
-  s.lc[2] = t2 - t3 * G.B[2];
-  s.lc[3] = t3;
+#pragma unroll
+  for (int mu = 0; mu < 4; mu++) {
+    const int q = fdiv(t, G.fstr[mu]);
+    s.lc[mu] = q - fdiv(q, G.fB[mu]) * G.B[mu];
+  }
   int q = fdiv(k, G.fnbh0);
   int r = k - q * G.nbh0;
   int q1 = fdiv(q, G.fNB1);
@@ -120,8 +128,7 @@ __host__ __device__ __forceinline__ int dd_index(const Geom& G, const int x[4]) 
   }
   int col = (bc[0] + bc[1] + bc[2] + bc[3]) & 1;
   int blin = bc[0] + G.NB[0] * (bc[1] + G.NB[1] * (bc[2] + G.NB[2] * bc[3]));
-  int local = lc[0] + G.B[0] * (lc[1] + G.B[1] * (lc[2] + G.B[2] * lc[3]));
-  return col * G.Vh + (blin >> 1) * G.Vb + local;
+  return col * G.Vh + (blin >> 1) * G.Vb + block_local(G, lc);
 }
 
 // global coordinates of the site with DD-order index g
@@ -148,9 +155,9 @@ __device__ __forceinline__ int nbr_across(const Geom& G, const Site& s, int mu, 
   }
   int col = (bc0 + bc1 + bc2 + bc3) & 1;
   int blin = bc0 + G.NB[0] * (bc1 + G.NB[1] * (bc2 + G.NB[2] * bc3));
-  int local = l0 + G.B[0] * (l1 + G.B[1] * (l2 + G.B[2] * l3));
+  const int lc[4] = {l0, l1, l2, l3};
   *ncol = col;
-  return col * G.Vh + (blin >> 1) * G.Vb + local;
+  return col * G.Vh + (blin >> 1) * G.Vb + block_local(G, lc);
 }
 
 // ---------------------------------------------------------------------------

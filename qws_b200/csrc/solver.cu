@@ -6,6 +6,7 @@
 // halo/aliasing bookkeeping replaced by fused kernels over the resident
 // lattice.  The SAP sweep is written once for every storage format (FP32,
 // FP16 with per-site scales).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -186,10 +187,36 @@ Ctx::Ctx(const int L[4], const int NB[4], int tbc, int nrhs) {
   G.nbh0 = NB[0] / 2;
   G.tbc = tbc;
   G.pad = round_up(G.V, 128);
-  G.str[0] = 1;
-  G.str[1] = G.B[0];
-  G.str[2] = G.B[0] * G.B[1];
-  G.str[3] = G.B[0] * G.B[1] * G.B[2];
+  // in-block order (block_local).  The faces of the fastest direction are
+  // the only strided ones, so it should have the largest extent; the
+  // slowest direction's stride Vb/B_slowest is how far apart in a launch
+  // a site and its farthest neighbour are read, which must stay within a
+  // few MB for the neighbour to be in L2 (16384 sites, ~13 MB of FP32
+  // operator traffic).  Take the largest-extent direction as fastest whose
+  // remaining largest extent, made slowest, satisfies that; else the
+  // largest slowest and the second largest fastest.  Ties: t, z, y, x.
+  {
+    int d[4] = {3, 2, 1, 0};
+    std::stable_sort(d, d + 4, [&](int a, int b) { return G.B[a] > G.B[b]; });
+    int order[4] = {d[1], d[2], d[3], d[0]};  // fastest .. slowest
+    for (int f = 0; f < 4; f++) {
+      const int slow = d[f == 0 ? 1 : 0];
+      if (G.Vb / G.B[slow] <= 16384) {
+        int k = 0;
+        order[k++] = d[f];
+        for (int j = 0; j < 4; j++)
+          if (j != f && d[j] != slow) order[k++] = d[j];
+        order[3] = slow;
+        break;
+      }
+    }
+    int stride = 1;
+    for (int k = 0; k < 4; k++) {
+      G.str[order[k]] = stride;
+      stride *= G.B[order[k]];
+    }
+  }
+  for (int mu = 0; mu < 4; mu++) G.fstr[mu] = make_fastdiv(G.str[mu]);
   for (int mu = 0; mu < 4; mu++) G.fB[mu] = make_fastdiv(G.B[mu]);
   G.fVb = make_fastdiv(G.Vb);
   G.fnbh0 = make_fastdiv(G.nbh0);
@@ -505,11 +532,10 @@ void Ctx::ensure_face_lists() {
   std::vector<int> lst[2];
   for (int g = 0; g < G.V; g++) {
     int col = g >= G.Vh;
-    int t = (g - col * G.Vh) % G.Vb;
+    const int t = (g - col * G.Vh) % G.Vb;
     bool face = false;
-    for (int mu = 0; mu < 4; mu++) {
-      int l = t % G.B[mu];
-      t /= G.B[mu];
+    for (int mu = 0; mu < 4; mu++) {  // block_local
+      const int l = (t / G.str[mu]) % G.B[mu];
       face |= (l == 0) || (l == G.B[mu] - 1);
     }
     if (face) lst[col].push_back(g);
