@@ -247,6 +247,46 @@ __global__ void k_h2h(Geom G, __half* dst, const __half* __restrict__ src) {
   reinterpret_cast<float*>(d + 3 * sp)[e] = reinterpret_cast<const float*>(s + 3 * sp)[e];
 }
 
+// the same three conversions for FP16 fields of two or more RHS (IOP
+// layout): one thread per (site, RHS pair)
+__global__ void k_s2h_pair(Geom G, __half* dst, const float* __restrict__ src) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (G.V << (G.lgnr - 1))) return;
+  const int sp = spad(G);
+  float a[24], b[24];
+  IO<float>::load_spinor(src, sp, 2 * e, a);
+  IO<float>::load_spinor(src, sp, 2 * e + 1, b);
+  F2 v[24];
+#pragma unroll
+  for (int j = 0; j < 24; j++) v[j] = F2{a[j], b[j]};
+  IOP::store_spinor(dst, sp >> 1, e, v);
+}
+__global__ void k_h2s_pair(Geom G, float* dst, const __half* __restrict__ src) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (G.V << (G.lgnr - 1))) return;
+  const int sp = spad(G);
+  F2 v[24];
+  IOP::load_spinor(src, sp >> 1, e, v);
+  float a[24], b[24];
+#pragma unroll
+  for (int j = 0; j < 24; j++) {
+    a[j] = v[j].x;
+    b[j] = v[j].y;
+  }
+  IO<float>::store_spinor(dst, sp, 2 * e, a);
+  IO<float>::store_spinor(dst, sp, 2 * e + 1, b);
+}
+__global__ void k_h2h_pair(Geom G, __half* dst, const __half* __restrict__ src) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (G.V << (G.lgnr - 1))) return;
+  const size_t pp = spad(G) >> 1;
+  const uint4* s = reinterpret_cast<const uint4*>(src);
+  uint4* d = reinterpret_cast<uint4*>(dst);
+#pragma unroll
+  for (int j = 0; j < 6; j++) d[j * pp + e] = s[j * pp + e];
+  reinterpret_cast<float2*>(d + 6 * pp)[e] = reinterpret_cast<const float2*>(s + 6 * pp)[e];
+}
+
 __global__ void k_fields_s2h(Geom G, __half* Uh, const float* __restrict__ Us, __half* Ch,
                              const float* __restrict__ Cs) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -333,17 +373,28 @@ void links_compress12(const Geom& G, float* U12, const float* Us, cudaStream_t s
   k_compress12<<<nb(G.V), 128, 0, st>>>(G, U12, Us);
 }
 
+// FP16 spinors of one RHS use IO<H16>, of two or more the IOP layout of the
+// paired hop kernels
 void spinor_s2h(const Geom& G, __half* dst, const float* src, cudaStream_t st) {
   count_launch();
-  k_s2h<<<nb(G.V << G.lgnr), 128, 0, st>>>(G, dst, src);
+  if (G.nr >= 2)
+    k_s2h_pair<<<nb(G.V << (G.lgnr - 1)), 128, 0, st>>>(G, dst, src);
+  else
+    k_s2h<<<nb(G.V), 128, 0, st>>>(G, dst, src);
 }
 void spinor_h2s(const Geom& G, float* dst, const __half* src, cudaStream_t st) {
   count_launch();
-  k_h2s<<<nb(G.V << G.lgnr), 128, 0, st>>>(G, dst, src);
+  if (G.nr >= 2)
+    k_h2s_pair<<<nb(G.V << (G.lgnr - 1)), 128, 0, st>>>(G, dst, src);
+  else
+    k_h2s<<<nb(G.V), 128, 0, st>>>(G, dst, src);
 }
 void spinor_h2h(const Geom& G, __half* dst, const __half* src, cudaStream_t st) {
   count_launch();
-  k_h2h<<<nb(G.V << G.lgnr), 128, 0, st>>>(G, dst, src);
+  if (G.nr >= 2)
+    k_h2h_pair<<<nb(G.V << (G.lgnr - 1)), 128, 0, st>>>(G, dst, src);
+  else
+    k_h2h<<<nb(G.V), 128, 0, st>>>(G, dst, src);
 }
 void fields_s2h(const Geom& G, __half* Uh, const float* Us, __half* Ch, const float* Cs,
                 cudaStream_t st) {

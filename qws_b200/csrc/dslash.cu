@@ -24,9 +24,55 @@
 
 namespace qwsg {
 
-template <typename T, int SEL, int MU, int DIR, typename R = typename Arith<T>::R>
-__device__ __forceinline__ void do_hop(const HopArgs<T>& a, const Site& s, int g, int rhs,
-                                       R acc[24]) {
+// How a thread's values map to memory.  Scalar: one (site, RHS) entry per
+// thread in the storage format's own layout.  Pair (FP16 multi-RHS fields):
+// two RHS of one site per thread as F2 lanes, IOP layout.
+template <typename T>
+struct OneRhs {
+  using V = typename Arith<T>::R;
+  using S = typename Store<T>::type;
+  __device__ __forceinline__ static int lanes_log(const Geom& G) { return G.lgnr; }
+  __device__ __forceinline__ static int pad(const Geom& G) { return spad(G); }
+  __device__ __forceinline__ static int entry(const Geom& G, int g, int lane) { return sentry(G, g, lane); }
+  __device__ __forceinline__ static void load_raw(const S* p, int pd, int e, V v[24], V& s) {
+    IO<T>::load_spinor_raw(p, pd, e, v, s);
+  }
+  __device__ __forceinline__ static void load_half_raw(const S* p, int pd, int e, int up, V v[24], V& s) {
+    IO<T>::load_half_raw(p, pd, e, up, v, s);
+  }
+  __device__ __forceinline__ static void load(const S* p, int pd, int e, V v[24]) {
+    IO<T>::load_spinor(p, pd, e, v);
+  }
+  __device__ __forceinline__ static void store(S* p, int pd, int e, const V v[24]) {
+    IO<T>::store_spinor(p, pd, e, v);
+  }
+};
+struct TwoRhs {
+  using V = F2;
+  using S = __half;
+  __device__ __forceinline__ static int lanes_log(const Geom& G) { return G.lgnr - 1; }
+  __device__ __forceinline__ static int pad(const Geom& G) { return spad(G) >> 1; }
+  __device__ __forceinline__ static int entry(const Geom& G, int g, int lane) {
+    return (g << (G.lgnr - 1)) + lane;
+  }
+  __device__ __forceinline__ static void load_raw(const S* p, int pd, int e, V v[24], V& s) {
+    IOP::load_spinor_raw(p, pd, e, v, s);
+  }
+  __device__ __forceinline__ static void load_half_raw(const S* p, int pd, int e, int up, V v[24], V& s) {
+    IOP::load_half_raw(p, pd, e, up, v, s);
+  }
+  __device__ __forceinline__ static void load(const S* p, int pd, int e, V v[24]) {
+    IOP::load_spinor(p, pd, e, v);
+  }
+  __device__ __forceinline__ static void store(S* p, int pd, int e, const V v[24]) {
+    IOP::store_spinor(p, pd, e, v);
+  }
+};
+
+template <typename T, typename P, int SEL, int MU, int DIR, typename V = typename P::V>
+__device__ __forceinline__ void do_hop(const HopArgs<T>& a, const Site& s, int g, int lane,
+                                       V acc[24]) {
+  using R = typename Arith<T>::R;
   const bool face = DIR > 0 ? (s.lc[MU] == a.G.B[MU] - 1) : (s.lc[MU] == 0);
   if (face) {
     if (!(SEL & HOP_OUTER)) return;
@@ -41,34 +87,40 @@ __device__ __forceinline__ void do_hop(const HopArgs<T>& a, const Site& s, int g
     gn = nbr_across(a.G, s, MU, DIR, &ncol);
     if (ncol == a.zero_col) return;  // that colour's source is defined as zero
   }
-  R v[24], sc;
-  const int sp = spad(a.G), en = sentry(a.G, gn, rhs);
+  V v[24], sc;
+  const int pd = P::pad(a.G), en = P::entry(a.G, gn, lane);
   // the projection and the link product are linear: the source's scale
   // (FP16 storage) is applied once, in the reconstruction
   if (MU == 3)
-    IO<T>::load_half_raw(a.src, sp, en, DIR > 0, v, sc);
+    P::load_half_raw(a.src, pd, en, DIR > 0, v, sc);
   else
-    IO<T>::load_spinor_raw(a.src, sp, en, v, sc);
-  R h[12], r[12], u[18];
-  project<R, MU, DIR>(v, h);
-  if constexpr (std::is_same<T, float>::value) {
-    if (a.U12)
-      load_link12(a.U12, a.G.pad, MU, DIR > 0 ? g : gn, u);
-    else
+    P::load_raw(a.src, pd, en, v, sc);
+  V h[12], r[12], ul[18];
+  project<V, MU, DIR>(v, h);
+  {
+    R u[18];
+    if constexpr (std::is_same<T, float>::value) {
+      if (a.U12)
+        load_link12(a.U12, a.G.pad, MU, DIR > 0 ? g : gn, u);
+      else
+        IO<T>::load_link(a.U, a.G.pad, MU, DIR > 0 ? g : gn, u);
+    } else {
       IO<T>::load_link(a.U, a.G.pad, MU, DIR > 0 ? g : gn, u);
-  } else {
-    IO<T>::load_link(a.U, a.G.pad, MU, DIR > 0 ? g : gn, u);
+    }
+#pragma unroll
+    for (int e = 0; e < 18; e++) ul[e] = Lanes<V>::bcast(u[e]);
   }
   if (DIR > 0)
-    link_mul<R, false>(u, h, r);
+    link_mul<V, false>(ul, h, r);
   else
-    link_mul<R, true>(u, h, r);
-  R f = sc;
+    link_mul<V, true>(ul, h, r);
+  V f = sc;
   if (MU == 3) {
-    f = 2 * sc;
-    if (face && (DIR > 0 ? s.bc[3] == a.G.NB[3] - 1 : s.bc[3] == 0)) f = (R)(2 * a.G.tbc) * sc;
+    f = Lanes<V>::bcast((R)2) * sc;
+    if (face && (DIR > 0 ? s.bc[3] == a.G.NB[3] - 1 : s.bc[3] == 0))
+      f = Lanes<V>::bcast((R)(2 * a.G.tbc)) * sc;
   }
-  reconstruct<R, MU, DIR>(r, acc, f);
+  reconstruct<V, MU, DIR>(r, acc, f);
 }
 
 // The FP32 block and face kernels and the FP16 block kernels are held to
@@ -84,13 +136,15 @@ struct MinCtas {
           : 1;
 };
 
-template <typename T, int SEL, int EPI>
-__global__ void __launch_bounds__(256, (MinCtas<T, SEL>::value)) k_hop(const HopArgs<T> a) {
-  using R = typename Arith<T>::R;
+template <typename T, typename P, int SEL, int EPI>
+__device__ __forceinline__ void hop_site(const HopArgs<T>& a) {
+  using V = typename P::V;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (a.nsites << a.G.lgnr)) return;
-  // consecutive threads: the right-hand sides of one site, then the next site
-  const int si = i >> a.G.lgnr, rhs = i & (a.G.nr - 1);
+  const int ll = P::lanes_log(a.G);
+  if (i >= (a.nsites << ll)) return;
+  // consecutive threads: the right-hand sides (or RHS pairs) of one site,
+  // then the next site
+  const int si = i >> ll, lane = i & ((1 << ll) - 1);
   const int g = a.list ? __ldg(a.list + si) : a.site0 + si;
   Site s;
   decode_site(a.G, g, s);
@@ -101,50 +155,78 @@ __global__ void __launch_bounds__(256, (MinCtas<T, SEL>::value)) k_hop(const Hop
     for (int mu = 0; mu < 4; mu++) face |= (s.lc[mu] == 0) | (s.lc[mu] == a.G.B[mu] - 1);
     if (!face) return;
   }
-  R acc[24];
+  V acc[24];
 #pragma unroll
-  for (int j = 0; j < 24; j++) acc[j] = 0;
-  do_hop<T, SEL, 0, +1>(a, s, g, rhs, acc);
-  do_hop<T, SEL, 0, -1>(a, s, g, rhs, acc);
-  do_hop<T, SEL, 1, +1>(a, s, g, rhs, acc);
-  do_hop<T, SEL, 1, -1>(a, s, g, rhs, acc);
-  do_hop<T, SEL, 2, +1>(a, s, g, rhs, acc);
-  do_hop<T, SEL, 2, -1>(a, s, g, rhs, acc);
-  do_hop<T, SEL, 3, +1>(a, s, g, rhs, acc);
-  do_hop<T, SEL, 3, -1>(a, s, g, rhs, acc);
-  clover_apply<T>(a.C, a.G.pad, g, acc);
-  const int sp = spad(a.G), e = sentry(a.G, g, rhs);
-  R o[24];
+  for (int j = 0; j < 24; j++) acc[j] = Lanes<V>::bcast((typename Arith<T>::R)0);
+  do_hop<T, P, SEL, 0, +1>(a, s, g, lane, acc);
+  do_hop<T, P, SEL, 0, -1>(a, s, g, lane, acc);
+  do_hop<T, P, SEL, 1, +1>(a, s, g, lane, acc);
+  do_hop<T, P, SEL, 1, -1>(a, s, g, lane, acc);
+  do_hop<T, P, SEL, 2, +1>(a, s, g, lane, acc);
+  do_hop<T, P, SEL, 2, -1>(a, s, g, lane, acc);
+  do_hop<T, P, SEL, 3, +1>(a, s, g, lane, acc);
+  do_hop<T, P, SEL, 3, -1>(a, s, g, lane, acc);
+  clover_apply<T, V>(a.C, a.G.pad, g, acc);
+  const int pd = P::pad(a.G), e = P::entry(a.G, g, lane);
+  const V coef = Lanes<V>::bcast(a.coef);
+  V o[24];
   if (EPI == EPI_D) {
-    IO<T>::load_spinor(a.src, sp, e, o);
+    P::load(a.src, pd, e, o);
 #pragma unroll
-    for (int j = 0; j < 24; j++) o[j] = o[j] + a.coef * acc[j];
+    for (int j = 0; j < 24; j++) o[j] = madd(coef, acc[j], o[j]);
   } else if (EPI == EPI_ADD) {
-    IO<T>::load_spinor(a.out, sp, e, o);
+    P::load(a.out, pd, e, o);
 #pragma unroll
-    for (int j = 0; j < 24; j++) o[j] = o[j] + a.coef * acc[j];
+    for (int j = 0; j < 24; j++) o[j] = madd(coef, acc[j], o[j]);
   } else if (EPI == EPI_JINV) {
-    IO<T>::load_spinor(a.aux, sp, e, o);
+    P::load(a.aux, pd, e, o);
 #pragma unroll
-    for (int j = 0; j < 24; j++) o[j] = o[j] + a.coef * acc[j];
+    for (int j = 0; j < 24; j++) o[j] = madd(coef, acc[j], o[j]);
   } else {  // EPI_SAPE: coef = -kappa
-    R in[24], av[24];
-    IO<T>::load_spinor(a.out, sp, e, o);
-    IO<T>::load_spinor(a.aux, sp, e, in);
-    IO<T>::load_spinor(a.src, sp, e, av);
+    V in[24], av[24];
+    P::load(a.out, pd, e, o);
+    P::load(a.aux, pd, e, in);
+    P::load(a.src, pd, e, av);
 #pragma unroll
-    for (int j = 0; j < 24; j++) o[j] = o[j] + (in[j] - (av[j] + a.coef * acc[j]));
+    for (int j = 0; j < 24; j++) o[j] = o[j] + (in[j] - madd(coef, acc[j], av[j]));
   }
-  IO<T>::store_spinor(a.out, sp, e, o);
+  P::store(a.out, pd, e, o);
+}
+
+// the same body with and without the 64-register bound (an explicit
+// minimum of one CTA per SM would let the compiler spend every register)
+template <typename T, int SEL, int EPI>
+__global__ void __launch_bounds__(256) k_hop(const HopArgs<T> a) {
+  hop_site<T, OneRhs<T>, SEL, EPI>(a);
+}
+template <typename T, int SEL, int EPI>
+__global__ void __launch_bounds__(256, 4) k_hop_r64(const HopArgs<T> a) {
+  hop_site<T, OneRhs<T>, SEL, EPI>(a);
+}
+// FP16 fields with two or more RHS: two RHS per thread in packed FP32x2
+// arithmetic (the link and clover of the site serve both lanes)
+template <int SEL, int EPI>
+__global__ void __launch_bounds__(256) k_hop_pair(const HopArgs<H16> a) {
+  hop_site<H16, TwoRhs, SEL, EPI>(a);
 }
 
 template <typename T, int SEL, int EPI>
 static void launch(const HopArgs<T>& a, cudaStream_t st) {
   if (a.nsites <= 0) return;
   const int threads = a.G.hop_threads;
-  const int blocks = ((a.nsites << a.G.lgnr) + threads - 1) / threads;
   count_launch();
-  k_hop<T, SEL, EPI><<<blocks, threads, 0, st>>>(a);
+  if constexpr (std::is_same<T, H16>::value) {
+    if (a.G.nr >= 2) {
+      const int blocks = ((a.nsites << (a.G.lgnr - 1)) + threads - 1) / threads;
+      k_hop_pair<SEL, EPI><<<blocks, threads, 0, st>>>(a);
+      return;
+    }
+  }
+  const int blocks = ((a.nsites << a.G.lgnr) + threads - 1) / threads;
+  if constexpr (MinCtas<T, SEL>::value == 4)
+    k_hop_r64<T, SEL, EPI><<<blocks, threads, 0, st>>>(a);
+  else
+    k_hop<T, SEL, EPI><<<blocks, threads, 0, st>>>(a);
 }
 
 template <typename T>

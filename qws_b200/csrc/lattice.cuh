@@ -25,6 +25,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace qwsg {
 
 // n / d for 0 <= n < 2^31 by a multiply-high (Granlund-Montgomery): with
@@ -159,6 +161,67 @@ __device__ __forceinline__ int nbr_across(const Geom& G, const Site& s, int mu, 
   *ncol = col;
   return col * G.Vh + (blin >> 1) * G.Vb + block_local(G, lc);
 }
+
+// ---------------------------------------------------------------------------
+// Values the stencil computes with: a scalar (float, double) or F2, two FP32
+// lanes (two right-hand sides of one site) in one 64-bit register pair,
+// computed with sm_100's packed FP32x2 instructions (add/sub/mul/fma .f32x2:
+// two IEEE single-precision results per instruction, each rounded as the
+// scalar instruction rounds it).  The stencil pieces below use madd(a, b, c)
+// = a*b + c with one rounding and a fixed order of operations, so a lane of
+// F2 computes bit for bit what the scalar float code computes.
+// ---------------------------------------------------------------------------
+struct F2 {
+  float x, y;
+};
+
+__device__ __forceinline__ unsigned long long f2_bits(F2 a) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+  return r;
+}
+__device__ __forceinline__ F2 f2_from_bits(unsigned long long r) {
+  F2 a;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+  return a;
+}
+__device__ __forceinline__ F2 operator+(F2 a, F2 b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+  return f2_from_bits(d);
+}
+__device__ __forceinline__ F2 operator-(F2 a, F2 b) {
+  unsigned long long d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+  return f2_from_bits(d);
+}
+__device__ __forceinline__ F2 operator*(F2 a, F2 b) {
+  unsigned long long d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+  return f2_from_bits(d);
+}
+__device__ __forceinline__ F2 operator-(F2 a) { return F2{-a.x, -a.y}; }
+__device__ __forceinline__ F2& operator+=(F2& a, F2 b) { return a = a + b; }
+__device__ __forceinline__ F2& operator-=(F2& a, F2 b) { return a = a - b; }
+
+__device__ __forceinline__ float madd(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double madd(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ F2 madd(F2 a, F2 b, F2 c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)), "l"(f2_bits(c)));
+  return f2_from_bits(d);
+}
+
+// a site quantity (link or clover entry) for every lane of V
+template <typename V>
+struct Lanes {
+  template <typename R>
+  __device__ __forceinline__ static V bcast(R a) { return (V)a; }
+};
+template <>
+struct Lanes<F2> {
+  __device__ __forceinline__ static F2 bcast(float a) { return F2{a, a}; }
+};
 
 // ---------------------------------------------------------------------------
 // plane I/O.  A storage tag T selects the in-memory format; arithmetic is in
@@ -484,6 +547,85 @@ struct IO<H16> {
   }
 };
 
+// FP16 spinors of a multi-RHS field computed two right-hand sides per
+// thread (F2 lanes): the entry of (site g, RHS pair p) is (g << (lgnr-1)) + p
+// with plane stride pad << (lgnr-1); six 16-byte planes whose 32-bit words
+// hold one component of both RHS as a half2 (plane k, word j: component
+// 4k + j), then a float2 plane of the two RHS' scales.  The same bytes per
+// (site, RHS) as IO<H16>, and the same half values: only the order differs.
+struct IOP {
+  __device__ __forceinline__ static F2 f2_of(unsigned w) {
+    __half2 h;
+    memcpy(&h, &w, 4);
+    const float2 f = __half22float2(h);
+    return F2{f.x, f.y};
+  }
+  __device__ __forceinline__ static unsigned word_of(F2 v) {
+    const __half2 h = __floats2half2_rn(v.x, v.y);
+    unsigned w;
+    memcpy(&w, &h, 4);
+    return w;
+  }
+  __device__ __forceinline__ static F2 scale(const __half* p, int ppad, int e) {
+    const float2 s =
+        __ldg(reinterpret_cast<const float2*>(reinterpret_cast<const uint4*>(p) + (size_t)6 * ppad) + e);
+    return F2{s.x, s.y};
+  }
+  __device__ __forceinline__ static void load_spinor_raw(const __half* __restrict__ p, int ppad,
+                                                         int e, F2 v[24], F2& s) {
+    const uint4* q = reinterpret_cast<const uint4*>(p);
+    s = scale(p, ppad, e);
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      const uint4 t = __ldg(q + (size_t)k * ppad + e);
+      v[4 * k] = f2_of(t.x);
+      v[4 * k + 1] = f2_of(t.y);
+      v[4 * k + 2] = f2_of(t.z);
+      v[4 * k + 3] = f2_of(t.w);
+    }
+  }
+  // spins 0-1 (upper = 0) or 2-3 of every colour: planes 2c + upper
+  __device__ __forceinline__ static void load_half_raw(const __half* __restrict__ p, int ppad,
+                                                       int e, int upper, F2 v[24], F2& s) {
+    const uint4* q = reinterpret_cast<const uint4*>(p);
+    s = scale(p, ppad, e);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const int k = 2 * c + (upper ? 1 : 0);
+      const uint4 t = __ldg(q + (size_t)k * ppad + e);
+      v[4 * k] = f2_of(t.x);
+      v[4 * k + 1] = f2_of(t.y);
+      v[4 * k + 2] = f2_of(t.z);
+      v[4 * k + 3] = f2_of(t.w);
+    }
+  }
+  __device__ __forceinline__ static void load_spinor(const __half* __restrict__ p, int ppad, int e,
+                                                     F2 v[24]) {
+    F2 s;
+    load_spinor_raw(p, ppad, e, v, s);
+#pragma unroll
+    for (int j = 0; j < 24; j++) v[j] = v[j] * s;
+  }
+  // per lane exactly IO<H16>::store_spinor
+  __device__ __forceinline__ static void store_spinor(__half* __restrict__ p, int ppad, int e,
+                                                      const F2 v[24]) {
+    float n0 = 0, n1 = 0;
+#pragma unroll
+    for (int j = 0; j < 24; j++) {
+      n0 = fmaxf(n0, fabsf(v[j].x));
+      n1 = fmaxf(n1, fabsf(v[j].y));
+    }
+    const bool k0 = n0 >= 1e-30f, k1 = n1 >= 1e-30f;
+    const F2 inv{k0 ? 1.0f / n0 : 0.0f, k1 ? 1.0f / n1 : 0.0f};
+    uint4* q = reinterpret_cast<uint4*>(p);
+#pragma unroll
+    for (int k = 0; k < 6; k++)
+      q[(size_t)k * ppad + e] = make_uint4(word_of(v[4 * k] * inv), word_of(v[4 * k + 1] * inv),
+                                           word_of(v[4 * k + 2] * inv), word_of(v[4 * k + 3] * inv));
+    reinterpret_cast<float2*>(q + (size_t)6 * ppad)[e] = make_float2(k0 ? n0 : 0.0f, k1 ? n1 : 0.0f);
+  }
+};
+
 // bytes each format moves per site (algorithmic traffic accounting)
 template <typename T>
 struct Bytes {
@@ -548,27 +690,72 @@ __device__ __forceinline__ void project(const R v[24], R h[12]) {
 #undef RE
 #undef IM
 
-// r = U h (forward) or U^dagger h (backward); U row-major complex [3][3]
+// r = U h (forward) or U^dagger h (backward); U row-major complex [3][3].
+// Products in a fixed order (one rounding each), the minus signs taken from
+// the negated h components.
+// (-a) b + c: a scalar takes the minus as an operand modifier of its fused
+// multiply-add; F2 lanes use a negated copy of b made once (same value:
+// negation is exact)
+template <typename R>
+struct Neg {
+  static constexpr bool copies = false;
+};
+template <>
+struct Neg<F2> {
+  static constexpr bool copies = true;
+};
+
 template <typename R, bool DAG>
 __device__ __forceinline__ void link_mul(const R u[18], const R h[12], R r[12]) {
+  if constexpr (std::is_same<R, double>::value) {
+    // FP64: sums left to the compiler's contraction (fewer registers)
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int k = 0; k < 2; k++) {
+        R re = 0, im = 0;
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+          const int e = DAG ? 3 * b + a : 3 * a + b;
+          const R ur = u[2 * e], ui = DAG ? -u[2 * e + 1] : u[2 * e + 1];
+          const R hr = h[4 * b + 2 * k], hi = h[4 * b + 2 * k + 1];
+          re += ur * hr - ui * hi;
+          im += ur * hi + ui * hr;
+        }
+        r[4 * a + 2 * k] = re;
+        r[4 * a + 2 * k + 1] = im;
+      }
+    return;
+  }
+  R nh[6];  // F2 only: -h_i (forward) or -h_r (backward)
+  if (Neg<R>::copies) {
+#pragma unroll
+    for (int j = 0; j < 6; j++) nh[j] = -h[2 * j + (DAG ? 0 : 1)];
+  }
 #pragma unroll
   for (int a = 0; a < 3; a++)
 #pragma unroll
     for (int k = 0; k < 2; k++) {
-      R re = 0, im = 0;
+      R re, im;
 #pragma unroll
       for (int b = 0; b < 3; b++) {
-        R ur, ui;
-        if (DAG) {
-          ur = u[2 * (3 * b + a)];
-          ui = -u[2 * (3 * b + a) + 1];
+        const int e = DAG ? 3 * b + a : 3 * a + b;
+        const R ur = u[2 * e], ui = u[2 * e + 1];
+        const R hr = h[4 * b + 2 * k], hi = h[4 * b + 2 * k + 1];
+        if (b == 0) {
+          re = ur * hr;
+          im = ur * hi;
         } else {
-          ur = u[2 * (3 * a + b)];
-          ui = u[2 * (3 * a + b) + 1];
+          re = madd(ur, hr, re);
+          im = madd(ur, hi, im);
         }
-        R hr = h[4 * b + 2 * k], hi = h[4 * b + 2 * k + 1];
-        re += ur * hr - ui * hi;
-        im += ur * hi + ui * hr;
+        if (DAG) {  // conj(u): re += ui hi, im -= ui hr
+          re = madd(ui, hi, re);
+          im = Neg<R>::copies ? madd(ui, nh[2 * b + k], im) : madd(-ui, hr, im);
+        } else {    // re -= ui hi, im += ui hr
+          re = Neg<R>::copies ? madd(ui, nh[2 * b + k], re) : madd(-ui, hi, re);
+          im = madd(ui, hr, im);
+        }
       }
       r[4 * a + 2 * k] = re;
       r[4 * a + 2 * k + 1] = im;
@@ -577,33 +764,74 @@ __device__ __forceinline__ void link_mul(const R u[18], const R h[12], R r[12]) 
 
 #define AR(c, s) acc[8 * (c) + 2 * (s)]
 #define AI(c, s) acc[8 * (c) + 2 * (s) + 1]
+// acc += recon(f r); f: the hop's factor times the source's scale (FP16
+// storage; 1 otherwise).  Additions as madd(+-f, r, acc).
 template <typename R, int MU, int DIR>
 __device__ __forceinline__ void reconstruct(const R r[12], R acc[24], R f) {
+  if constexpr (std::is_same<R, double>::value) {
+    // FP64 (f = 1 but for the t hops): plain sums
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const R r0 = f * r[4 * c], i0 = f * r[4 * c + 1], r1 = f * r[4 * c + 2], i1 = f * r[4 * c + 3];
+      if (MU == 3) {
+        if (DIR > 0) {
+          AR(c, 2) += r0; AI(c, 2) += i0; AR(c, 3) += r1; AI(c, 3) += i1;
+        } else {
+          AR(c, 0) += r0; AI(c, 0) += i0; AR(c, 1) += r1; AI(c, 1) += i1;
+        }
+        continue;
+      }
+      AR(c, 0) += r0; AI(c, 0) += i0; AR(c, 1) += r1; AI(c, 1) += i1;
+      if (MU == 0 && DIR > 0) {
+        AR(c, 2) -= i1; AI(c, 2) += r1; AR(c, 3) -= i0; AI(c, 3) += r0;
+      } else if (MU == 0) {
+        AR(c, 2) += i1; AI(c, 2) -= r1; AR(c, 3) += i0; AI(c, 3) -= r0;
+      } else if (MU == 1 && DIR > 0) {
+        AR(c, 2) += r1; AI(c, 2) += i1; AR(c, 3) -= r0; AI(c, 3) -= i0;
+      } else if (MU == 1) {
+        AR(c, 2) -= r1; AI(c, 2) -= i1; AR(c, 3) += r0; AI(c, 3) += i0;
+      } else if (MU == 2 && DIR > 0) {
+        AR(c, 2) -= i0; AI(c, 2) += r0; AR(c, 3) += i1; AI(c, 3) -= r1;
+      } else {
+        AR(c, 2) += i0; AI(c, 2) -= r0; AR(c, 3) -= i1; AI(c, 3) += r1;
+      }
+    }
+    return;
+  }
+  const R nf = -f;
 #pragma unroll
   for (int c = 0; c < 3; c++) {
-    R r0 = r[4 * c], i0 = r[4 * c + 1], r1 = r[4 * c + 2], i1 = r[4 * c + 3];
+    const R r0 = r[4 * c], i0 = r[4 * c + 1], r1 = r[4 * c + 2], i1 = r[4 * c + 3];
     if (MU == 3) {
       if (DIR > 0) {
-        AR(c, 2) += f * r0; AI(c, 2) += f * i0; AR(c, 3) += f * r1; AI(c, 3) += f * i1;
+        AR(c, 2) = madd(f, r0, AR(c, 2)); AI(c, 2) = madd(f, i0, AI(c, 2));
+        AR(c, 3) = madd(f, r1, AR(c, 3)); AI(c, 3) = madd(f, i1, AI(c, 3));
       } else {
-        AR(c, 0) += f * r0; AI(c, 0) += f * i0; AR(c, 1) += f * r1; AI(c, 1) += f * i1;
+        AR(c, 0) = madd(f, r0, AR(c, 0)); AI(c, 0) = madd(f, i0, AI(c, 0));
+        AR(c, 1) = madd(f, r1, AR(c, 1)); AI(c, 1) = madd(f, i1, AI(c, 1));
       }
       continue;
     }
-    // f: the source's scale (FP16 storage; 1 otherwise, folded at compile time)
-    AR(c, 0) += f * r0; AI(c, 0) += f * i0; AR(c, 1) += f * r1; AI(c, 1) += f * i1;
+    AR(c, 0) = madd(f, r0, AR(c, 0)); AI(c, 0) = madd(f, i0, AI(c, 0));
+    AR(c, 1) = madd(f, r1, AR(c, 1)); AI(c, 1) = madd(f, i1, AI(c, 1));
     if (MU == 0 && DIR > 0) {
-      AR(c, 2) -= f * i1; AI(c, 2) += f * r1; AR(c, 3) -= f * i0; AI(c, 3) += f * r0;
+      AR(c, 2) = madd(nf, i1, AR(c, 2)); AI(c, 2) = madd(f, r1, AI(c, 2));
+      AR(c, 3) = madd(nf, i0, AR(c, 3)); AI(c, 3) = madd(f, r0, AI(c, 3));
     } else if (MU == 0) {
-      AR(c, 2) += f * i1; AI(c, 2) -= f * r1; AR(c, 3) += f * i0; AI(c, 3) -= f * r0;
+      AR(c, 2) = madd(f, i1, AR(c, 2)); AI(c, 2) = madd(nf, r1, AI(c, 2));
+      AR(c, 3) = madd(f, i0, AR(c, 3)); AI(c, 3) = madd(nf, r0, AI(c, 3));
     } else if (MU == 1 && DIR > 0) {
-      AR(c, 2) += f * r1; AI(c, 2) += f * i1; AR(c, 3) -= f * r0; AI(c, 3) -= f * i0;
+      AR(c, 2) = madd(f, r1, AR(c, 2)); AI(c, 2) = madd(f, i1, AI(c, 2));
+      AR(c, 3) = madd(nf, r0, AR(c, 3)); AI(c, 3) = madd(nf, i0, AI(c, 3));
     } else if (MU == 1) {
-      AR(c, 2) -= f * r1; AI(c, 2) -= f * i1; AR(c, 3) += f * r0; AI(c, 3) += f * i0;
+      AR(c, 2) = madd(nf, r1, AR(c, 2)); AI(c, 2) = madd(nf, i1, AI(c, 2));
+      AR(c, 3) = madd(f, r0, AR(c, 3)); AI(c, 3) = madd(f, i0, AI(c, 3));
     } else if (MU == 2 && DIR > 0) {
-      AR(c, 2) -= f * i0; AI(c, 2) += f * r0; AR(c, 3) += f * i1; AI(c, 3) -= f * r1;
+      AR(c, 2) = madd(nf, i0, AR(c, 2)); AI(c, 2) = madd(f, r0, AI(c, 2));
+      AR(c, 3) = madd(f, i1, AR(c, 3)); AI(c, 3) = madd(nf, r1, AI(c, 3));
     } else {
-      AR(c, 2) += f * i0; AI(c, 2) -= f * r0; AR(c, 3) -= f * i1; AI(c, 3) += f * r1;
+      AR(c, 2) = madd(f, i0, AR(c, 2)); AI(c, 2) = madd(nf, r0, AI(c, 2));
+      AR(c, 3) = madd(nf, i1, AR(c, 3)); AI(c, 3) = madd(f, r1, AI(c, 3));
     }
   }
 }
@@ -613,40 +841,60 @@ __device__ __forceinline__ void reconstruct(const R r[12], R acc[24], R f) {
 // v <- A^-1 v with the packed chiral clover (clover_def.h:88-284):
 // x0 = (s0+s2, s1+s3), x1 = (s0-s2, s1-s3) per colour (no 1/2), y_i = A_i x_i,
 // s0 = y0+y1, s2 = y0-y1 (colours 0..2), s1/s3 likewise from entries 3..5.
-template <typename T, typename R = typename Arith<T>::R>
+// V: the value type (the field's arithmetic type, or F2 for two lanes that
+// share the site's clover).
+template <typename T, typename V = typename Arith<T>::R>
 __device__ __forceinline__ void clover_apply(const typename Store<T>::type* __restrict__ C, int pad,
-                                             int g, R v[24]) {
-  R xr[2][6], xi[2][6];
+                                             int g, V v[24]) {
+  using R = typename Arith<T>::R;
+  V xr[2][6], xi[2][6];
 #pragma unroll
   for (int c = 0; c < 3; c++) {
-    R s0r = v[8 * c], s0i = v[8 * c + 1], s1r = v[8 * c + 2], s1i = v[8 * c + 3];
-    R s2r = v[8 * c + 4], s2i = v[8 * c + 5], s3r = v[8 * c + 6], s3i = v[8 * c + 7];
+    const V s0r = v[8 * c], s0i = v[8 * c + 1], s1r = v[8 * c + 2], s1i = v[8 * c + 3];
+    const V s2r = v[8 * c + 4], s2i = v[8 * c + 5], s3r = v[8 * c + 6], s3i = v[8 * c + 7];
     xr[0][c] = s0r + s2r; xi[0][c] = s0i + s2i;
     xr[0][3 + c] = s1r + s3r; xi[0][3 + c] = s1i + s3i;
     xr[1][c] = s0r - s2r; xi[1][c] = s0i - s2i;
     xr[1][3 + c] = s1r - s3r; xi[1][3 + c] = s1i - s3i;
   }
-  R yr[2][6], yi[2][6];
+  V yr[2][6], yi[2][6];
 #pragma unroll
   for (int i = 0; i < 2; i++) {
     R a[36];
     IO<T>::load_clover_block(C, pad, g, i, a);
 #pragma unroll
     for (int j = 0; j < 6; j++) {
-      yr[i][j] = a[j] * xr[i][j];
-      yi[i][j] = a[j] * xi[i][j];
+      const V d = Lanes<V>::bcast(a[j]);
+      yr[i][j] = d * xr[i][j];
+      yi[i][j] = d * xi[i][j];
     }
     int n = 0;
 #pragma unroll
     for (int j = 0; j < 6; j++)
 #pragma unroll
       for (int k = j + 1; k < 6; k++, n++) {
-        R mr = a[6 + 2 * n], mi = a[7 + 2 * n];
-        // y_j += M_jk x_k ; y_k += conj(M_jk) x_j
-        yr[i][j] += mr * xr[i][k] - mi * xi[i][k];
-        yi[i][j] += mr * xi[i][k] + mi * xr[i][k];
-        yr[i][k] += mr * xr[i][j] + mi * xi[i][j];
-        yi[i][k] += mr * xi[i][j] - mi * xr[i][j];
+        if constexpr (std::is_same<V, double>::value) {
+          // FP64: left to the compiler's contraction (the explicit chain
+          // below costs FP64 kernels ~80 registers)
+          const double mr = a[6 + 2 * n], mi = a[7 + 2 * n];
+          yr[i][j] += mr * xr[i][k] - mi * xi[i][k];
+          yi[i][j] += mr * xi[i][k] + mi * xr[i][k];
+          yr[i][k] += mr * xr[i][j] + mi * xi[i][j];
+          yi[i][k] += mr * xi[i][j] - mi * xr[i][j];
+          continue;
+        }
+        // y_j += M_jk x_k ; y_k += conj(M_jk) x_j; the minus signs on m_i
+        // (negation is exact, so every form computes the same value)
+        const V mr = Lanes<V>::bcast(a[6 + 2 * n]), mi = Lanes<V>::bcast(a[7 + 2 * n]);
+        const V nmi = Lanes<V>::bcast(-a[7 + 2 * n]);
+        yr[i][j] = madd(mr, xr[i][k], yr[i][j]);
+        yr[i][j] = madd(nmi, xi[i][k], yr[i][j]);
+        yi[i][j] = madd(mr, xi[i][k], yi[i][j]);
+        yi[i][j] = madd(mi, xr[i][k], yi[i][j]);
+        yr[i][k] = madd(mr, xr[i][j], yr[i][k]);
+        yr[i][k] = madd(mi, xi[i][j], yr[i][k]);
+        yi[i][k] = madd(mr, xi[i][j], yi[i][k]);
+        yi[i][k] = madd(nmi, xr[i][j], yi[i][k]);
       }
   }
 #pragma unroll
