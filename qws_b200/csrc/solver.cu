@@ -661,6 +661,8 @@ static void graphed(Ctx& c, const Ctx::GraphKey& k, F&& body) {
   cudaGraphDestroy(g);
   QWSG_CUDA(e);
   if (c.graphs.size() >= 16) {  // a bounded cache: drop the oldest
+    // (after the stream has finished any launch of it)
+    QWSG_CUDA(cudaStreamSynchronize(c.st));
     cudaGraphExecDestroy(c.graphs.front().exec);
     c.graphs.erase(c.graphs.begin());
   }

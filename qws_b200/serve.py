@@ -78,7 +78,7 @@ class _Resident:
     """One gauge field on the device (a Lattice), with the clover term of the
     kappa/csw it was last built for.  Held by one job at a time."""
 
-    def __init__(self, L, gauge_id, U, NB, hop_threads=128):
+    def __init__(self, L, gauge_id, U, NB, hop_threads=128, graphs=True):
         import torch
 
         import qws_b200
@@ -87,6 +87,8 @@ class _Resident:
         self.stream = torch.cuda.Stream()
         self.lat = qws_b200.Lattice(L, NB, tbc=-1, kappa=0.0, stream=self.stream)
         self.lat.set_hop_threads(hop_threads)
+        self.lat.set_graphs(graphs)
+        self.graphs = graphs
         if isinstance(U, dict):  # {"seed", "n_smear", "alpha"}: generate on the device
             self.plaquette = self.lat.gen_gauge_device(U["seed"], U["n_smear"], U["alpha"])
         else:
@@ -132,8 +134,11 @@ class Service:
 
     def __init__(self, gauge_source, budget_bytes=150e9, workers=3, max_batch=16,
                  block_grid=None, maxiter=100, tol_s=1e-6, maxiter_s=50, nsap=None, nm=None,
-                 reliable=5):
+                 reliable=5, graphs=True):
         self.gauge_source = gauge_source
+        # CUDA graphs of the SAP sequences are captured per (buffers, kappa);
+        # they pay off when requests repeat a kappa
+        self.graphs = bool(graphs)
         self.budget = float(budget_bytes)
         self.max_batch = int(max_batch)
         # SAP block grid / sweep counts / CTA size per volume: as given, else
@@ -296,7 +301,7 @@ class Service:
         cfg = self.config(res.L)
         if isinstance(res, _Placeholder):  # first use of this field: make it resident
             U = self.gauge_source(res.L, res.gid)
-            live = _Resident(res.L, res.gid, U, cfg["NB"], cfg["hop_threads"])
+            live = _Resident(res.L, res.gid, U, cfg["NB"], cfg["hop_threads"], self.graphs)
             live.busy = True
             with self.cv:
                 self.residents[(res.L, res.gid)] = live
@@ -307,6 +312,7 @@ class Service:
         B = res.work.get(nr)
         if B is None:  # work buffers of an nr-RHS solve on this field, kept for reuse
             B = res.lat.batch(nr, stream=res.stream)
+            B.set_graphs(self.graphs)
             res.work[nr] = B
         s = self.solver
         with torch.cuda.stream(res.stream):
