@@ -1,0 +1,99 @@
+"""The solve service's scheduling on CPU (no GPU work): compatible pending
+requests merge into a power-of-two batch of at most max_batch, the oldest
+request goes first, a busy field holds back its requests, and admission
+evicts idle work buffers, then idle fields, least recently used first,
+never the field the job needs."""
+import threading
+
+import numpy as np
+
+from qws_b200 import serve
+
+
+class FakeHandle:
+    def __init__(self):
+        self.closed = False
+
+    def close(self):
+        self.closed = True
+
+
+class FakeResident:
+    def __init__(self, L, gid, last_used, busy=False, work=()):
+        self.L, self.gid, self.last_used, self.busy = L, gid, last_used, busy
+        self.lat = FakeHandle()
+        self.bytes = serve.field_bytes(L)
+        self.work = {nr: FakeHandle() for nr in work}
+        self.closed = False
+
+    def close(self):
+        self.closed = True
+
+
+def make_service(budget, max_batch=16):
+    svc = serve.Service.__new__(serve.Service)  # the scheduling state only, no threads
+    svc.budget, svc.max_batch = float(budget), max_batch
+    svc.pending, svc.residents, svc.used, svc.merged = [], {}, 0.0, 0
+    svc.cv = threading.Condition()
+    return svc
+
+
+def req(L, gauge, kappa, tol=1e-10):
+    return serve.Request(L=L, gauge=gauge, kappa=kappa, csw=1.7, tol=tol, source=np.zeros(1))
+
+
+L1, L2 = (8, 8, 8, 8), (16, 16, 16, 32)
+
+
+def test_merge_power_of_two_and_order():
+    svc = make_service(1e12, max_batch=4)
+    a = [req(L1, 0, 0.13) for _ in range(5)]
+    b = req(L1, 0, 0.12)
+    svc.pending = [b] + a
+    res, group = svc._pick()
+    assert group == [b]                      # the oldest request first
+    res.busy = False
+    res2, group2 = svc._pick()
+    assert group2 == a[:4] and svc.merged == 3  # 5 compatible -> a batch of 4
+    assert svc.pending == [a[4]]
+
+
+def test_busy_field_waits():
+    svc = make_service(1e12)
+    svc.residents[(L1, 0)] = FakeResident(L1, 0, 1.0, busy=True)
+    r1, r2 = req(L1, 0, 0.13), req(L2, 1, 0.13)
+    svc.pending = [r1, r2]
+    res, group = svc._pick()
+    assert group == [r2]      # r1's field is busy: the next request starts
+    assert svc.pending == [r1]
+
+
+def test_eviction_lru_and_keep():
+    nr_bytes = serve.work_bytes(L2, 1)
+    old = FakeResident(L2, 0, last_used=1.0, work=(1,))
+    new = FakeResident(L2, 1, last_used=2.0, work=(1,))
+    busy = FakeResident(L2, 2, last_used=0.5, busy=True)
+    svc = make_service(budget=3 * serve.field_bytes(L2) + 2 * nr_bytes)
+    svc.residents = {(L2, 0): old, (L2, 1): new, (L2, 2): busy}
+    svc.used = 3 * serve.field_bytes(L2) + 2 * nr_bytes
+    # a new field for another volume: idle work buffers go first (oldest
+    # first), then the least recently used idle field; never the busy one
+    need = serve.field_bytes(L2) + 2 * nr_bytes
+    assert svc._evict(need)
+    assert old.work == {} and new.work == {}
+    assert old.closed and (L2, 0) not in svc.residents
+    assert not new.closed and not busy.closed
+    # `keep` is never evicted, even when it is the only idle field
+    svc2 = make_service(budget=serve.field_bytes(L2))
+    k = FakeResident(L2, 3, last_used=0.1)
+    svc2.residents = {(L2, 3): k}
+    svc2.used = serve.field_bytes(L2)
+    assert not svc2._evict(1, keep=k) and not k.closed
+
+
+def test_admission_reserves_bytes():
+    svc = make_service(budget=serve.field_bytes(L1) + serve.work_bytes(L1, 2))
+    svc.pending = [req(L1, 0, 0.13), req(L1, 0, 0.13), req(L2, 0, 0.13)]
+    res, group = svc._pick()
+    assert len(group) == 2 and svc.used == serve.field_bytes(L1) + serve.work_bytes(L1, 2)
+    assert svc._pick() is None  # L2 does not fit while L1's field is busy
