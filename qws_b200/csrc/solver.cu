@@ -305,8 +305,9 @@ void Ctx::ensure_sap() {
     sap_t = alloc_spinor<float>();
   }
 }
+// (the FP32 SAP buffers are allocated by the FP32 SAP itself: the
+// precision form's inner solve does not need them)
 void Ctx::ensure_inner() {
-  ensure_sap();
   if (!in_q) {
     in_q = alloc_spinor<float>();
     in_r = alloc_spinor<float>();

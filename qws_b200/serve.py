@@ -32,7 +32,7 @@ import numpy as np
 
 # bytes per padded site of the pieces a job holds on the device
 _FIELD_BYTES = 72 * (8 + 4 + 2) * 2       # gauge + clover, FP64/FP32/FP16 copies
-_WORK_BYTES_PER_RHS = 9 * 24 * 8 + 12 * 24 * 4 + 4 * 52  # FP64, FP32, FP16 work spinors
+_WORK_BYTES_PER_RHS = 9 * 24 * 8 + 9 * 24 * 4 + 4 * 52  # FP64, FP32, FP16 work spinors
 
 
 def _pad(V):
