@@ -39,7 +39,7 @@ def test_allreduce_max_gloo():
     import torch.multiprocessing as mp
 
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_worker, args=(2, port, out), nprocs=2, join=True)
         assert dict(out) == {0: 2.5, 1: 2.5}
