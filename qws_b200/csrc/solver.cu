@@ -734,6 +734,10 @@ int bicgstab_precdd_s(Ctx& c, float* x, const float* b, double tol, int maxiter,
   blas_bicg_init<float>(G, b, nullptr, r, p, r0, c.d_res, c.rb, c.st);
   const double* h = c.fetch(2);
   const float bnorm = (float)h[0];
+  if (bnorm == 0) {  // b = 0: x = 0 (zeroed above)
+    if (final_rel) *final_rel = 0;
+    return 0;
+  }
   std::complex<float> rho0(bnorm, 0), rho, beta, omega, alpha, ctmp;
   float rnorm = bnorm;
   int done = maxiter;
@@ -790,6 +794,10 @@ int bicgstab_precdd_s_h(Ctx& c, float* x, const float* b, double tol, int maxite
   blas_bicg_init<float>(G, b, nullptr, r, p, r0, c.d_res, c.rb, c.st);
   const double* h = c.fetch(2);
   const float bnorm = (float)h[0];
+  if (bnorm == 0) {  // b = 0: x = 0 (zeroed above)
+    if (final_rel) *final_rel = 0;
+    return 0;
+  }
   std::complex<float> rho0(bnorm, 0), rho, beta, omega, alpha, ctmp;
   float rnorm = bnorm;
   int done = maxiter;
@@ -869,6 +877,11 @@ static int outer_loop(Ctx& c, double* x, const double* b, double tol, int iter_b
   blas_bicg_init<double>(G, b, q, r, p, r0, c.d_res, c.rb, c.st);
   const double* h = c.fetch(2);
   const double bnorm = h[0];
+  if (bnorm == 0) {  // b = 0: x = 0 (the reference would divide 0 by 0)
+    blas_zero<double>(G, x, 0, G.V, c.st);
+    *rel_out = 0;
+    return iter_begin;
+  }
   std::complex<double> rho0(h[1], 0), rho, beta, omega, alpha, ctmp;
   double rnorm = h[1];
   long inner = 0;
@@ -938,6 +951,7 @@ double true_residual(Ctx& c, const double* x, const double* b) {
   dslash_full_d(c, c.out_t, x);
   blas_bicg_init<double>(c.G, b, c.out_t, c.out_q, c.out_p, c.out_r0, c.d_res, c.rb, c.st);
   const double* h = c.fetch(2);
+  if (h[0] == 0) return h[1] == 0 ? 0.0 : INFINITY;  // b = 0: exact only for D x = 0
   return std::sqrt(h[1] / h[0]);
 }
 
