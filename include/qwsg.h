@@ -66,6 +66,12 @@ int qwsg_sync(qwsg_lattice* lat);
  * qwsg_batch_stats gives each RHS's.  Fields, kappa and the even-odd family
  * stay on the parent.  Destroy with qwsg_destroy before the parent. */
 int qwsg_create_batch(qwsg_lattice** out, qwsg_lattice* parent, int nrhs);
+/* a different kappa for every RHS of a multi-RHS handle (no counterpart in
+ * the reference): builds the clover term of the parent's gauge field for
+ * kappas[r] (csw as qwsg_build_clover) into the handle's own per-RHS planes;
+ * every operator and solver on the handle then applies kappas[r] and its
+ * clover to RHS r.  Call again to change the kappas. */
+int qwsg_batch_set_kappas(qwsg_lattice* batch, const double* kappas, double csw);
 int qwsg_nrhs(const qwsg_lattice* lat, int* nrhs);
 /* per-RHS results of the last multi-RHS solve: stats of the DD solvers,
  * iteration counts of the inner solvers (either pointer may be NULL) */

@@ -58,6 +58,7 @@ def load_library(path: str | os.PathLike | None = None):
         "qwsg_sync": [vp],
         "qwsg_create_batch": [ctypes.POINTER(vp), vp, c_int],
         "qwsg_nrhs": [vp, ip],
+        "qwsg_batch_set_kappas": [vp, vp, c_double],
         "qwsg_batch_stats": [vp, ctypes.POINTER(SolveStats), ip],
         "qwsg_build_clover": [vp, c_double],
         "qwsg_set_graphs": [vp, c_int],
@@ -548,7 +549,15 @@ class BatchLattice(Lattice):
         self.set_stream(stream if stream is not None else torch.cuda.current_stream())
 
     def set_kappa(self, kappa):
-        raise QwsgError("kappa belongs to the parent lattice")
+        raise QwsgError("kappa belongs to the parent lattice (or use set_kappas)")
+
+    def set_kappas(self, kappas, csw):
+        """A kappa per RHS: clover terms of the parent's gauge field built on
+        the GPU for each (qwsg_batch_set_kappas)."""
+        k = np.ascontiguousarray(kappas, np.float64)
+        assert k.size == self.nr
+        _check(self.lib.qwsg_batch_set_kappas(self.h, ctypes.c_void_p(k.ctypes.data), float(csw)))
+        self.kappas = k.copy()
 
     def load_fields(self, *a, **k):
         raise QwsgError("fields belong to the parent lattice")

@@ -1,4 +1,5 @@
 // Native qwsg_* C ABI (include/qwsg.h).
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -228,6 +229,17 @@ int qwsg_create_batch(qwsg_lattice** out, qwsg_lattice* parent, int nrhs) {
       throw;
     }
     *out = new qwsg_lattice{c};
+  });
+}
+
+int qwsg_batch_set_kappas(qwsg_lattice* l, const double* kappas, double csw) {
+  return guarded([&] {
+    check_ctx(l);
+    if (!kappas) throw Error(1, "qwsg_batch_set_kappas: NULL argument");
+    for (int r = 0; r < l->c->G.nr; r++)
+      if (!(kappas[r] > 0) || !std::isfinite(kappas[r]))
+        throw Error(1, "qwsg_batch_set_kappas: kappa must be positive and finite");
+    set_rhs_kappas(*l->c, kappas, csw);
   });
 }
 

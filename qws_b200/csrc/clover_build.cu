@@ -161,8 +161,11 @@ __device__ bool invert6(Cx a[6][6]) {
   return true;
 }
 
+// writes the FP64 and FP32 planes at entry (g << oshift) + orhs, plane
+// stride ostride (a lattice's own clover: 0, 0, pad; one RHS of a handle
+// with per-RHS kappa: lgnr, rhs, spad)
 __global__ void k_build_clover(Geom G, const double* __restrict__ U, double* Cd, float* Cs,
-                               double ck, unsigned* bad) {
+                               double ck, unsigned* bad, int oshift, int orhs, int ostride) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= G.V) return;
   int x[4];
@@ -214,19 +217,16 @@ __global__ void k_build_clover(Geom G, const double* __restrict__ U, double* Cd,
   }
   double2* qd = reinterpret_cast<double2*>(Cd);
   float4* qs = reinterpret_cast<float4*>(Cs);
-  for (int j = 0; j < 36; j++) qd[(size_t)j * G.pad + g] = make_double2(out[2 * j], out[2 * j + 1]);
+  const size_t e = ((size_t)g << oshift) + orhs;
+  for (int j = 0; j < 36; j++) qd[(size_t)j * ostride + e] = make_double2(out[2 * j], out[2 * j + 1]);
   for (int j = 0; j < 18; j++)
-    qs[(size_t)j * G.pad + g] = make_float4((float)out[4 * j], (float)out[4 * j + 1],
-                                            (float)out[4 * j + 2], (float)out[4 * j + 3]);
+    qs[(size_t)j * ostride + e] = make_float4((float)out[4 * j], (float)out[4 * j + 1],
+                                              (float)out[4 * j + 2], (float)out[4 * j + 3]);
 }
 
 }  // namespace
 
-// clover term of the resident FP64 gauge field for this context's kappa:
-// writes the FP64 and FP32 clover planes (the FP16 copies follow on demand)
-void build_clover(Ctx& c, double csw) {
-  if (!c.Ud) throw Error(4, "gauge field not loaded");
-  if (c.parent) throw Error(1, "build the clover term on the parent lattice");
+static const double (*chiral_tables())[2][2][2][2] {
   struct Tables {
     double S[6][2][2][2][2];
     double off;
@@ -234,19 +234,75 @@ void build_clover(Ctx& c, double csw) {
   };
   static const Tables tab;  // built once, thread-safe
   if (tab.off > 1e-14) throw Error(3, "sigma_{mu nu} is not block diagonal in the chiral basis");
-  c.ensure_fields_d();
-  c.ensure_fields_s();
-  QWSG_CUDA(cudaMemcpyToSymbolAsync(c_S, tab.S, sizeof(tab.S), 0, cudaMemcpyHostToDevice, c.st));
+  return tab.S;
+}
+
+// one clover build on c's stream into (Cd, Cs) at (oshift, orhs, ostride)
+static void build_into(Ctx& c, const double* Ud, double* Cd, float* Cs, double ck, int oshift,
+                       int orhs, int ostride) {
+  QWSG_CUDA(cudaMemcpyToSymbolAsync(c_S, chiral_tables(), sizeof(double) * 6 * 16, 0,
+                                    cudaMemcpyHostToDevice, c.st));
   unsigned* bad = c.rb.counter + 1;  // a spare counter slot
   QWSG_CUDA(cudaMemsetAsync(bad, 0, sizeof(unsigned), c.st));
   count_launch();
-  k_build_clover<<<(c.G.V + 127) / 128, 128, 0, c.st>>>(c.G, c.Ud, c.Cd, c.Cs, csw * c.kappa, bad);
+  k_build_clover<<<(c.G.V + 127) / 128, 128, 0, c.st>>>(c.G, Ud, Cd, Cs, ck, bad, oshift, orhs,
+                                                         ostride);
   c.check_launch("build_clover");
   unsigned h_bad = 0;
   QWSG_CUDA(cudaMemcpyAsync(&h_bad, bad, sizeof(unsigned), cudaMemcpyDeviceToHost, c.st));
   QWSG_CUDA(cudaStreamSynchronize(c.st));
-  c.fields_h_valid = false;
   if (h_bad) throw Error(2, "clover term singular on " + std::to_string(h_bad) + " blocks");
+}
+
+// clover term of the resident FP64 gauge field for this context's kappa:
+// writes the FP64 and FP32 clover planes (the FP16 copies follow on demand)
+void build_clover(Ctx& c, double csw) {
+  if (!c.Ud) throw Error(4, "gauge field not loaded");
+  if (c.parent) throw Error(1, "build the clover term on the parent lattice");
+  c.ensure_fields_d();
+  c.ensure_fields_s();
+  c.fields_h_valid = false;
+  build_into(c, c.Ud, c.Cd, c.Cs, csw * c.kappa, 0, 0, c.G.pad);
+}
+
+// per-RHS kappa on a multi-RHS handle: the clover term of the parent's gauge
+// field for kappas[r], into the handle's per-RHS planes (FP64, FP32 and the
+// FP16 copy), and the kappa tables the Dirac kernels read
+void set_rhs_kappas(Ctx& c, const double* kappas, double csw) {
+  if (!c.parent) throw Error(1, "per-RHS kappa needs a multi-RHS handle");
+  c.sync_from_parent(false);
+  if (!c.Ud) throw Error(4, "gauge field not loaded");
+  const size_t n = (size_t)72 * spad(c.G);
+  if (c.rhs_kappas.empty()) {  // graphs captured before read the parent's clover
+    QWSG_CUDA(cudaStreamSynchronize(c.st));
+    c.clear_graphs();
+  }
+  if (!c.Cdr) {
+    QWSG_CUDA(cudaMalloc(&c.Cdr, sizeof(double) * n));
+    QWSG_CUDA(cudaMalloc(&c.Csr, sizeof(float) * n));
+    QWSG_CUDA(cudaMalloc(&c.Chr, sizeof(__half) * n));
+    QWSG_CUDA(cudaMalloc(&c.kap_d, sizeof(double) * Ctx::kMaxRhs));
+    QWSG_CUDA(cudaMalloc(&c.kap_s, sizeof(float) * Ctx::kMaxRhs));
+    c.owned.push_back(c.Cdr);
+    c.owned.push_back(c.Csr);
+    c.owned.push_back(c.Chr);
+    c.owned.push_back(c.kap_d);
+    c.owned.push_back(c.kap_s);
+  }
+  for (int r = 0; r < c.G.nr; r++)
+    build_into(c, c.Ud, c.Cdr, c.Csr, csw * kappas[r], c.G.lgnr, r, spad(c.G));
+  clover_s2h_entries(c.G, c.Chr, c.Csr, c.st);
+  c.check_launch("clover_s2h_entries");
+  double kd[Ctx::kMaxRhs];
+  float ks[Ctx::kMaxRhs];
+  for (int r = 0; r < c.G.nr; r++) {
+    kd[r] = kappas[r];
+    ks[r] = (float)kappas[r];
+  }
+  QWSG_CUDA(cudaMemcpyAsync(c.kap_d, kd, sizeof(double) * c.G.nr, cudaMemcpyHostToDevice, c.st));
+  QWSG_CUDA(cudaMemcpyAsync(c.kap_s, ks, sizeof(float) * c.G.nr, cudaMemcpyHostToDevice, c.st));
+  QWSG_CUDA(cudaStreamSynchronize(c.st));
+  c.rhs_kappas.assign(kappas, kappas + c.G.nr);
 }
 
 }  // namespace qwsg

@@ -287,6 +287,17 @@ __global__ void k_h2h_pair(Geom G, __half* dst, const __half* __restrict__ src) 
   reinterpret_cast<float2*>(d + 6 * pp)[e] = reinterpret_cast<const float2*>(s + 6 * pp)[e];
 }
 
+// FP16 copy of per-RHS clover planes (entry (g << lgnr) + r, stride spad)
+__global__ void k_clover_s2h_entries(Geom G, __half* Ch, const float* __restrict__ Cs) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (G.V << G.lgnr)) return;
+  const int sp = spad(G);
+  float a[72];
+  IO<float>::load_clover_block(Cs, sp, e, 0, a);
+  IO<float>::load_clover_block(Cs, sp, e, 1, a + 36);
+  IO<H16>::store_clover(Ch, sp, e, a);
+}
+
 __global__ void k_fields_s2h(Geom G, __half* Uh, const float* __restrict__ Us, __half* Ch,
                              const float* __restrict__ Cs) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -395,6 +406,10 @@ void spinor_h2h(const Geom& G, __half* dst, const __half* src, cudaStream_t st) 
     k_h2h_pair<<<nb(G.V << (G.lgnr - 1)), 128, 0, st>>>(G, dst, src);
   else
     k_h2h<<<nb(G.V), 128, 0, st>>>(G, dst, src);
+}
+void clover_s2h_entries(const Geom& G, __half* Ch, const float* Cs, cudaStream_t st) {
+  count_launch();
+  k_clover_s2h_entries<<<nb(G.V << G.lgnr), 128, 0, st>>>(G, Ch, Cs);
 }
 void fields_s2h(const Geom& G, __half* Uh, const float* Us, __half* Ch, const float* Cs,
                 cudaStream_t st) {

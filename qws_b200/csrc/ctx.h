@@ -138,6 +138,14 @@ struct Ctx {
   // work spinors with per-site scales, and the flexible inner solver's w
   __half* Uh = nullptr;
   __half* Ch = nullptr;
+  // per-RHS kappa on a multi-RHS handle (set_rhs_kappas): clover planes per
+  // (site, RHS) entry in FP64/FP32/FP16 and the kappas; empty: the parent's
+  std::vector<double> rhs_kappas;
+  double* Cdr = nullptr;
+  float* Csr = nullptr;
+  __half* Chr = nullptr;
+  double* kap_d = nullptr;
+  float* kap_s = nullptr;
   bool fields_h_valid = false;
   __half* h_s = nullptr;
   __half* h_a = nullptr;
@@ -273,6 +281,8 @@ void mtilde_dag_d(Ctx& c, double* out, const double* in);  // qws.cc:557-565
 void mtilde_s(Ctx& c, float* out, const float* in);        // qws.cc:598-604
 int bicgstab_vm(Ctx& c, double* x, const double* b, int maxiter);  // bicgstab.cc:68
 void mtdagmt_d(Ctx& c, double* out, const double* in);              // qws.cc:566-571
+// per-RHS kappa on a multi-RHS handle (no counterpart in the reference)
+void set_rhs_kappas(Ctx& c, const double* kappas, double csw);
 int cg_vm(Ctx& c, double* x, const double* b, int maxiter);        // cg.cc:65
 // X: n solution fields back to back (spinor_elems() doubles each)
 int mcg_vm(Ctx& c, double* X, const double* b, int n, const double* sigma,

@@ -46,6 +46,19 @@ struct OneRhs {
   __device__ __forceinline__ static void store(S* p, int pd, int e, const V v[24]) {
     IO<T>::store_spinor(p, pd, e, v);
   }
+  // A^-1 v with the site's clover, or the entry's (PRK: per-RHS kappa)
+  template <bool PRK>
+  __device__ __forceinline__ static void clover(const HopArgs<T>& a, int g, int lane, V v[24]) {
+    if constexpr (PRK)
+      clover_apply<T, V>(a.Cr, spad(a.G), sentry(a.G, g, lane), v);
+    else
+      clover_apply<T, V>(a.C, a.G.pad, g, v);
+  }
+  template <bool PRK>
+  __device__ __forceinline__ static V coef(const HopArgs<T>& a, int lane) {
+    if constexpr (PRK) return copysign(a.kap[lane], a.coef);
+    return a.coef;
+  }
 };
 struct TwoRhs {
   using V = F2;
@@ -66,6 +79,30 @@ struct TwoRhs {
   }
   __device__ __forceinline__ static void store(S* p, int pd, int e, const V v[24]) {
     IOP::store_spinor(p, pd, e, v);
+  }
+  // the site's clover for both lanes, or each lane's own (PRK: per-RHS kappa)
+  template <bool PRK>
+  __device__ __forceinline__ static void clover(const HopArgs<H16>& a, int g, int lane, V v[24]) {
+    if constexpr (PRK) {
+      const int sp = spad(a.G), e0 = sentry(a.G, g, 2 * lane);
+      clover_apply_with<F2>(
+          [&](int i, F2 c[36]) {
+            float s0[36], s1[36];
+            IO<H16>::load_clover_block(a.Cr, sp, e0, i, s0);
+            IO<H16>::load_clover_block(a.Cr, sp, e0 + 1, i, s1);
+#pragma unroll
+            for (int k = 0; k < 36; k++) c[k] = F2{s0[k], s1[k]};
+          },
+          v);
+    } else {
+      clover_apply<H16, F2>(a.C, a.G.pad, g, v);
+    }
+  }
+  template <bool PRK>
+  __device__ __forceinline__ static V coef(const HopArgs<H16>& a, int lane) {
+    if constexpr (PRK)
+      return F2{copysignf(a.kap[2 * lane], a.coef), copysignf(a.kap[2 * lane + 1], a.coef)};
+    return Lanes<F2>::bcast(a.coef);
   }
 };
 
@@ -136,7 +173,7 @@ struct MinCtas {
           : 1;
 };
 
-template <typename T, typename P, int SEL, int EPI>
+template <typename T, typename P, int SEL, int EPI, bool PRK>
 __device__ __forceinline__ void hop_site(const HopArgs<T>& a) {
   using V = typename P::V;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -166,9 +203,9 @@ __device__ __forceinline__ void hop_site(const HopArgs<T>& a) {
   do_hop<T, P, SEL, 2, -1>(a, s, g, lane, acc);
   do_hop<T, P, SEL, 3, +1>(a, s, g, lane, acc);
   do_hop<T, P, SEL, 3, -1>(a, s, g, lane, acc);
-  clover_apply<T, V>(a.C, a.G.pad, g, acc);
+  P::template clover<PRK>(a, g, lane, acc);
   const int pd = P::pad(a.G), e = P::entry(a.G, g, lane);
-  const V coef = Lanes<V>::bcast(a.coef);
+  const V coef = P::template coef<PRK>(a, lane);
   V o[24];
   if (EPI == EPI_D) {
     P::load(a.src, pd, e, o);
@@ -195,38 +232,47 @@ __device__ __forceinline__ void hop_site(const HopArgs<T>& a) {
 
 // the same body with and without the 64-register bound (an explicit
 // minimum of one CTA per SM would let the compiler spend every register)
-template <typename T, int SEL, int EPI>
+// PRK: per-RHS kappa (clover planes and kappa per RHS, multi-RHS handles only)
+template <typename T, int SEL, int EPI, bool PRK>
 __global__ void __launch_bounds__(256) k_hop(const HopArgs<T> a) {
-  hop_site<T, OneRhs<T>, SEL, EPI>(a);
+  hop_site<T, OneRhs<T>, SEL, EPI, PRK>(a);
 }
-template <typename T, int SEL, int EPI>
+template <typename T, int SEL, int EPI, bool PRK>
 __global__ void __launch_bounds__(256, 4) k_hop_r64(const HopArgs<T> a) {
-  hop_site<T, OneRhs<T>, SEL, EPI>(a);
+  hop_site<T, OneRhs<T>, SEL, EPI, PRK>(a);
 }
 // FP16 fields with two or more RHS: two RHS per thread in packed FP32x2
 // arithmetic (the link and clover of the site serve both lanes)
-template <int SEL, int EPI>
+template <int SEL, int EPI, bool PRK>
 __global__ void __launch_bounds__(256) k_hop_pair(const HopArgs<H16> a) {
-  hop_site<H16, TwoRhs, SEL, EPI>(a);
+  hop_site<H16, TwoRhs, SEL, EPI, PRK>(a);
 }
 
-template <typename T, int SEL, int EPI>
-static void launch(const HopArgs<T>& a, cudaStream_t st) {
-  if (a.nsites <= 0) return;
+template <typename T, int SEL, int EPI, bool PRK>
+static void launch_v(const HopArgs<T>& a, cudaStream_t st) {
   const int threads = a.G.hop_threads;
-  count_launch();
   if constexpr (std::is_same<T, H16>::value) {
     if (a.G.nr >= 2) {
       const int blocks = ((a.nsites << (a.G.lgnr - 1)) + threads - 1) / threads;
-      k_hop_pair<SEL, EPI><<<blocks, threads, 0, st>>>(a);
+      k_hop_pair<SEL, EPI, PRK><<<blocks, threads, 0, st>>>(a);
       return;
     }
   }
   const int blocks = ((a.nsites << a.G.lgnr) + threads - 1) / threads;
   if constexpr (MinCtas<T, SEL>::value == 4)
-    k_hop_r64<T, SEL, EPI><<<blocks, threads, 0, st>>>(a);
+    k_hop_r64<T, SEL, EPI, PRK><<<blocks, threads, 0, st>>>(a);
   else
-    k_hop<T, SEL, EPI><<<blocks, threads, 0, st>>>(a);
+    k_hop<T, SEL, EPI, PRK><<<blocks, threads, 0, st>>>(a);
+}
+
+template <typename T, int SEL, int EPI>
+static void launch(const HopArgs<T>& a, cudaStream_t st) {
+  if (a.nsites <= 0) return;
+  count_launch();
+  if (a.Cr && a.kap)
+    launch_v<T, SEL, EPI, true>(a, st);
+  else
+    launch_v<T, SEL, EPI, false>(a, st);
 }
 
 template <typename T>

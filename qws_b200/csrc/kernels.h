@@ -26,6 +26,11 @@ struct HopArgs {
   S* out;
   const S* U;     // gauge planes
   const S* U12;   // FP32 only: links in 12-real form (null: use U)
+  // per-RHS kappa (multi-RHS handles): clover planes per (site, RHS) entry
+  // (stride spad) and kappa per RHS; the epilogue's coefficient is then
+  // kap[rhs] with coef's sign (coef is +-kappa in every such launch)
+  const S* Cr;
+  const typename Arith<T>::R* kap;
   const S* C;     // clover planes
   typename Arith<T>::R coef;
   const int* list;  // if set: thread i handles site list[i], else site0 + i
@@ -138,6 +143,8 @@ void spinor_h2h(const Geom& G, __half* dst, const __half* src, cudaStream_t st);
 // FP16 copies of the FP32 gauge (9 complex planes per mu) and clover planes
 void fields_s2h(const Geom& G, __half* Uh, const float* Us, __half* Ch, const float* Cs,
                 cudaStream_t st);
+// FP16 copy of per-RHS FP32 clover planes (entries of a multi-RHS handle)
+void clover_s2h_entries(const Geom& G, __half* Ch, const float* Cs, cudaStream_t st);
 // y = (float)(x * s)   /   y = (double)x * s   (cf: per-RHS s, cf[4*rhs])
 void blas_d2s(const Geom& G, float* y, const double* x, double s, cudaStream_t st,
               const double* cf = nullptr);

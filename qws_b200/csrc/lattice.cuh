@@ -843,10 +843,9 @@ __device__ __forceinline__ void reconstruct(const R r[12], R acc[24], R f) {
 // s0 = y0+y1, s2 = y0-y1 (colours 0..2), s1/s3 likewise from entries 3..5.
 // V: the value type (the field's arithmetic type, or F2 for two lanes that
 // share the site's clover).
-template <typename T, typename V = typename Arith<T>::R>
-__device__ __forceinline__ void clover_apply(const typename Store<T>::type* __restrict__ C, int pad,
-                                             int g, V v[24]) {
-  using R = typename Arith<T>::R;
+// load_block(i, a) fills block i's 36 values for every lane of V.
+template <typename V, typename Load>
+__device__ __forceinline__ void clover_apply_with(Load&& load_block, V v[24]) {
   V xr[2][6], xi[2][6];
 #pragma unroll
   for (int c = 0; c < 3; c++) {
@@ -860,13 +859,12 @@ __device__ __forceinline__ void clover_apply(const typename Store<T>::type* __re
   V yr[2][6], yi[2][6];
 #pragma unroll
   for (int i = 0; i < 2; i++) {
-    R a[36];
-    IO<T>::load_clover_block(C, pad, g, i, a);
+    V a[36];
+    load_block(i, a);
 #pragma unroll
     for (int j = 0; j < 6; j++) {
-      const V d = Lanes<V>::bcast(a[j]);
-      yr[i][j] = d * xr[i][j];
-      yi[i][j] = d * xi[i][j];
+      yr[i][j] = a[j] * xr[i][j];
+      yi[i][j] = a[j] * xi[i][j];
     }
     int n = 0;
 #pragma unroll
@@ -885,8 +883,8 @@ __device__ __forceinline__ void clover_apply(const typename Store<T>::type* __re
         }
         // y_j += M_jk x_k ; y_k += conj(M_jk) x_j; the minus signs on m_i
         // (negation is exact, so every form computes the same value)
-        const V mr = Lanes<V>::bcast(a[6 + 2 * n]), mi = Lanes<V>::bcast(a[7 + 2 * n]);
-        const V nmi = Lanes<V>::bcast(-a[7 + 2 * n]);
+        const V mr = a[6 + 2 * n], mi = a[7 + 2 * n];
+        const V nmi = -a[7 + 2 * n];
         yr[i][j] = madd(mr, xr[i][k], yr[i][j]);
         yr[i][j] = madd(nmi, xi[i][k], yr[i][j]);
         yi[i][j] = madd(mr, xi[i][k], yi[i][j]);
@@ -908,6 +906,22 @@ __device__ __forceinline__ void clover_apply(const typename Store<T>::type* __re
     v[8 * c + 6] = yr[0][3 + c] - yr[1][3 + c];
     v[8 * c + 7] = yi[0][3 + c] - yi[1][3 + c];
   }
+}
+
+// the clover of site g (or entry g of per-RHS clover planes) from field T's
+// planes, the same for every lane of V
+template <typename T, typename V = typename Arith<T>::R>
+__device__ __forceinline__ void clover_apply(const typename Store<T>::type* __restrict__ C, int pad,
+                                             int g, V v[24]) {
+  using R = typename Arith<T>::R;
+  clover_apply_with<V>(
+      [&](int i, V a[36]) {
+        R s[36];
+        IO<T>::load_clover_block(C, pad, g, i, s);
+#pragma unroll
+        for (int k = 0; k < 36; k++) a[k] = Lanes<V>::bcast(s[k]);
+      },
+      v);
 }
 
 // FP32 links in 12-real form: the first two rows of U_mu (6 complex) as three

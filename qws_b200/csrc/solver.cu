@@ -34,20 +34,35 @@ HopArgs<T> hop_args(const Geom& G, const typename Store<T>::type* U,
 // when they are on
 template <typename T>
 HopArgs<T> hop_args_c(Ctx& c);
+// (with per-RHS kappa: the handle's clover planes and kappa tables)
 template <>
 HopArgs<float> hop_args_c<float>(Ctx& c) {
   c.ensure_links12();
   auto a = hop_args<float>(c.G, c.Us, c.Cs);
   a.U12 = c.links12_on ? c.Us12 : nullptr;
+  if (!c.rhs_kappas.empty()) {
+    a.Cr = c.Csr;
+    a.kap = c.kap_s;
+  }
   return a;
 }
 template <>
 HopArgs<double> hop_args_c<double>(Ctx& c) {
-  return hop_args<double>(c.G, c.Ud, c.Cd);
+  auto a = hop_args<double>(c.G, c.Ud, c.Cd);
+  if (!c.rhs_kappas.empty()) {
+    a.Cr = c.Cdr;
+    a.kap = c.kap_d;
+  }
+  return a;
 }
 template <>
 HopArgs<H16> hop_args_c<H16>(Ctx& c) {
-  return hop_args<H16>(c.G, c.Uh, c.Ch);
+  auto a = hop_args<H16>(c.G, c.Uh, c.Ch);
+  if (!c.rhs_kappas.empty()) {
+    a.Cr = c.Chr;
+    a.kap = c.kap_s;
+  }
+  return a;
 }
 
 // algorithmic bytes moved per handled site: each spinor stream once per

@@ -4,8 +4,9 @@ Requests (gauge field, kappa, csw, source, tolerance) arrive at any time.
 The service keeps gauge fields resident on the device, builds each
 request's clover term there (qwsg_build_clover), admits work against an
 HBM budget, merges compatible pending requests -- same lattice, gauge
-field, kappa, csw and tolerance -- into one multi-RHS solve
-(qwsg_create_batch), and runs several solves at once on separate CUDA
+field, csw and tolerance; each keeps its own kappa, whose clover term is
+built on the GPU for its RHS (qwsg_batch_set_kappas) -- into one multi-RHS
+solve (qwsg_create_batch), and runs several solves at once on separate CUDA
 streams, so requests that arrive while others are on the GPU start as soon
 as a worker slot and memory are free.  Every result carries its own latency
 (completion minus arrival); `summarize` gives p50/p99 and solves/s.
@@ -43,8 +44,12 @@ def field_bytes(L):
     return _FIELD_BYTES * _pad(int(np.prod(L)))
 
 
+_RHS_CLOVER_BYTES = 72 * (8 + 4 + 2)  # per-RHS clover planes of a merged solve
+
+
 def work_bytes(L, nr):
-    return _WORK_BYTES_PER_RHS * _pad(int(np.prod(L))) * nr
+    per = _WORK_BYTES_PER_RHS + (_RHS_CLOVER_BYTES if nr > 1 else 0)
+    return per * _pad(int(np.prod(L))) * nr
 
 
 @dataclass
@@ -67,7 +72,9 @@ class Request:
     done: threading.Event = field(default_factory=threading.Event)
 
     def key(self):
-        return (self.L, self.gauge, self.kappa, self.csw, self.tol)
+        """Requests with the same key merge into one multi-RHS solve (each
+        keeps its own kappa: per-RHS clover terms, qwsg_batch_set_kappas)."""
+        return (self.L, self.gauge, self.csw, self.tol)
 
     @property
     def latency(self):
@@ -85,7 +92,8 @@ class _Resident:
 
         self.L, self.gid = L, gauge_id
         self.stream = torch.cuda.Stream()
-        self.lat = qws_b200.Lattice(L, NB, tbc=-1, kappa=0.0, stream=self.stream)
+        # (kappa is set per job; a merged job's kernels take only its sign)
+        self.lat = qws_b200.Lattice(L, NB, tbc=-1, kappa=0.125, stream=self.stream)
         self.lat.set_hop_threads(hop_threads)
         self.lat.set_graphs(graphs)
         self.graphs = graphs
@@ -308,12 +316,15 @@ class Service:
             res = live
         r0 = group[0]
         nr = len(group)
-        res.prepare(r0.kappa, r0.csw)
+        if nr == 1:
+            res.prepare(r0.kappa, r0.csw)  # the field's own clover term
         B = res.work.get(nr)
         if B is None:  # work buffers of an nr-RHS solve on this field, kept for reuse
             B = res.lat.batch(nr, stream=res.stream)
             B.set_graphs(self.graphs)
             res.work[nr] = B
+        if nr > 1:  # every request its own kappa: per-RHS clover terms
+            B.set_kappas([q.kappa for q in group], r0.csw)
         s = self.solver
         with torch.cuda.stream(res.stream):
             S = group[0].source if nr == 1 else np.stack([q.source for q in group])

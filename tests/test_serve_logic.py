@@ -47,8 +47,8 @@ L1, L2 = (8, 8, 8, 8), (16, 16, 16, 32)
 
 def test_merge_power_of_two_and_order():
     svc = make_service(1e12, max_batch=4)
-    a = [req(L1, 0, 0.13) for _ in range(5)]
-    b = req(L1, 0, 0.12)
+    a = [req(L1, 0, 0.13 + 0.001 * k) for k in range(5)]  # kappas differ: still compatible
+    b = req(L1, 0, 0.12, tol=1e-8)
     svc.pending = [b] + a
     res, group = svc._pick()
     assert group == [b]                      # the oldest request first
