@@ -860,7 +860,8 @@ def bench_serving(args):
         svc.close()
     out.update({"rate_per_s": args.serve_rate, "window_s": args.serve_window,
                 "warmup_s": round(warmup_s, 2), "warmup_errors": sum(q.error is not None for q in warm),
-                "requests": len(reqs), "merged": svc.merged,
+                "warmup_error_kinds": serve.summarize(warm).get("error_kinds", {}),
+                "requests": len(reqs), "merged": svc.merged, "fields_evicted": svc.evicted,
                 "gauges_per_volume": args.serve_gauges, "workers": 3, "budget_gb": 150,
                 "solver": "bicgstab_dd_mix2_hf (reliable 5), clover built on the GPU per kappa"})
     return out

@@ -32,7 +32,8 @@ from dataclasses import dataclass, field
 import numpy as np
 
 # bytes per padded site of the pieces a job holds on the device
-_FIELD_BYTES = 72 * (8 + 4 + 2) * 2       # gauge + clover, FP64/FP32/FP16 copies
+_FIELD_BYTES = 72 * (8 + 4 + 2) * 2 + 4 * 12 * 4  # gauge + clover, FP64/FP32/FP16
+#                                                   copies; 12-real FP32 links
 _WORK_BYTES_PER_RHS = 9 * 24 * 8 + 9 * 24 * 4 + 4 * 52  # FP64, FP32, FP16 work spinors
 
 
@@ -67,6 +68,11 @@ class Request:
     stats: dict | None = None
     t_start: float = 0.0
     t_done: float = 0.0
+    # phases of the job that ran it (s): field made resident (0 if it was),
+    # clover terms, host->device + solve + device->host
+    t_resident: float = 0.0
+    t_clover: float = 0.0
+    t_solve: float = 0.0
     batch: int = 0
     error: str | None = None
     done: threading.Event = field(default_factory=threading.Event)
@@ -164,6 +170,7 @@ class Service:
         self.ids = itertools.count()
         self.completed = []
         self.merged = 0
+        self.evicted = 0                  # resident fields freed for others
         self.stop = False
         self.workers = [threading.Thread(target=self._worker, daemon=True) for _ in range(workers)]
         for t in self.workers:
@@ -208,15 +215,27 @@ class Service:
         for r in self.residents.values():
             r.close()
         self.residents.clear()
+        import torch
+
+        torch.cuda.empty_cache()  # the result buffers' blocks cached per stream
 
     # ---- scheduling ------------------------------------------------------------
+    def _idle(self, keep=None):
+        return sorted((r for r in self.residents.values()
+                       if not r.busy and r.lat is not None and r is not keep),
+                      key=lambda r: r.last_used)
+
     def _evict(self, need, keep=None):
         """Free idle work handles, then idle resident fields (least recently
         used first; never `keep`) until `need` more bytes fit the budget.
-        Called with cv held."""
-        idle = sorted((r for r in self.residents.values()
-                       if not r.busy and r.lat is not None and r is not keep),
-                      key=lambda r: r.last_used)
+        Frees nothing when even all of that would not make room.  Called with
+        cv held."""
+        if self.used + need <= self.budget:
+            return True
+        idle = self._idle(keep)
+        freeable = sum(r.bytes + sum(work_bytes(r.L, nr) for nr in r.work) for r in idle)
+        if self.used - freeable + need > self.budget:
+            return False
         for r in idle:
             for nr in list(r.work):
                 if self.used + need <= self.budget:
@@ -229,17 +248,36 @@ class Service:
             r.close()
             self.residents.pop((r.L, r.gid))
             self.used -= r.bytes
+            self.evicted += 1
         return self.used + need <= self.budget
+
+    def _reject(self, q, why):
+        self.pending.remove(q)
+        q.error = why
+        q.t_start = q.t_done = time.monotonic()
+        self.completed.append(q)
+        q.done.set()
 
     def _pick(self):
         """The oldest request that can start now, with the compatible pending
-        requests merged into its batch (a power of two, at most max_batch).
-        Called with cv held; reserves the memory and the resident field."""
+        requests merged into its batch (a power of two, at most max_batch, and
+        no larger than the memory allows).  Once a request waits for memory
+        that only running jobs can give back, later requests start only if
+        they need no new memory, so that the waiting one is not overtaken
+        for ever.  A request that cannot fit the budget at all fails at
+        once.  Called with cv held; reserves the memory and the resident
+        field."""
         tried = set()
-        for r in self.pending:
+        blocked = False
+        for r in list(self.pending):
             if r.key() in tried:
                 continue
             tried.add(r.key())
+            if field_bytes(r.L) + work_bytes(r.L, 1) > self.budget:
+                self._reject(r, f"MemoryError: a {'x'.join(map(str, r.L))} solve needs "
+                                f"{(field_bytes(r.L) + work_bytes(r.L, 1)) / 1e9:.1f} GB, "
+                                f"over the {self.budget / 1e9:.1f} GB budget")
+                continue
             res = self.residents.get((r.L, r.gauge))
             if res is not None and res.busy:
                 continue
@@ -247,12 +285,19 @@ class Service:
             nr = 1
             while nr * 2 <= min(len(group), self.max_batch, 32):
                 nr *= 2
-            group = group[:nr]
-            need = (field_bytes(r.L) if res is None else 0) + \
-                (work_bytes(r.L, nr) if res is None or nr not in res.work else 0)
-            if self.used + need > self.budget and not self._evict(need, keep=res):
+            fit = None
+            while fit is None and nr >= 1:
+                need = (field_bytes(r.L) if res is None else 0) + \
+                    (work_bytes(r.L, nr) if res is None or nr not in res.work else 0)
+                if need == 0 or (not blocked and self._evict(need, keep=res)):
+                    fit = need
+                else:
+                    nr //= 2
+            if fit is None:
+                blocked = True
                 continue
-            self.used += need
+            group = group[:nr]
+            self.used += fit
             if res is None:
                 res = _Placeholder(r.L, r.gauge)
                 self.residents[(r.L, r.gauge)] = res
@@ -307,13 +352,16 @@ class Service:
         for q in group:
             q.t_start = t0
         cfg = self.config(res.L)
-        if isinstance(res, _Placeholder):  # first use of this field: make it resident
+        made = isinstance(res, _Placeholder)
+        if made:  # first use of this field: make it resident
             U = self.gauge_source(res.L, res.gid)
             live = _Resident(res.L, res.gid, U, cfg["NB"], cfg["hop_threads"], self.graphs)
             live.busy = True
             with self.cv:
                 self.residents[(res.L, res.gid)] = live
             res = live
+            res.stream.synchronize()
+        t1 = time.monotonic()
         r0 = group[0]
         nr = len(group)
         if nr == 1:
@@ -325,6 +373,8 @@ class Service:
             res.work[nr] = B
         if nr > 1:  # every request its own kappa: per-RHS clover terms
             B.set_kappas([q.kappa for q in group], r0.csw)
+        res.stream.synchronize()
+        t2 = time.monotonic()
         s = self.solver
         with torch.cuda.stream(res.stream):
             S = group[0].source if nr == 1 else np.stack([q.source for q in group])
@@ -337,29 +387,41 @@ class Service:
             per = B.batch_stats()[0] if nr > 1 else [st]
             del bd, xd
         truer = [truer] if nr == 1 else truer
-        t1 = time.monotonic()
+        t3 = time.monotonic()
         for k, q in enumerate(group):
             q.x = X if nr == 1 else X[k]
             q.stats = {"outer_iters": per[k]["outer_iters"], "true_rel_resid": truer[k],
                        "inner_iters": per[k]["inner_iters"]}
             q.batch = nr
-            q.t_done = t1
+            q.t_resident, q.t_clover, q.t_solve = (t1 - t0) if made else 0.0, t2 - t1, t3 - t2
+            q.t_done = t3
 
 
 def summarize(reqs, t_begin=None, t_end=None):
     """p50/p99 latency (ms), solves/s over the span from the first arrival to
     the last completion, batch sizes and errors."""
     ok = [q for q in reqs if q.error is None and q.t_done > 0]
+    kinds = {}
+    for q in reqs:
+        if q.error is not None:
+            kinds[q.error[:160]] = kinds.get(q.error[:160], 0) + 1
     if not ok:
-        return {"completed": 0, "errors": len(reqs)}
+        return {"completed": 0, "errors": len(reqs), "error_kinds": kinds}
     lat = np.array([q.latency for q in ok]) * 1e3
     t0 = min(q.t_arrival for q in ok) if t_begin is None else t_begin
     t1 = max(q.t_done for q in ok) if t_end is None else t_end
-    return {"completed": len(ok), "errors": len(reqs) - len(ok),
+    return {"completed": len(ok), "errors": len(reqs) - len(ok), "error_kinds": kinds,
             "solves_per_s": len(ok) / max(t1 - t0, 1e-9),
             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
             "mean_ms": float(lat.mean()), "max_ms": float(lat.max()),
             "mean_batch": float(np.mean([q.batch for q in ok])),
+            # where the latency goes (p50 / p99 of each phase, ms)
+            "phases_ms": {k: [round(float(np.percentile(v, 50)), 1), round(float(np.percentile(v, 99)), 1)]
+                          for k, v in (("queue", [1e3 * (q.t_start - q.t_arrival) for q in ok]),
+                                       ("resident", [1e3 * q.t_resident for q in ok]),
+                                       ("clover", [1e3 * q.t_clover for q in ok]),
+                                       ("solve", [1e3 * q.t_solve for q in ok]))},
+            "requests_with_field_load": sum(q.t_resident > 0 for q in ok),
             "max_true_rel_resid": max(q.stats["true_rel_resid"] for q in ok),
             "above_tol": sum(q.stats["true_rel_resid"] >= q.tol for q in ok)}
 

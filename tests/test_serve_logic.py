@@ -33,7 +33,8 @@ class FakeResident:
 def make_service(budget, max_batch=16):
     svc = serve.Service.__new__(serve.Service)  # the scheduling state only, no threads
     svc.budget, svc.max_batch = float(budget), max_batch
-    svc.pending, svc.residents, svc.used, svc.merged = [], {}, 0.0, 0
+    svc.pending, svc.residents, svc.used, svc.merged, svc.evicted = [], {}, 0.0, 0, 0
+    svc.completed = []
     svc.cv = threading.Condition()
     return svc
 
@@ -92,8 +93,55 @@ def test_eviction_lru_and_keep():
 
 
 def test_admission_reserves_bytes():
-    svc = make_service(budget=serve.field_bytes(L1) + serve.work_bytes(L1, 2))
+    one2 = serve.field_bytes(L2) + serve.work_bytes(L2, 1)
+    svc = make_service(budget=one2)
     svc.pending = [req(L1, 0, 0.13), req(L1, 0, 0.13), req(L2, 0, 0.13)]
     res, group = svc._pick()
     assert len(group) == 2 and svc.used == serve.field_bytes(L1) + serve.work_bytes(L1, 2)
     assert svc._pick() is None  # L2 does not fit while L1's field is busy
+
+
+def test_batch_capped_by_memory():
+    """Four compatible requests whose 4-RHS batch would not fit the budget
+    run as a batch of two (a batch that can never fit must not wait for
+    ever)."""
+    svc = make_service(budget=serve.field_bytes(L2) + serve.work_bytes(L2, 2) + 1)
+    svc.pending = [req(L2, 0, 0.13 + 0.001 * k) for k in range(4)]
+    res, group = svc._pick()
+    assert len(group) == 2 and len(svc.pending) == 2
+
+
+def test_never_fits_fails_at_once():
+    svc = make_service(budget=serve.field_bytes(L2))
+    big, small = req(L2, 0, 0.13), req(L1, 0, 0.13)
+    svc.pending = [big, small]
+    res, group = svc._pick()
+    assert group == [small]
+    assert big.done.is_set() and "MemoryError" in big.error and svc.pending == []
+
+
+def test_no_futile_eviction():
+    """Idle fields stay when evicting all of them would still not make room."""
+    svc = make_service(budget=2 * serve.field_bytes(L2))
+    idle = FakeResident(L2, 0, last_used=1.0)
+    busy = FakeResident(L2, 1, last_used=1.0, busy=True)
+    svc.residents = {(L2, 0): idle, (L2, 1): busy}
+    svc.used = 2 * serve.field_bytes(L2)
+    assert not svc._evict(2 * serve.field_bytes(L2))
+    assert not idle.closed and (L2, 0) in svc.residents
+
+
+def test_waiting_request_not_overtaken():
+    """A request that waits for memory held by a running job blocks later
+    requests that need new memory; one that needs none still starts."""
+    f2, w2 = serve.field_bytes(L2), serve.work_bytes(L2, 1)
+    svc = make_service(budget=2 * (f2 + w2) - 1)
+    busy = FakeResident(L2, 0, last_used=1.0, busy=True, work=(1,))
+    warm = FakeResident(L1, 0, last_used=1.0, work=(1,))
+    svc.residents = {(L2, 0): busy, (L1, 0): warm}
+    svc.used = f2 + w2 + warm.bytes + serve.work_bytes(L1, 1)
+    waiting, later, ready = req(L2, 1, 0.13), req(L1, 1, 0.13), req(L1, 0, 0.13)
+    svc.pending = [waiting, later, ready]
+    res, group = svc._pick()
+    assert group == [ready] and res is warm
+    assert svc.pending == [waiting, later]
