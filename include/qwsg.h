@@ -95,7 +95,9 @@ int qwsg_build_clover(qwsg_lattice* lat, double csw);
 /* No counterpart in the reference.  A seeded SU(3) gauge field smoothed by
  * n_smear APE-style steps, generated directly into this lattice's FP64 and
  * FP32 gauge planes with the host generator's construction and random
- * streams (qwsg_gen_gauge; equal to rounding); *plaq gets the plaquette. */
+ * streams (qwsg_gen_gauge; equal to rounding); *plaq gets the plaquette.
+ * The smearing uses the FP64 clover planes as scratch: build or load the
+ * clover term afterwards. */
 int qwsg_gen_gauge_device(qwsg_lattice* lat, unsigned long long seed, int n_smear, double alpha,
                           double* plaq);
 

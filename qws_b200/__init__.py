@@ -310,7 +310,9 @@ class Lattice:
         return even, odd
 
     def gen_gauge_device(self, seed, n_smear=5, alpha=0.36):
-        """Seeded SU(3) + APE gauge field generated on the GPU; returns the plaquette."""
+        """Seeded SU(3) + APE gauge field generated on the GPU; returns the
+        plaquette.  The FP64 clover planes serve as scratch: build or load
+        the clover term afterwards."""
         p = ctypes.c_double()
         _check(self.lib.qwsg_gen_gauge_device(self.h, int(seed), int(n_smear), float(alpha),
                                               ctypes.byref(p)))

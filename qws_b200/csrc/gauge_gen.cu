@@ -208,11 +208,12 @@ double gen_gauge_device(Ctx& c, unsigned long long seed, int n_smear, double alp
   c.ensure_fields_s();
   const Geom& G = c.G;
   const size_t n = (size_t)72 * G.pad;
-  double* tmp = nullptr;
-  if (n_smear > 0) QWSG_CUDA(cudaMalloc(&tmp, sizeof(double) * n));
+  // the smearing steps ping-pong between the link planes and the FP64
+  // clover planes (the same size; the clover term of the new field is
+  // built, or loaded, afterwards), so a field of any size needs no scratch
   const int nb = (4 * G.V + 127) / 128;
   double* cur = c.Ud;
-  double* nxt = tmp;
+  double* nxt = c.Cd;
   count_launch();
   k_random_su3<<<nb, 128, 0, c.st>>>(G, cur, seed);
   for (int it = 0; it < n_smear; it++) {
@@ -227,16 +228,15 @@ double gen_gauge_device(Ctx& c, unsigned long long seed, int n_smear, double alp
   count_launch();
   k_d2f_planes<<<(unsigned)((n + 255) / 256), 256, 0, c.st>>>(c.Ud, c.Us, n);
   const int pb = (G.V + 127) / 128;
-  double* part = nullptr;
-  QWSG_CUDA(cudaMalloc(&part, sizeof(double) * pb));
+  double* part = nullptr;  // stream-ordered: no device-wide synchronisation
+  QWSG_CUDA(cudaMallocAsync(&part, sizeof(double) * pb, c.st));
   count_launch();
   k_plaquette<<<pb, 128, 0, c.st>>>(G, c.Ud, part);
   c.check_launch("gen_gauge_device");
   std::vector<double> h(pb);
   QWSG_CUDA(cudaMemcpyAsync(h.data(), part, sizeof(double) * pb, cudaMemcpyDeviceToHost, c.st));
+  QWSG_CUDA(cudaFreeAsync(part, c.st));
   QWSG_CUDA(cudaStreamSynchronize(c.st));
-  cudaFree(part);
-  if (tmp) cudaFree(tmp);
   c.fields_h_valid = false;
   double tot = 0;
   for (double v : h) tot += v;
