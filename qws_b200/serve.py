@@ -53,6 +53,19 @@ def work_bytes(L, nr):
     return per * _pad(int(np.prod(L))) * nr
 
 
+def stream_priority(L):
+    """CUDA stream priority of the jobs on a lattice of extents L: one level
+    higher for every factor 4 of volume below 2^24 sites (at most 3 levels),
+    so that when several solves share the GPU the block scheduler serves
+    the short ones first and their latency does not queue behind the
+    kernels of a large lattice (a lower number is a higher priority)."""
+    V = int(np.prod(L))
+    level = 0
+    while level < 3 and V * 4 ** (level + 1) <= 1 << 24:
+        level += 1
+    return -level
+
+
 @dataclass
 class Request:
     L: tuple
@@ -97,7 +110,7 @@ class _Resident:
         import qws_b200
 
         self.L, self.gid = L, gauge_id
-        self.stream = torch.cuda.Stream()
+        self.stream = torch.cuda.Stream(priority=stream_priority(L))
         # (kappa is set per job; a merged job's kernels take only its sign)
         self.lat = qws_b200.Lattice(L, NB, tbc=-1, kappa=0.125, stream=self.stream)
         self.lat.set_hop_threads(hop_threads)
@@ -422,6 +435,12 @@ def summarize(reqs, t_begin=None, t_end=None):
                                        ("clover", [1e3 * q.t_clover for q in ok]),
                                        ("solve", [1e3 * q.t_solve for q in ok]))},
             "requests_with_field_load": sum(q.t_resident > 0 for q in ok),
+            # per lattice: requests, p50 latency, p50 of the solve phase (ms)
+            "by_volume": {"x".join(map(str, L)): [
+                len(v), round(float(np.percentile([q.latency * 1e3 for q in v], 50)), 1),
+                round(float(np.percentile([q.t_solve * 1e3 for q in v], 50)), 1)]
+                for L in sorted({q.L for q in ok}, key=lambda L: int(np.prod(L)))
+                for v in [[q for q in ok if q.L == L]]},
             "max_true_rel_resid": max(q.stats["true_rel_resid"] for q in ok),
             "above_tol": sum(q.stats["true_rel_resid"] >= q.tol for q in ok)}
 

@@ -145,3 +145,11 @@ def test_waiting_request_not_overtaken():
     res, group = svc._pick()
     assert group == [ready] and res is warm
     assert svc.pending == [waiting, later]
+
+
+def test_stream_priority_by_volume():
+    """Smaller lattices get higher CUDA stream priority (lower numbers), one
+    level per factor 4 of volume, at most three levels above the default."""
+    vols = [(48, 48, 48, 96), (32, 32, 32, 64), (24, 24, 24, 48), (16, 16, 16, 32), (8, 8, 8, 8)]
+    pr = [serve.stream_priority(L) for L in vols]
+    assert pr == sorted(pr, reverse=True) and pr[0] == 0 and min(pr) == -3
