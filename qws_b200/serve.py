@@ -73,7 +73,10 @@ class Request:
     kappa: float
     csw: float
     tol: float
-    source: np.ndarray            # natural layout [V, 24] FP64
+    source: np.ndarray            # natural layout [V, 24] FP64 (page-locked: faster upload)
+    # where the solution goes: None -> a new host array; or a C-contiguous
+    # FP64 [V, 24] array of the caller's (page-locked: faster download)
+    out: np.ndarray | None = None
     rid: int = -1
     t_arrival: float = 0.0
     # filled in by the service
@@ -390,19 +393,32 @@ class Service:
         t2 = time.monotonic()
         s = self.solver
         with torch.cuda.stream(res.stream):
-            S = group[0].source if nr == 1 else np.stack([q.source for q in group])
+            if nr == 1:
+                S = group[0].source  # pinned by the client, or pageable
+            else:  # the sources side by side in the handle's pinned buffer
+                S = getattr(B, "pinned_sources", None)
+                if S is None:
+                    S = torch.empty((nr, B.V, 24), dtype=torch.float64, pin_memory=True).numpy()
+                    B.pinned_sources = S
+                for k, q in enumerate(group):
+                    S[k] = q.source
             bd = B.to_device(S)
             xd = B.empty("f64")
             st = B.bicgstab_dd_mix2_hf(xd, bd, r0.tol, s["maxiter"], s["tol_s"], s["maxiter_s"],
                                        cfg["nsap"], cfg["nm"], reliable=s["reliable"])
             truer = B.true_residual(xd, bd)
-            X = B.to_host(xd)
+            if nr == 1:
+                X = B.to_host(xd, out=r0.out)
+            else:
+                X = B.to_host(xd)
             per = B.batch_stats()[0] if nr > 1 else [st]
             del bd, xd
         truer = [truer] if nr == 1 else truer
         t3 = time.monotonic()
         for k, q in enumerate(group):
-            q.x = X if nr == 1 else X[k]
+            if nr > 1 and q.out is not None:
+                q.out[...] = X[k]
+            q.x = X if nr == 1 else (X[k] if q.out is None else q.out)
             q.stats = {"outer_iters": per[k]["outer_iters"], "true_rel_resid": truer[k],
                        "inner_iters": per[k]["inner_iters"]}
             q.batch = nr
@@ -464,15 +480,22 @@ def poisson_workload(service, rate, window, volumes, weights, n_gauges, kappa_ra
     """Poisson arrivals at `rate` per second for `window` seconds.  Each
     request draws a volume (with `weights`), a gauge id, kappa uniform in
     kappa_range, a tolerance and a Gaussian or point source.  Sources come from
-    a small pool made before the window opens, so the feeder keeps up with the
-    arrival times.  Returns the submitted requests (wait on req.done)."""
+    a small pool of page-locked host arrays made before the window opens, so
+    the feeder keeps up with the arrival times.  Returns the submitted requests (wait on req.done)."""
     import qws_b200
+
+    import torch
+
+    def pinned(a):  # the client's source in page-locked memory (DMA to the GPU)
+        p = torch.empty(a.shape, dtype=torch.float64, pin_memory=True).numpy()
+        p[...] = a
+        return p
 
     rng = np.random.default_rng(seed)
     pool = {}
     for L in volumes:
-        pool[L] = [qws_b200.gen_source(L, 5000 + k, "gauss") for k in range(sources_per_volume)]
-        pool[L] += [qws_b200.gen_source(L, 0, "point", k) for k in range(2)]
+        pool[L] = [pinned(qws_b200.gen_source(L, 5000 + k, "gauss")) for k in range(sources_per_volume)]
+        pool[L] += [pinned(qws_b200.gen_source(L, 0, "point", k)) for k in range(2)]
     t = 0.0
     arrivals = []
     while True:

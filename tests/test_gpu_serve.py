@@ -74,3 +74,39 @@ def test_small_budget_evicts_and_completes():
         assert svc.used <= budget
     finally:
         svc.close()
+
+
+def test_caller_output_buffers():
+    """A request's solution lands in the caller's array (page-locked or not),
+    alone and when merged into a batch; sources may be page-locked."""
+    import torch
+
+    from qws_b200 import serve
+
+    reqs = make_requests(serve, 12, 3)
+    svc = serve.Service(serve.seeded_gauge(), budget_bytes=40e9, workers=2, max_batch=8)
+    try:
+        ref = []
+        for r in reqs:
+            q = svc.submit(clone(serve, r))
+            q.done.wait()
+            assert q.error is None, q.error
+            ref.append(q.x)
+        subs = []
+        for k, r in enumerate(reqs):
+            q = clone(serve, r)
+            shape = (int(np.prod(r.L)), 24)
+            pin = torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+            pin[...] = r.source
+            q.source = pin
+            q.out = (torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy() if k % 2
+                     else np.empty(shape))
+            subs.append(svc.submit(q))
+        for q, x in zip(subs, ref):
+            q.done.wait()
+            assert q.error is None, q.error
+            assert q.x is q.out
+            assert np.linalg.norm(q.out - x) / np.linalg.norm(x) < 1e-8
+        assert max(q.batch for q in subs) > 1
+    finally:
+        svc.close()
