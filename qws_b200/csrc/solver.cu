@@ -74,7 +74,10 @@ double hop_bytes(int sel, int epi, int nr, bool links12 = false) {
                lc = (links12 ? Bytes<T>::links * 2 / 3 : Bytes<T>::links) + Bytes<T>::clover;
   if (epi == EPI_JINV) return 3 * sp + lc;  // src, b, out
   if (epi == EPI_SAPE) return 4 * sp + lc;  // a, in, s (r+w)
-  if (epi == EPI_ADD) return 3 * sp + lc;   // out (r+w), one face neighbour
+  // out (r+w), one face neighbour and its one link (a face site has 1.1
+  // face hops on average at the reference partition), clover
+  if (epi == EPI_ADD)
+    return 3 * sp + (links12 ? Bytes<T>::links * 2 / 3 : Bytes<T>::links) / 4 + Bytes<T>::clover;
   (void)sel;
   return 2 * sp + lc;                       // in, out
 }
