@@ -407,10 +407,20 @@ class Service:
             st = B.bicgstab_dd_mix2_hf(xd, bd, r0.tol, s["maxiter"], s["tol_s"], s["maxiter_s"],
                                        cfg["nsap"], cfg["nm"], reliable=s["reliable"])
             truer = B.true_residual(xd, bd)
-            if nr == 1:
+            if nr == 1 and r0.out is not None:
                 X = B.to_host(xd, out=r0.out)
             else:
-                X = B.to_host(xd)
+                # download into the handle's page-locked buffer (DMA), then
+                # a multi-threaded copy into fresh host memory, which also
+                # spreads the new pages' first-touch faults over the threads
+                P = getattr(B, "pinned_result", None)
+                if P is None:
+                    shape = (B.V, 24) if nr == 1 else (nr, B.V, 24)
+                    P = torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+                    B.pinned_result = P
+                B.to_host(xd, out=P)
+                X = np.empty_like(P)
+                torch.from_numpy(X).copy_(torch.from_numpy(P))
             per = B.batch_stats()[0] if nr > 1 else [st]
             del bd, xd
         truer = [truer] if nr == 1 else truer
