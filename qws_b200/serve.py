@@ -393,15 +393,22 @@ class Service:
         t2 = time.monotonic()
         s = self.solver
         with torch.cuda.stream(res.stream):
-            if nr == 1:
-                S = group[0].source  # pinned by the client, or pageable
-            else:  # the sources side by side in the handle's pinned buffer
-                S = getattr(B, "pinned_sources", None)
-                if S is None:
-                    S = torch.empty((nr, B.V, 24), dtype=torch.float64, pin_memory=True).numpy()
-                    B.pinned_sources = S
-                for k, q in enumerate(group):
-                    S[k] = q.source
+            S = np.ascontiguousarray(group[0].source, np.float64) if nr == 1 else None
+            if S is None or not torch.from_numpy(S).is_pinned():
+                # pageable (or several) sources: a multi-threaded copy into the
+                # handle's page-locked buffer, from which the upload is a DMA
+                P = getattr(B, "pinned_sources", None)
+                if P is None:
+                    shape = (B.V, 24) if nr == 1 else (nr, B.V, 24)
+                    P = torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+                    B.pinned_sources = P
+                if nr == 1:
+                    torch.from_numpy(P).copy_(torch.from_numpy(S.reshape(P.shape)))
+                else:
+                    for k, q in enumerate(group):
+                        torch.from_numpy(P[k]).copy_(torch.from_numpy(
+                            np.ascontiguousarray(q.source, np.float64).reshape(P[k].shape)))
+                S = P
             bd = B.to_device(S)
             xd = B.empty("f64")
             st = B.bicgstab_dd_mix2_hf(xd, bd, r0.tol, s["maxiter"], s["tol_s"], s["maxiter_s"],
