@@ -394,7 +394,10 @@ def bench_ours(args, w, name):
                     "bytes_per_launch": kbytes / nl, "avg_launch_us": kms / nl * 1e3,
                     "launches": nl,
                     "share_of_kernel_time": round(kms / sum(v[1] for v in kstats.values()), 4)}
-    kernels = kernel_table(kstats, peak)
+    kernels = kernel_table(kstats, peak, w["L"], w["NB"])
+    if roofline and "GFLOPs" in kernels.get(roofline["kernel"], {}):
+        roofline["gflops"] = kernels[roofline["kernel"]]["GFLOPs"]
+        roofline["flop_convention"] = "1872 per site (1320 hops + 504 clover + 48 axpy)"
 
     line = {
         "metric": METRIC,
@@ -438,7 +441,7 @@ def bench_ours(args, w, name):
             "inner_iters": sum(s["inner_iters"] for s in hstats) / len(hstats),
             "config": {"block_grid": list(tl.NB), **cfg},
             "tuning": tuned,
-            "kernels": kernel_table(hf_kstats, peak),
+            "kernels": kernel_table(hf_kstats, peak, w["L"], tl.NB),
             "at_reference_partition": {
                 "block_grid": list(w["NB"]), "nsap": w["nsap"], "nm": w["nm"],
                 "value": world * args.steps / (hf_ref_ms * 1e-3),
@@ -479,9 +482,31 @@ def bench_ours(args, w, name):
         print(json.dumps(line), flush=True)
 
 
-def kernel_table(kstats, peak):
+# flops per handled site, the convention of the Wilson-clover D: 1320 for
+# the eight hops (165 each: projection, SU(3) x half-spinor, reconstruction),
+# 504 for the packed-Hermitian clover product, 48 for the axpy epilogue;
+# a block or Richardson application counts as a whole site, a face site as
+# its 1.1 face hops (average at the reference partition) + clover + axpy
+FLOPS_PER_SITE = {"dslash_full": 1872, "dslash_block": 1872, "jinv_step": 1872,
+                  "sap_update": 1872 + 48, "dslash_face": round(1.1 * 165) + 504 + 48}
+
+
+def sites_per_launch(kind, L, NB, nr):
+    """sites one launch of kernel kind handles (times the RHS count)"""
+    V = int(np.prod(L))
+    if kind.startswith("dslash_full"):
+        return V * nr
+    if kind.startswith("dslash_face"):
+        B = [L[m] // NB[m] for m in range(4)]
+        inner = int(np.prod([b - 2 if b > 2 else 0 for b in B]))
+        return int(np.prod(NB)) // 2 * (int(np.prod(B)) - inner) * nr
+    return V // 2 * nr
+
+
+def kernel_table(kstats, peak, L=None, NB=None, nr=1):
     """{kernel: launches, device ms, share of the solve's kernel time,
-    algorithmic GB/s and its fraction of the measured HBM peak}"""
+    algorithmic GB/s and its fraction of the measured HBM peak, and GFLOP/s
+    in the 1872-flop-per-site convention (FLOPS_PER_SITE)}"""
     total = sum(v[1] for v in kstats.values()) or 1.0
     out = {}
     for k, (n, ms, by) in sorted(kstats.items(), key=lambda kv: -kv[1][1]):
@@ -489,6 +514,10 @@ def kernel_table(kstats, peak):
         out[k] = {"launches": n, "ms": round(ms, 3), "share": round(ms / total, 4),
                   "GBps": round(gbs, 1) if gbs else None,
                   "frac_of_peak": round(gbs / peak, 4) if gbs else None}
+        base = k.rsplit("_", 1)[0]
+        if L is not None and base in FLOPS_PER_SITE and ms:
+            fl = FLOPS_PER_SITE[base] * sites_per_launch(k, L, NB, nr) * n
+            out[k]["GFLOPs"] = round(fl / (ms * 1e-3) / 1e9, 1)
     return out
 
 

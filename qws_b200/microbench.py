@@ -97,6 +97,9 @@ def main():
     if nbytes:
         res["bytes_per_launch"] = nbytes
         res["GBps"] = nbytes / (us * 1e-6) / 1e9
+        # 1872 flops per site (1320 hops + 504 clover + 48 axpy), per RHS
+        sites = (V if k in ("dslash_s", "dslash_d") else V // 2) * nr
+        res["GFLOPs"] = 1872 * sites / (us * 1e-6) / 1e9
     print(json.dumps(res), flush=True)
     lat.close()
     if lat is not base:
