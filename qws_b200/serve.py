@@ -279,10 +279,11 @@ class Service:
         requests merged into its batch (a power of two, at most max_batch, and
         no larger than the memory allows).  Once a request waits for memory
         that only running jobs can give back, later requests start only if
-        they need no new memory, so that the waiting one is not overtaken
-        for ever.  A request that cannot fit the budget at all fails at
-        once.  Called with cv held; reserves the memory and the resident
-        field."""
+        they fit the free budget without evicting anything: the idle memory
+        the waiting request will need stays in place, and a short job that
+        takes free memory gives it back when it ends.  A request that cannot
+        fit the budget at all fails at once.  Called with cv held; reserves
+        the memory and the resident field."""
         tried = set()
         blocked = False
         for r in list(self.pending):
@@ -305,7 +306,8 @@ class Service:
             while fit is None and nr >= 1:
                 need = (field_bytes(r.L) if res is None else 0) + \
                     (work_bytes(r.L, nr) if res is None or nr not in res.work else 0)
-                if need == 0 or (not blocked and self._evict(need, keep=res)):
+                if need == 0 or self.used + need <= self.budget or \
+                        (not blocked and self._evict(need, keep=res)):
                     fit = need
                 else:
                     nr //= 2

@@ -133,18 +133,31 @@ def test_no_futile_eviction():
 
 def test_waiting_request_not_overtaken():
     """A request that waits for memory held by a running job blocks later
-    requests that need new memory; one that needs none still starts."""
+    requests that would have to evict idle memory; one that needs no new
+    memory, or fits the free budget, still starts."""
     f2, w2 = serve.field_bytes(L2), serve.work_bytes(L2, 1)
-    svc = make_service(budget=2 * (f2 + w2) - 1)
-    busy = FakeResident(L2, 0, last_used=1.0, busy=True, work=(1,))
-    warm = FakeResident(L1, 0, last_used=1.0, work=(1,))
-    svc.residents = {(L2, 0): busy, (L1, 0): warm}
-    svc.used = f2 + w2 + warm.bytes + serve.work_bytes(L1, 1)
-    waiting, later, ready = req(L2, 1, 0.13), req(L1, 1, 0.13), req(L1, 0, 0.13)
-    svc.pending = [waiting, later, ready]
+    warm_bytes = serve.field_bytes(L1) + serve.work_bytes(L1, 1)
+
+    def setup(budget):
+        svc = make_service(budget=budget)
+        busy = FakeResident(L2, 0, last_used=1.0, busy=True, work=(1,))
+        warm = FakeResident(L1, 0, last_used=1.0, work=(1,))
+        svc.residents = {(L2, 0): busy, (L1, 0): warm}
+        svc.used = f2 + w2 + warm_bytes
+        waiting, later, ready = req(L2, 1, 0.13), req(L1, 1, 0.13), req(L1, 0, 0.13)
+        svc.pending = [waiting, later, ready]
+        return svc, warm, waiting, later, ready
+
+    # `later` (a new L1 field) would need `warm` evicted: it waits
+    svc, warm, waiting, later, ready = setup(f2 + w2 + 2 * warm_bytes - 1)
     res, group = svc._pick()
-    assert group == [ready] and res is warm
+    assert group == [ready] and res is warm and not warm.closed
     assert svc.pending == [waiting, later]
+    # with room for it in the free budget, `later` starts before `ready`
+    svc, warm, waiting, later, ready = setup(f2 + w2 + 2 * warm_bytes)
+    res, group = svc._pick()
+    assert group == [later] and not warm.closed
+    assert svc.pending == [waiting, ready]
 
 
 def test_stream_priority_by_volume():
