@@ -166,3 +166,23 @@ def test_stream_priority_by_volume():
     vols = [(48, 48, 48, 96), (32, 32, 32, 64), (24, 24, 24, 48), (16, 16, 16, 32), (8, 8, 8, 8)]
     pr = [serve.stream_priority(L) for L in vols]
     assert pr == sorted(pr, reverse=True) and pr[0] == 0 and min(pr) == -3
+
+
+def test_summarize_phases_errors_and_volumes():
+    """summarize: failed requests are counted by kind and left out of the
+    latencies; phases and per-volume figures come from the completed ones."""
+    def done(L, lat, solve, err=None, res=0.0):
+        q = req(L, 0, 0.13)
+        q.t_arrival, q.t_start, q.t_done = 0.0, 0.01, lat
+        q.t_resident, q.t_clover, q.t_solve = res, 0.001, solve
+        q.stats, q.batch, q.error = {"true_rel_resid": 1e-12}, 1, err
+        return q
+
+    reqs = [done(L1, 0.05, 0.02), done(L1, 0.07, 0.03), done(L2, 0.5, 0.3, res=0.1),
+            done(L2, 0.0, 0.0, err="MemoryError: too big")]
+    st = serve.summarize(reqs)
+    assert st["completed"] == 3 and st["errors"] == 1
+    assert st["error_kinds"] == {"MemoryError: too big": 1}
+    assert st["requests_with_field_load"] == 1 and st["above_tol"] == 0
+    assert st["by_volume"]["8x8x8x8"][0] == 2 and st["by_volume"]["16x16x16x32"] == [1, 500.0, 300.0]
+    assert st["phases_ms"]["queue"][0] == 10.0
