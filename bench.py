@@ -46,15 +46,6 @@ METRIC = "solves/s @1e-10 resid: mixed-prec vs plain FP64 on B200; Dslash GB/s; 
 METRIC_DETAIL = ("value: plain DD BiCGStab solves/s (FP64 outer / FP32 SAP inner, 1e-10 true "
                  "relative residual); precision_form: the mixed-precision solver on the same "
                  "workload; roofline: the dominant stencil kernel's HBM GB/s")
-# iteration counts of one full solve of each workload, measured with this
-# repository's GPU solver (same algorithm and partition as the reference);
-# used to scale the reference's bounded CPU sample to solves/s.
-REF_COUNTS = {
-    "plain_32c64": {"inner_iters": 16, "n_approx": 2, "n_ddd_d": 4},
-    "plain_16c32": {"inner_iters": 16, "n_approx": 2, "n_ddd_d": 4},
-}
-
-
 _T0 = time.time()
 
 
@@ -134,11 +125,15 @@ def make_fields(w):
     return U, C, b, plaq, time.time() - t0
 
 
-def run_reference_sample(w, counts, threads=None, repeats=1):
-    """The reference's CPU solver timed on this host (subprocess)."""
-    spec = dict(w)
-    spec["counts"] = counts
-    spec["repeats"] = repeats
+def run_reference(w, warmup, steps, solution_out=None, threads=None):
+    """Complete solves of the reference's own CPU solver on this host
+    (oracle/refbench.py in a subprocess, all host threads): `warmup` untimed
+    then `steps` timed bicgstab_dd_mix_ calls on the workload's fields, which
+    the oracle generates bit-equal to the product's."""
+    spec = {k: (list(v) if isinstance(v, tuple) else v) for k, v in w.items()}
+    spec.update(warmup=int(warmup), steps=int(steps))
+    if solution_out:
+        spec["solution_out"] = str(solution_out)
     env = dict(os.environ)
     n = threads or len(os.sched_getaffinity(0))
     env["OMP_NUM_THREADS"] = str(n)
@@ -147,8 +142,26 @@ def run_reference_sample(w, counts, threads=None, repeats=1):
     res = subprocess.run([sys.executable, str(ROOT / "oracle" / "refbench.py"), json.dumps(spec)],
                          capture_output=True, text=True, env=env, timeout=3600)
     if res.returncode != 0:
-        raise RuntimeError("reference sample failed: " + res.stderr[-2000:])
+        raise RuntimeError("reference run failed: " + res.stderr[-2000:])
     return json.loads(res.stdout.strip().splitlines()[-1])
+
+
+def field_digests(U, C, b):
+    """SHA-256 of the arrays a solve consumes (compared with the reference arm's)."""
+    import hashlib
+
+    h = lambda a: hashlib.sha256(memoryview(np.ascontiguousarray(a)).cast("B")).hexdigest()
+    return {"gauge": h(U), "clover": h(C), "source": h(b)}
+
+
+def config_of(w, name):
+    """The `config` object of both arms' lines: the workload, nothing else."""
+    return {"workload": name, "lattice": "x".join(map(str, w["L"])),
+            "block_grid": list(w["NB"]), "kappa": w["kappa"], "csw": w["csw"],
+            "tol": w["tol"], "tol_s": w["tol_s"], "maxiter_s": w["maxiter_s"],
+            "nsap": w["nsap"], "nm": w["nm"],
+            "l2": "inputs larger than L2 (one FP64 spinor = %.0f MB)"
+                  % (int(np.prod(w["L"])) * 24 * 8 / 1e6)}
 
 
 def dist_setup(n_gpus):
@@ -196,6 +209,7 @@ def bench_ours(args, w, name):
     world, rank, local = dist_setup(args.gpus)
     progress(f"fields for {name}")
     U, C, b, plaq, t_gen = make_fields(w)
+    digests = field_digests(U, C, b) if rank == 0 and not args.no_cpu_baseline else None
     stream = torch.cuda.Stream()
     lat = qws_b200.Lattice(w["L"], w["NB"], tbc=w["tbc"], kappa=w["kappa"], stream=stream)
     lat.load_fields(U, C)
@@ -246,6 +260,8 @@ def bench_ours(args, w, name):
         torch.cuda.synchronize()
         kstats = lat.kernel_stats()
         lat.kernel_timing(False)
+        # the plain solver's solution, checked against the reference's below
+        x_gpu = lat.to_host(xd) if rank == 0 and world == 1 and not args.no_cpu_baseline else None
 
         progress("end-to-end solves")
         # ---- end to end through the public API with host buffers --------------
@@ -414,12 +430,7 @@ def bench_ours(args, w, name):
         "dtype": "f64 outer / f32 inner",
         "data": "synthetic: seeded SU(3) links + 5 APE steps (plaquette %.4f), clover-leaf "
                 "clover, Gaussian source" % plaq,
-        "config": {"workload": name, "lattice": "x".join(map(str, w["L"])),
-                   "block_grid": list(w["NB"]), "kappa": w["kappa"], "csw": w["csw"],
-                   "tol": w["tol"], "tol_s": w["tol_s"], "maxiter_s": w["maxiter_s"],
-                   "nsap": w["nsap"], "nm": w["nm"],
-                   "l2": "inputs larger than L2 (one FP64 spinor = %.0f MB)" % (V * 24 * 8 / 1e6),
-                   "parallelism": f"replicas x{world}"},
+        "config": dict(config_of(w, name), parallelism=f"replicas x{world}"),
         "solve": {"outer_iters": outer_iters, "inner_iters": inner_iters,
                   "true_rel_resid": true_rel, "recursive_rel_resid": stats[-1]["rel_resid_recursive"]},
         "e2e": (dict(e2e_ref_api, value=world * e2e_ref_api["value"])
@@ -464,13 +475,9 @@ def bench_ours(args, w, name):
         batched["speedup_vs_plain"] = batched["value"] / line["value"]
         batched["speedup_vs_precision_single"] = batched["value"] / line["precision_form"]["value"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            ref = run_reference_sample(w, counts)
-            line["cpu_baseline"] = {"value": ref["solves_per_s"], "unit": "solves/s",
-                                    "cores": ref["threads"], "kind": "reference",
-                                    "sample": ref["sample"]}
-        except Exception as e:  # the baseline is reported, never required
-            line["cpu_baseline"] = {"value": None, "unit": "solves/s", "error": str(e)[-300:]}
+        progress("cpu baseline: complete reference solves")
+        line["cpu_baseline"] = sub(cpu_baseline, w, x_gpu, digests, line["solve"])
+    del x_gpu
     lat.close()
     if tl is not lat:
         tl.close()
@@ -896,32 +903,58 @@ def bench_serving(args):
     return out
 
 
+def cpu_baseline(w, x_gpu, digests, gpu_solve):
+    """The reference's CPU solver on this host, one untimed and one timed
+    complete solve of the same workload (about 30 s of host work), and the
+    GPU solution's distance to the reference's solution.  The reference's
+    inputs come from the oracle's generator; their digests must equal the
+    GPU arm's (the same arrays)."""
+    import tempfile
+
+    with tempfile.TemporaryDirectory() as td:
+        sol = Path(td) / "x_ref.npy"
+        ref = run_reference(w, 1, 1, solution_out=sol)
+        x_ref = np.load(sol)
+    err = float(np.linalg.norm(x_gpu - x_ref) / np.linalg.norm(x_ref))
+    return {"value": ref["solves_per_s"], "unit": "solves/s", "cores": ref["threads"],
+            "kind": "reference", "sample": ref["sample"],
+            "reference_solve": {"outer_iters": ref["outer_iters"],
+                                "inner_iters": ref["inner_iters_per_solve"],
+                                "true_rel_resid": ref["true_rel_resid"]},
+            "gpu_solve": {"outer_iters": gpu_solve["outer_iters"],
+                          "inner_iters": gpu_solve["inner_iters"],
+                          "true_rel_resid": gpu_solve["true_rel_resid"]},
+            "rel_error_vs_reference": err,
+            "same_fields": digests == ref["field_sha256"]}
+
+
 def bench_reference(args, w, name):
+    """The reference arm: the reference's own bicgstab_dd_mix_ (built from its
+    sources, oracle/_ref) on this host's cores, `warmup` untimed and `steps`
+    timed complete solves of the same workload, in one process."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    counts = REF_COUNTS.get(name)
-    if counts is None:
-        print(json.dumps({"impl": "reference",
-                          "unavailable": f"no recorded iteration counts for workload {name}"}))
-        return
-    # one process: fields and the reference's state are set up once, then
-    # warmup + steps bounded samples are timed back to back
-    ref = run_reference_sample(w, counts, repeats=args.warmup + args.steps)
-    vals = ref["solves_per_s_samples"][args.warmup:]
-    v = statistics.median(vals)
+    ref = run_reference(w, args.warmup, args.steps)
+    v = ref["solves_per_s"]
     line = {
         "impl": "reference",
         "metric": METRIC,
         "metric_detail": METRIC_DETAIL,
         "value": v, "unit": "solves/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64 outer / f32 inner", "data": "synthetic (same fields as the GPU arm)",
-        "config": {"workload": name, "lattice": "x".join(map(str, w["L"])),
-                   "block_grid": list(w["NB"])},
+        "dtype": "f64 outer / f32 inner", "data": "synthetic: seeded SU(3) links + 5 APE steps "
+        "(plaquette %.4f), clover-leaf clover, Gaussian source; arrays bit-equal to the GPU "
+        "arm's (field_sha256)" % ref["plaquette"],
+        "config": dict(config_of(w, name), parallelism="host threads x%d" % ref["threads"]),
         "cpu_baseline": {"value": v, "unit": "solves/s", "cores": ref["threads"],
                          "kind": "reference", "sample": ref["sample"]},
         "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "solve": {"outer_iters": ref["outer_iters"], "inner_iters": ref["inner_iters_per_solve"],
+                  "inner_solves": ref["inner_solves_per_solve"],
+                  "true_rel_resid": ref["true_rel_resid"]},
+        "solve_s": ref["solve_s"],
+        "field_sha256": ref["field_sha256"],
     }
     print(json.dumps(line), flush=True)
 

@@ -129,7 +129,10 @@ int qwsg_jinv_s(qwsg_lattice* lat, float* x, const float* b, int colour, int nm)
  * reserved on every GPU that loads it; lattices whose padded volume exceeds
  * 349,525 sites are rejected (code 2).  The first call on a device looks up
  * the array's device address (make it before any stream capture).  All calls
- * share the array: calls that overlap on the GPU race. */
+ * share the array: calls that overlap on the GPU race.  Handles made by
+ * qwsg_create_batch are rejected (code 1).  The 12-real links are read when
+ * an earlier FP32 call on the handle made them (qwsg_jinv_s does on SU(3)
+ * fields), else the full links (equal to a few FP32 roundoffs). */
 int qwsg_jinv_s_noalloc(qwsg_lattice* lat, float* x, const float* b, int colour, int nm);
 /* prec_ddd_s_ (qws.cc:776) out = D M_SAP in ; prec_s_ (qws.cc:929) out = M_SAP in */
 int qwsg_prec_ddd_s(qwsg_lattice* lat, float* out, const float* in, int nsap, int nm);
@@ -152,6 +155,21 @@ int qwsg_true_residual(qwsg_lattice* lat, const double* x, const double* b, doub
  * + the final stage, fields and spinors stored in FP16 (the reference stores
  * the spinor with one global scale and computes in FP16, qws_h.cc:175-269) */
 int qwsg_prec_s_h(qwsg_lattice* lat, float* out, const float* in, int nsap, int nm);
+/* Single applications of the FP16-storage kernels the SAP above is made of,
+ * FP32 in and out: the operands are stored in FP16 with per-site scales (as
+ * the SAP stores them), the kernel runs, the result is converted back.
+ * ddd_in_h_ (ddd_in_h.h:54): out = D_blk in on one colour's blocks */
+int qwsg_ddd_in_h(qwsg_lattice* lat, float* out, const float* in, int colour);
+/* jinv_ddd_in_h_ (jinv_ddd_in_h.h:53): nm Richardson steps on one colour */
+int qwsg_jinv_h(qwsg_lattice* lat, float* x, const float* b, int colour, int nm);
+/* ddd_out_pre_h_ + ddd_out_pos_h_ (ddd_out_h.h:57,283): out += factor
+ * A^-1 H_face in on one colour's block faces */
+int qwsg_ddd_out_h(qwsg_lattice* lat, float* out, const float* in, int colour, double factor);
+/* The SAP half-sweep update s_c += in_c - D_blk a_c on one colour, in FP32
+ * and in FP16 storage: the reference's inline loops qws.cc:815-818 and
+ * prec_ddd_s_h.h:143-150 (no separate entry point there). */
+int qwsg_sap_update_s(qwsg_lattice* lat, float* s, const float* a, const float* in, int colour);
+int qwsg_sap_update_h(qwsg_lattice* lat, float* s, const float* a, const float* in, int colour);
 /* bicgstab_precdd_s_h_ (bicgstab_precdd_s_h.cc:83): flexible FP32 BiCGStab
  * with the FP16 SAP preconditioner; x solves D x = b */
 int qwsg_bicgstab_precdd_s_h(qwsg_lattice* lat, float* x, const float* b, double tol, int maxiter,

@@ -55,8 +55,9 @@ def load_oracle():
     global _oracle
     if _oracle is not None:
         return _oracle
-    src = ORACLE_DIR / "qws_oracle.cc"
-    if not ORACLE_SO.exists() or ORACLE_SO.stat().st_mtime < src.stat().st_mtime:
+    srcs = [ORACLE_DIR / n for n in ("qws_oracle.cc", "qws_oracle.h", "fields_oracle.cc")]
+    if not ORACLE_SO.exists() or any(ORACLE_SO.stat().st_mtime < s.stat().st_mtime
+                                     for s in srcs if s.exists()):
         subprocess.run(["make", "-C", str(ORACLE_DIR), "oracle", "CXX=g++"], check=True,
                        stdout=subprocess.DEVNULL)
     lib = ctypes.CDLL(str(ORACLE_SO))
@@ -110,6 +111,13 @@ def load_oracle():
     lib.orc_cg_vm.argtypes = [vp, _dp, _dp, ctypes.c_int]
     lib.orc_mcg_vm.restype = ctypes.c_int
     lib.orc_mcg_vm.argtypes = [vp, _dp, _dp, ctypes.c_int, _dp, ctypes.c_int]
+    lib.orc_gen_gauge.argtypes = [_dp, _ip, ctypes.c_ulonglong, ctypes.c_int, ctypes.c_double,
+                                  _dp]
+    lib.orc_plaquette.restype = ctypes.c_double
+    lib.orc_plaquette.argtypes = [_dp, _ip]
+    lib.orc_gen_clover.restype = ctypes.c_int
+    lib.orc_gen_clover.argtypes = [_dp, _dp, _ip, ctypes.c_double, ctypes.c_double]
+    lib.orc_gen_source.argtypes = [_dp, _ip, ctypes.c_ulonglong, ctypes.c_int, ctypes.c_int]
     lib.orc_norm2_d.restype = ctypes.c_double
     lib.orc_norm2_d.argtypes = [_dp, ctypes.c_long]
     lib.orc_norm2_s.restype = ctypes.c_double
@@ -289,6 +297,44 @@ class Oracle:
         self.lib.orc_bicgstab_dd_mix(self.h, dptr(x), dptr(np.ascontiguousarray(b)), tol, maxiter,
                                      tol_s, maxiter_s, nsap, nm, dptr(stats), dptr(hist))
         return x, stats, hist
+
+
+def gen_gauge(L, seed=1, n_smear=5, alpha=0.36):
+    """The benchmark's seeded SU(3) links after n_smear smoothing steps,
+    natural layout [4, V, 18] (fields_oracle.cc); returns (U, plaquette).
+    Bit-equal to the product's qws_b200.gen_gauge."""
+    lib = load_oracle()
+    V = int(np.prod(L))
+    U = np.empty((4, V, 18), np.float64)
+    p = ctypes.c_double()
+    lib.orc_gen_gauge(dptr(U), iarr(L), int(seed), int(n_smear), float(alpha), ctypes.byref(p))
+    return U, p.value
+
+
+def plaquette(U, L):
+    return float(load_oracle().orc_plaquette(dptr(np.ascontiguousarray(U, np.float64)), iarr(L)))
+
+
+def gen_clover(U, L, csw, kappa):
+    """Clover-leaf term of U as the packed inverse [V, 72] (fields_oracle.cc)."""
+    lib = load_oracle()
+    V = int(np.prod(L))
+    C = np.empty((V, 72), np.float64)
+    bad = lib.orc_gen_clover(dptr(C), dptr(np.ascontiguousarray(U, np.float64)), iarr(L),
+                             float(csw), float(kappa))
+    if bad:
+        raise ValueError(f"{bad} singular clover blocks")
+    return C
+
+
+def gen_source(L, seed=2, kind="gauss", arg=0):
+    """Sources [V, 24]: kind gauss | point (arg = 4*colour+spin) | z2 (fields_oracle.cc)."""
+    lib = load_oracle()
+    V = int(np.prod(L))
+    S = np.empty((V, 24), np.float64)
+    lib.orc_gen_source(dptr(S), iarr(L), int(seed), {"gauss": 0, "point": 1, "z2": 2}[kind],
+                       int(arg))
+    return S
 
 
 def gen_main_fields(Lloc, npe=(1, 1, 1, 1), nsrc=2):

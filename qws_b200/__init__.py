@@ -108,6 +108,11 @@ def load_library(path: str | os.PathLike | None = None):
         "qwsg_mtilde_s": [vp, vp, vp],
         "qwsg_bicgstab_vm": [vp, vp, vp, c_int, ip],
         "qwsg_prec_s_h": [vp, vp, vp, c_int, c_int],
+        "qwsg_ddd_in_h": [vp, vp, vp, c_int],
+        "qwsg_jinv_h": [vp, vp, vp, c_int, c_int],
+        "qwsg_ddd_out_h": [vp, vp, vp, c_int, c_double],
+        "qwsg_sap_update_s": [vp, vp, vp, vp, c_int],
+        "qwsg_sap_update_h": [vp, vp, vp, vp, c_int],
         "qwsg_bicgstab_precdd_s_h": [vp, vp, vp, c_double, c_int, c_int, c_int, ip,
                                      ctypes.POINTER(c_double)],
         "qwsg_bicgstab_dd_mix2_hf": [vp, vp, vp, c_double, c_int, c_double, c_int, c_int, c_int,
@@ -473,6 +478,30 @@ class Lattice:
         _check(self.lib.qwsg_prec_s_h(self.h, _ptr(out), _ptr(x), int(nsap), int(nm)))
         return out
 
+    def ddd_in_h(self, x, colour, out=None):
+        """D_blk on one colour with the FP16-storage kernel (FP32 in/out)."""
+        out = self._out(x, out)
+        _check(self.lib.qwsg_ddd_in_h(self.h, _ptr(out), _ptr(x), int(colour)))
+        return out
+
+    def jinv_h(self, b, colour, nm, out=None):
+        """nm Richardson steps on one colour with the FP16-storage kernel."""
+        out = self._out(b, out)
+        _check(self.lib.qwsg_jinv_h(self.h, _ptr(out), _ptr(b), int(colour), int(nm)))
+        return out
+
+    def ddd_out_h(self, x, colour, factor, out=None):
+        """out += factor A^-1 H_face x on one colour, FP16-storage kernel."""
+        out = self._out(x, out)
+        _check(self.lib.qwsg_ddd_out_h(self.h, _ptr(out), _ptr(x), int(colour), float(factor)))
+        return out
+
+    def sap_update(self, s, a, rhs, colour, half=False):
+        """s_c += rhs_c - D_blk a_c in place (FP32 kernel, or FP16 storage)."""
+        fn = self.lib.qwsg_sap_update_h if half else self.lib.qwsg_sap_update_s
+        _check(fn(self.h, _ptr(s), _ptr(a), _ptr(rhs), int(colour)))
+        return s
+
     def bicgstab_precdd_h(self, b, tol, maxiter, nsap=4, nm=2, out=None):
         out = self._out(b, out)
         it, rel = ctypes.c_int(), ctypes.c_double()
@@ -518,10 +547,10 @@ class Lattice:
 
     def kernel_stats(self):
         """{kernel name: (launches, total device ms, algorithmic bytes)} since enabling."""
-        n = ctypes.c_int(16)
-        L = (ctypes.c_long * 16)()
-        ms = (ctypes.c_double * 16)()
-        by = (ctypes.c_double * 16)()
+        n = ctypes.c_int(32)
+        L = (ctypes.c_long * 32)()
+        ms = (ctypes.c_double * 32)()
+        by = (ctypes.c_double * 32)()
         _check(self.lib.qwsg_kernel_stats(self.h, ctypes.byref(n), L, ms, by))
         return {self.lib.qwsg_kernel_name(k).decode(): (L[k], ms[k], by[k]) for k in range(n.value)
                 if L[k] > 0}

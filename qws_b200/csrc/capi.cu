@@ -610,6 +610,41 @@ int qwsg_prec_s_h(qwsg_lattice* l, float* out, const float* in, int nsap, int nm
     prec_s_h(*l->c, out, in, nsap, nm);
   });
 }
+int qwsg_ddd_in_h(qwsg_lattice* l, float* out, const float* in, int colour) {
+  return guarded([&] {
+    check_ctx(l);
+    need_fields(*l->c, false);
+    sap_kernel(*l->c, out, in, nullptr, 0, colour, 0, 0.0, true);
+  });
+}
+int qwsg_jinv_h(qwsg_lattice* l, float* x, const float* b, int colour, int nm) {
+  return guarded([&] {
+    check_ctx(l);
+    need_fields(*l->c, false);
+    sap_kernel(*l->c, x, b, nullptr, 1, colour, nm, 0.0, true);
+  });
+}
+int qwsg_ddd_out_h(qwsg_lattice* l, float* out, const float* in, int colour, double factor) {
+  return guarded([&] {
+    check_ctx(l);
+    need_fields(*l->c, false);
+    sap_kernel(*l->c, out, in, nullptr, 2, colour, 0, factor, true);
+  });
+}
+int qwsg_sap_update_s(qwsg_lattice* l, float* s, const float* a, const float* in, int colour) {
+  return guarded([&] {
+    check_ctx(l);
+    need_fields(*l->c, false);
+    sap_kernel(*l->c, s, a, in, 3, colour, 0, 0.0, false);
+  });
+}
+int qwsg_sap_update_h(qwsg_lattice* l, float* s, const float* a, const float* in, int colour) {
+  return guarded([&] {
+    check_ctx(l);
+    need_fields(*l->c, false);
+    sap_kernel(*l->c, s, a, in, 3, colour, 0, 0.0, true);
+  });
+}
 int qwsg_bicgstab_precdd_s_h(qwsg_lattice* l, float* x, const float* b, double tol, int maxiter,
                              int nsap, int nm, int* iters, double* final_rel) {
   return guarded([&] {

@@ -212,7 +212,8 @@ enum {
   K_JINV_F16 = 8,   // the same three in FP16 storage
   K_SAPE_F16 = 9,
   K_OUT_F16 = 10,
-  K_NKIND = 11
+  K_DIN_F16 = 11,   // block-interior D, FP16 storage
+  K_NKIND = 12
 };
 const char* kernel_kind_name(int k);
 // drain event records into per-kind totals (launches, ms, algorithmic bytes)
@@ -234,6 +235,14 @@ void prec_s(Ctx& c, float* out, const float* in, int nsap, int nm);
 // count (assign_mult_mSAP_s_h_, prec_ddd_s_h.h:63-231: nsap-1 sweeps + the
 // final stage); FP32 in and out
 void prec_s_h(Ctx& c, float* out, const float* in, int nsap, int nm);
+// single applications of the kernels the SAP is built from, for checking
+// each on its own: op 0 out_c = D_blk in_c ; op 1 out_c = J_c(in_c) (nm
+// Richardson steps) ; op 2 out += factor A^-1 H_face in on colour c's face
+// sites ; op 3 out_c += aux_c - D_blk in_c (the SAP update).  half: the
+// operands are stored in FP16 with per-site scales first (as the SAP stores
+// them) and the result converted back; else the FP32 kernels.
+void sap_kernel(Ctx& c, float* out, const float* in, const float* aux, int op, int col, int nm,
+                double factor, bool half);
 // flexible inner BiCGStab with the FP16 SAP (bicgstab_precdd_s_h.cc:83-369)
 int bicgstab_precdd_s_h(Ctx& c, float* x, const float* b, double tol, int maxiter, int nsap,
                         int nm, double* final_rel);

@@ -28,6 +28,16 @@
 // Nothing in it has to start at zero, because each call writes every scratch
 // site it later reads (the Richardson steps only read sites of the colour they
 // have just written).
+//
+// It takes handles made by qwsg_create only: a handle made by
+// qwsg_create_batch reads its parent's fields through a synchronisation
+// with the parent's stream and may carry a kappa per RHS, which this path
+// does not follow (it returns code 1 for such handles).  It reads the 12-real
+// links when an earlier FP32 call on the handle has found the links SU(3)
+// and made that copy (qwsg_jinv_s does so on its first call), otherwise the
+// full 18-real links; the two forms agree to a few FP32 roundoffs.  Its
+// launches count in the library's launch counter and in the handle's jinv
+// call count; per-kernel timing does not record them.
 #include <mutex>
 
 #include "../../include/qwsg.h"
@@ -71,6 +81,10 @@ extern "C" int qwsg_jinv_s_noalloc(qwsg_lattice* lat, float* x, const float* b, 
     return 4;
   }
   Ctx& c = *lat->c;
+  if (c.parent) {
+    set_error("qwsg_jinv_s_noalloc: not available on a handle made by qwsg_create_batch");
+    return 1;
+  }
   if (c.G.nr != 1) {
     set_error("qwsg_jinv_s_noalloc: not available on a multi-RHS handle");
     return 1;
@@ -109,6 +123,7 @@ extern "C" int qwsg_jinv_s_noalloc(qwsg_lattice* lat, float* x, const float* b, 
   HopArgs<float> a{};
   a.G = c.G;
   a.U = c.Us;
+  a.U12 = (c.links12_valid && c.links12_on) ? c.Us12 : nullptr;  // made earlier, if at all
   a.C = c.Cs;
   a.aux = b;
   a.coef = (float)c.kappa;
@@ -124,6 +139,7 @@ extern "C" int qwsg_jinv_s_noalloc(qwsg_lattice* lat, float* x, const float* b, 
     launch_hop<float>(HOP_INNER, EPI_JINV, a, c.st);
     src = dst;
   }
+  c.n_jinv++;
   e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_error(std::string("qwsg_jinv_s_noalloc: launch failed: ") + cudaGetErrorString(e));

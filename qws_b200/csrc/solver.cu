@@ -90,7 +90,7 @@ int kind_of(int sel, int epi) {
   if (sel == HOP_OUTER) return h ? K_OUT_F16 : d ? K_OUT_F64 : K_OUT_F32;
   if (epi == EPI_JINV) return h ? K_JINV_F16 : K_JINV_F32;
   if (epi == EPI_SAPE) return h ? K_SAPE_F16 : K_SAPE_F32;
-  return d ? K_DIN_F64 : K_DIN_F32;
+  return h ? K_DIN_F16 : d ? K_DIN_F64 : K_DIN_F32;
 }
 
 // sites of one colour that touch a block face
@@ -151,7 +151,7 @@ const char* kernel_kind_name(int k) {
   static const char* n[K_NKIND] = {"dslash_full_f64", "dslash_full_f32", "dslash_block_f64",
                                    "dslash_block_f32", "jinv_step_f32", "sap_update_f32",
                                    "dslash_face_f64", "dslash_face_f32", "jinv_step_f16",
-                                   "sap_update_f16", "dslash_face_f16"};
+                                   "sap_update_f16", "dslash_face_f16", "dslash_block_f16"};
   return (k >= 0 && k < K_NKIND) ? n[k] : "?";
 }
 
@@ -739,6 +739,54 @@ void prec_s_h(Ctx& c, float* out, const float* in, int nsap, int nm) {
     c.n_prec_s_h++;
   });
   c.check_launch("prec_s_h");
+}
+
+// One kernel of the SAP on its own (ctx.h).  The reference's counterparts:
+// ddd_in_s_/ddd_in_h_ (ddd_in_s.cc:376, ddd_in_h.h:54), jinv_ddd_in_s_/_h_
+// (static_solver.cc:141, jinv_ddd_in_h.h:53-118), ddd_out_pre+pos_s_/_h_
+// (ddd_out_s.cc:639,661, ddd_out_h.h:57,283) and the update loop of a SAP
+// half-sweep (qws.cc:815-818, prec_ddd_s_h.h:143-150).  The FP16 forms use
+// the SAP's own FP16 work planes, which no other call holds between calls.
+template <typename T>
+static void sap_kernel_t(Ctx& c, typename Store<T>::type* out, const typename Store<T>::type* in,
+                         const typename Store<T>::type* aux, int op, int col, int nm,
+                         double factor, typename Store<T>::type* tmp) {
+  using R = typename Arith<T>::R;
+  if (op == 1) {
+    jinv_t<T>(c, out, in, col, nm, tmp);
+    return;
+  }
+  if (op == 2) {
+    outer_t<T>(c, out, in, col, -1, factor, -1);
+    return;
+  }
+  auto a = hop_args_c<T>(c);
+  a.src = in;
+  a.aux = aux;
+  a.out = out;
+  a.coef = (R)(-c.kappa);
+  site_range(c, col, a.site0, a.nsites);
+  run_hop<T>(c, HOP_INNER, op == 0 ? EPI_D : EPI_SAPE, a);
+}
+
+void sap_kernel(Ctx& c, float* out, const float* in, const float* aux, int op, int col, int nm,
+                double factor, bool half) {
+  if (op < 0 || op > 3) throw Error(1, "sap_kernel: op must be 0..3");
+  if (col != 0 && col != 1) throw Error(1, "colour must be 0 or 1");
+  if (op == 3 && !aux) throw Error(1, "sap_kernel: the SAP update needs its right-hand side");
+  c.ensure_face_lists();
+  if (!half) {
+    c.ensure_sap();
+    sap_kernel_t<float>(c, out, in, aux, op, col, nm, factor, c.sap_t);
+  } else {
+    c.ensure_hp();
+    spinor_s2h(c.G, c.h_b, in, c.st);
+    spinor_s2h(c.G, c.h_s, out, c.st);
+    if (aux) spinor_s2h(c.G, c.h_a, aux, c.st);
+    sap_kernel_t<H16>(c, c.h_s, c.h_b, aux ? c.h_a : nullptr, op, col, nm, factor, c.h_t);
+    spinor_h2s(c.G, out, c.h_s, c.st);
+  }
+  c.check_launch("sap_kernel");
 }
 
 // bicgstab_precdd_s_ (bicgstab_precdd_s.cc:85-559).  Returns the number of

@@ -6,9 +6,10 @@ driver, README:68-80) with check.sh's extraction rule (`name : value` and
 arguments (local lattice, rank grid) next to the list of (name, value).
 
 Run in a container that has the reference checked out:
-    python tests/golden/make_golden.py /root/reference/data > tests/golden/case_norms.json
+    python tests/golden/make_golden.py $QWS_REFERENCE/data > tests/golden/case_norms.json
 """
 import json
+import os
 import re
 import sys
 from pathlib import Path
@@ -53,7 +54,8 @@ def extract_hp_history(text):
 
 
 def main():
-    data = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/data")
+    data = Path(sys.argv[1] if len(sys.argv) > 1 else
+                os.path.join(os.environ.get("QWS_REFERENCE", "/root/reference"), "data"))
     res = {}
     for name, (lloc, npe, opts) in CASES.items():
         text = (data / name).read_text()

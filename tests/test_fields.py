@@ -77,3 +77,27 @@ def test_sources():
     z = qws_b200.gen_source(L, seed=4, kind="z2")
     assert np.allclose(np.abs(z), 1 / np.sqrt(2))
     assert z.shape == (V, 24)
+
+
+@pytest.mark.parametrize("Lg,n_smear,csw,kappa", [
+    ((8, 4, 4, 8), 5, 1.7, 0.1365),
+    ((32, 6, 4, 3), 0, 1.0, 0.125),  # the plain CPU-runnable workload's fields
+    ((6, 6, 4, 4), 2, 1.7, 0.1355),
+])
+def test_oracle_generator_bit_equal(Lg, n_smear, csw, kappa):
+    """The reference arm builds its inputs with the oracle's restatement of
+    the generator (oracle/fields_oracle.cc) so that it never loads the
+    product library; both arms of a comparison must see identical arrays,
+    so the two generators agree bit for bit (links, clover, every source kind)."""
+    import qwsref
+
+    bits = lambda a: np.ascontiguousarray(a).view(np.uint64)
+    U, p = qws_b200.gen_gauge(Lg, seed=11, n_smear=n_smear, alpha=0.36)
+    Uo, po = qwsref.gen_gauge(Lg, seed=11, n_smear=n_smear, alpha=0.36)
+    np.testing.assert_array_equal(bits(U), bits(Uo))
+    assert abs(p - po) < 1e-13  # reduction order of the threads may differ
+    np.testing.assert_array_equal(bits(qws_b200.gen_clover(U, Lg, csw, kappa)),
+                                  bits(qwsref.gen_clover(Uo, Lg, csw, kappa)))
+    for kind, arg in (("gauss", 0), ("z2", 0), ("point", 7)):
+        np.testing.assert_array_equal(bits(qws_b200.gen_source(Lg, 12, kind, arg)),
+                                      bits(qwsref.gen_source(Lg, 12, kind, arg)))
