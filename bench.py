@@ -329,6 +329,10 @@ def bench_ours(args, w, name):
     if "NB" in tuned and tuple(tuned["NB"]) != tuple(w["NB"]):
         tl = qws_b200.Lattice(w["L"], tuned["NB"], tbc=w["tbc"], kappa=w["kappa"], stream=stream)
         tl.load_fields(U, C)
+    # the plain solver in the autotuner's configuration for it, on the same
+    # fields: the precision form's gain at equal footing (both tuned)
+    progress("plain solver, tuned")
+    plain_tuned = sub(bench_plain_tuned, args, w, U, C, b, stream, world)
     del U, C
     cfg = {k: tuned.get(k, w.get(k, d)) for k, d in
            (("nsap", 4), ("nm", 2), ("hop_threads", 128))}
@@ -447,6 +451,10 @@ def bench_ours(args, w, name):
             "value": world * args.steps / (hf_ms * 1e-3), "unit": "solves/s",
             "ms_per_step": hf_ms / args.steps,
             "speedup_vs_plain": ms_max / hf_ms,
+            "speedup_vs_plain_tuned": (plain_tuned["value"] and
+                                       (args.steps / (hf_ms * 1e-3)) / plain_tuned["value"])
+                                      if "value" in plain_tuned else None,
+            "plain_tuned": plain_tuned,
             "true_rel_resid": hf_true,
             "outer_iters": sum(s["outer_iters"] for s in hstats) / len(hstats),
             "inner_iters": sum(s["inner_iters"] for s in hstats) / len(hstats),
@@ -669,24 +677,68 @@ def bench_batched(args, w, lat, stream, world, cfg):
                       "all RHS, per-RHS scalars and convergence"}
 
 
+def rep_times(fn, reps, stream):
+    """Device time (ms) of each of `reps` calls of fn after one untimed call,
+    CUDA events on `stream`; returns (times, the last call's result)."""
+    import torch
+
+    fn()
+    torch.cuda.synchronize()
+    out, st = [], None
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out.append(e0.elapsed_time(e1))
+    return out, st
+
+
+def spread(ms, per=1):
+    """solves/s from the median of repeated timings, with min/median/max (ms)"""
+    med = statistics.median(ms)
+    return {"solves_per_s": per * 1e3 / med, "median_ms": round(med, 2),
+            "min_ms": round(min(ms), 2), "max_ms": round(max(ms), 2), "reps": len(ms)}
+
+
+def reference_samples_48():
+    """The reference's own 48^3x96 solutions on a fixed sample of sites
+    (tests/golden/make_ref_solutions.py), if the fixture is present."""
+    p = ROOT / "tests" / "golden" / "ref_solutions_48c96.npz"
+    if not p.exists():
+        return None
+    z = np.load(p)
+    meta = json.loads(str(z["meta"]))
+    return {"sites": z["sites"], "meta": meta,
+            "x": {float(k): z[f"x_{k}"] for k in meta}}
+
+
 def bench_precision_48(args, world):
-    """48^3x96, seeded SU(3) + 5 APE steps (generated on the GPU), csw 1.7,
-    kappa 0.1365 and 0.1355, Gaussian source, 1e-10.  Per kappa: the plain
-    solver (FP64 outer / FP32 SAP inner) on the reference's one-rank block
-    partition, and the precision form (FP16-storage SAP, FP64 outer with
-    reliable restarts) on one RHS at the reference partition and in the
-    autotuner's configuration, and on a --batch48-RHS handle (default 4) in
-    the autotuner's configuration.  Each result
-    has its true residual and its error against a reference solution of the
-    same system solved to 1e-13 (FP64 outer, plain solver).  The two block
+    """48^3x96 (the precision-form workload), seeded SU(3) + 5 APE steps
+    (generated on the GPU), csw 1.7, kappa 0.1365 and 0.1355, Gaussian
+    source, 1e-10.  Per kappa, each timed over `reps` solves (median, min,
+    max):
+      plain      the plain solver (FP64 outer / FP32 SAP inner) at the
+                 reference's one-rank partition, and in the autotuner's
+                 configuration for the plain solver;
+      precision  the precision form (FP16-storage SAP, FP64 outer with
+                 reliable restarts) at the reference partition, in its own
+                 tuned configuration on one RHS, and on a --batch48-RHS handle;
+    and the speed-ups at an equal partition and with both solvers tuned.
+    Every solution has its true residual and its error against a 1e-13 solve
+    of the same system, and the reference's own solution on a sample of
+    sites where tests/golden/ref_solutions_48c96.npz holds it.  The block
     grids run one after the other (their work buffers do not fit in HBM
-    together); the fields are generated from the same seeds on both."""
+    together); the fields are generated from the same seeds on each."""
     import torch
 
     import qws_b200
+    from qws_b200 import autotune
 
     L, NB = (48, 48, 48, 96), (2, 1, 1, 1)
     kappas = (0.1365, 0.1355)
+    reps = max(5, int(args.reps48))
     stream = torch.cuda.Stream()
     b = qws_b200.gen_source(L, 12, "gauss")
     nrb = max(1, int(args.batch48))
@@ -694,123 +746,155 @@ def bench_precision_48(args, world):
     tuned = tuned_config(args, L, 0)
     cfg = {k: tuned.get(k, d) for k, d in (("nsap", 4), ("nm", 2), ("hop_threads", 128))}
     NBt = tuple(tuned.get("NB", NB))
-    out = {"lattice": "48x48x48x96", "tol": 1e-10, "reference_partition": list(NB),
-           "tuned": {"block_grid": list(NBt), **cfg, "tuning": tuned}, "per_kappa": []}
+    ptuned = autotune.lookup(L, "plain", 1) or {}
+    pcfg = {k: ptuned.get(k, d) for k, d in (("nsap", 4), ("nm", 2), ("hop_threads", 128))}
+    NBp = tuple(ptuned.get("NB", NB))
+    ref = reference_samples_48()
+    out = {"lattice": "48x48x48x96", "tol": 1e-10, "reps": reps,
+           "reference_partition": list(NB),
+           "precision_tuned": {"block_grid": list(NBt), **cfg, "tuning": tuned},
+           "plain_tuned": {"block_grid": list(NBp), **pcfg,
+                           "tuning": ptuned or "no cached plain tuning: reference partition"},
+           "fields": "gauge generated and clover built on the GPU (equal to the host "
+                     "generator's to rounding); the reference solved the host generator's",
+           "per_kappa": []}
+    per = {k: {"kappa": k} for k in kappas}
+    xref = {}
 
-    def timed(fn, reps):
-        fn()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(reps):
-            st = fn()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / reps, st
+    def errors(lat, x, kappa):
+        xh = lat.to_host(x)
+        e = {"rel_error_vs_fp64_solve": float(np.linalg.norm(xh - xref[kappa]) /
+                                                np.linalg.norm(xref[kappa]))}
+        if ref is not None and kappa in ref["x"]:
+            xs, rs = xh[ref["sites"]], ref["x"][kappa]
+            e["rel_error_vs_reference_sample"] = float(np.linalg.norm(xs - rs) / np.linalg.norm(rs))
+        return e
 
-    def rel_err(xh, xr):
-        return float(np.linalg.norm(xh - xr) / np.linalg.norm(xr))
-
-    def single_run(lat, nsap, nm, xr):
-        """the precision form on one RHS; error against xr"""
+    def plain_run(lat, nsap, nm, kappa):
         with torch.cuda.stream(stream):
-            bd = lat.to_device(b)
-            x = lat.empty("f64")
+            bd, x = lat.to_device(b), lat.empty("f64")
 
-            def prec():
+            def solve():
                 x.zero_()
-                return lat.bicgstab_dd_mix2_hf(x, bd, 1e-10, 200, 1e-6, 50, nsap, nm, reliable=5)
+                return lat.bicgstab_dd_mix(x, bd, 1e-10, 200, 1e-6, 50, nsap, nm)
 
-            ms_h, st_h = timed(prec, 2)
-            res = {"ms": ms_h, "true_rel_resid": lat.true_residual(x, bd),
-                   "rel_error_vs_reference": rel_err(lat.to_host(x), xr),
-                   "outer_iters": st_h["outer_iters"], "inner_iters": st_h["inner_iters"]}
+            ms, st = rep_times(solve, reps, stream)
+            res = dict(spread(ms), true_rel_resid=lat.true_residual(x, bd),
+                       outer_iters=st["outer_iters"], inner_iters=st["inner_iters"],
+                       **errors(lat, x, kappa))
             del x, bd
             torch.cuda.empty_cache()
         return res
 
-    def batched_run(lat, nsap, nm, xr, nr):
-        """the precision form on an nr-RHS handle (RHS 0 = the single source)"""
-        B = lat.batch(nr, stream=stream)
+    def precision_run(lat, nsap, nm, kappa):
+        with torch.cuda.stream(stream):
+            bd, x = lat.to_device(b), lat.empty("f64")
+
+            def solve():
+                x.zero_()
+                return lat.bicgstab_dd_mix2_hf(x, bd, 1e-10, 200, 1e-6, 50, nsap, nm, reliable=5)
+
+            ms, st = rep_times(solve, reps, stream)
+            res = dict(spread(ms), true_rel_resid=lat.true_residual(x, bd),
+                       outer_iters=st["outer_iters"], inner_iters=st["inner_iters"],
+                       **errors(lat, x, kappa))
+            del x, bd
+            torch.cuda.empty_cache()
+        return res
+
+    def batched_run(lat, nsap, nm, kappa):
+        B = lat.batch(nrb, stream=stream)
         try:
             with torch.cuda.stream(stream):
-                bb = B.to_device(bn[:nr])
-                xb = B.empty("f64")
+                bb, xb = B.to_device(bn[:nrb]), B.empty("f64")
 
-                def batched():
+                def solve():
                     xb.zero_()
                     return B.bicgstab_dd_mix2_hf(xb, bb, 1e-10, 200, 1e-6, 50, nsap, nm,
                                                  reliable=5)
 
-                ms_b, _ = timed(batched, 2)
-                res = {"ms": ms_b, "nrhs": nr, "max_true_rel_resid": max(B.true_residual(xb, bb)),
-                       "rel_error_vs_reference": rel_err(B.to_host(xb)[0], xr)}
+                ms, _ = rep_times(solve, reps, stream)
+                xh = B.to_host(xb)[0]
+                res = dict(spread(ms, nrb), nrhs=nrb,
+                           max_true_rel_resid=max(B.true_residual(xb, bb)),
+                           rel_error_vs_fp64_solve=float(np.linalg.norm(xh - xref[kappa]) /
+                                                         np.linalg.norm(xref[kappa])))
                 del xb, bb
         finally:
             B.close()
             torch.cuda.empty_cache()
         return res
 
-    # ---- reference partition: the reference solution, plain, precision form
-    per = {k: {"kappa": k} for k in kappas}
-    xref = {}
-    lat = qws_b200.Lattice(L, NB, tbc=-1, kappa=kappas[0], stream=stream)
+    def lattice(NBx, threads):
+        lat = qws_b200.Lattice(L, NBx, tbc=-1, kappa=kappas[0], stream=stream)
+        plaq = lat.gen_gauge_device(11, 5, 0.36)
+        lat.set_hop_threads(threads)
+        return lat, plaq
+
+    # ---- reference partition: the 1e-13 solution, plain, precision form -----
+    lat, out["plaquette"] = lattice(NB, 128)
     try:
-        out["plaquette"] = lat.gen_gauge_device(11, 5, 0.36)
         for kappa in kappas:
             lat.set_kappa(kappa)
             lat.build_clover(1.7)
             with torch.cuda.stream(stream):
-                bd = lat.to_device(b)
-                x = lat.empty("f64")
+                bd, x = lat.to_device(b), lat.empty("f64")
                 lat.bicgstab_dd_mix(x, bd, 1e-13, 200, 1e-6, 50)
                 xref[kappa] = lat.to_host(x)
-
-                def plain():
-                    x.zero_()
-                    return lat.bicgstab_dd_mix(x, bd, 1e-10, 200, 1e-6, 50)
-
-                ms_p, st_p = timed(plain, 2)
-                per[kappa]["plain"] = {
-                    "solves_per_s": 1e3 / ms_p, "true_rel_resid": lat.true_residual(x, bd),
-                    "rel_error_vs_reference": rel_err(lat.to_host(x), xref[kappa]),
-                    "outer_iters": st_p["outer_iters"], "inner_iters": st_p["inner_iters"]}
                 del x, bd
-                torch.cuda.empty_cache()
-            single = single_run(lat, 4, 2, xref[kappa])
-            per[kappa]["precision_reference_partition"] = {
-                "single": dict(single, solves_per_s=1e3 / single.pop("ms"))}
+            per[kappa]["plain_reference_partition"] = plain_run(lat, 4, 2, kappa)
+            per[kappa]["precision_reference_partition"] = precision_run(lat, 4, 2, kappa)
     finally:
         lat.close()
         torch.cuda.empty_cache()
-
-    # ---- tuned configuration: the precision form ------------------------------
-    lat = qws_b200.Lattice(L, NBt, tbc=-1, kappa=kappas[0], stream=stream)
+    # ---- the plain solver in its tuned configuration ------------------------
+    if (NBp, pcfg["nsap"], pcfg["nm"], pcfg["hop_threads"]) != (NB, 4, 2, 128):
+        lat, _ = lattice(NBp, pcfg["hop_threads"])
+        try:
+            for kappa in kappas:
+                lat.set_kappa(kappa)
+                lat.build_clover(1.7)
+                per[kappa]["plain_tuned"] = plain_run(lat, pcfg["nsap"], pcfg["nm"], kappa)
+        finally:
+            lat.close()
+            torch.cuda.empty_cache()
+    else:
+        for kappa in kappas:
+            per[kappa]["plain_tuned"] = per[kappa]["plain_reference_partition"]
+    # ---- the precision form in its tuned configuration ----------------------
+    lat, _ = lattice(NBt, cfg["hop_threads"])
     try:
-        lat.gen_gauge_device(11, 5, 0.36)
-        lat.set_hop_threads(cfg["hop_threads"])
         # the multi-RHS runs first: the lattice's own single-RHS work buffers
-        # (allocated by the single solve, kept until the lattice closes) and
-        # an nr-RHS handle's do not fit in HBM together at 48^3x96
+        # (kept until the lattice closes) and an nr-RHS handle's do not fit
+        # in HBM together at 48^3x96
         for kappa in kappas:
             lat.set_kappa(kappa)
             lat.build_clover(1.7)
-            plain_sps = per[kappa]["plain"]["solves_per_s"]
-            pair = batched_run(lat, cfg["nsap"], cfg["nm"], xref[kappa], nrb)
-            p_sps = nrb * 1e3 / pair.pop("ms")
-            per[kappa]["precision_batched"] = dict(pair, solves_per_s=p_sps,
-                                                   speedup_vs_plain=p_sps / plain_sps)
+            per[kappa]["precision_tuned_batched"] = batched_run(lat, cfg["nsap"], cfg["nm"], kappa)
         for kappa in kappas:
             lat.set_kappa(kappa)
             lat.build_clover(1.7)
-            plain_sps = per[kappa]["plain"]["solves_per_s"]
-            single = single_run(lat, cfg["nsap"], cfg["nm"], xref[kappa])
-            s_sps = 1e3 / single.pop("ms")
-            per[kappa]["precision_single"] = dict(single, solves_per_s=s_sps,
-                                                  speedup_vs_plain=s_sps / plain_sps)
+            per[kappa]["precision_tuned"] = precision_run(lat, cfg["nsap"], cfg["nm"], kappa)
     finally:
         lat.close()
         torch.cuda.empty_cache()
+    for kappa in kappas:
+        p = per[kappa]
+        sps = lambda k: p[k]["solves_per_s"]
+        p["speedups"] = {
+            "precision_vs_plain_same_partition":
+                sps("precision_reference_partition") / sps("plain_reference_partition"),
+            "precision_tuned_vs_plain_tuned": sps("precision_tuned") / sps("plain_tuned"),
+            "batched_tuned_vs_plain_tuned": sps("precision_tuned_batched") / sps("plain_tuned"),
+            "precision_tuned_vs_plain_reference_partition":
+                sps("precision_tuned") / sps("plain_reference_partition"),
+        }
+        if ref is not None and f"{kappa:.4f}" in ref["meta"]:
+            m = ref["meta"][f"{kappa:.4f}"]
+            p["reference_solve"] = {"outer_iters": m["outer_iters"],
+                                    "inner_iters": m["inner_iters_per_solve"],
+                                    "true_rel_resid": m["true_rel_resid"],
+                                    "variant": m["variant"], "sample_sites": len(ref["sites"])}
     out["per_kappa"] = [per[k] for k in kappas]
     return out
 
@@ -842,7 +926,7 @@ def bench_uneven(args):
                 reqs = [svc.submit(serve.Request(L=L, gauge=i, kappa=0.1365, csw=1.7, tol=1e-10,
                                                  source=src[L])) for i, L in enumerate(picks)]
                 for q in reqs:
-                    q.done.wait()
+                    q.wait(600)
                 t1 = time.monotonic()
                 st = serve.summarize(reqs, t0, t1)
                 return st, t1 - t0
@@ -885,12 +969,12 @@ def bench_serving(args):
                                          source=qws_b200.gen_source(L, 4000 + gid, "gauss")))
                 for L in vols for gid in range(args.serve_gauges)]
         for q in warm:
-            q.done.wait()
+            q.wait(600)
         warmup_s = time.monotonic() - t0
         reqs = serve.poisson_workload(svc, args.serve_rate, args.serve_window, vols,
                                       [0.4, 0.3, 0.2, 0.1], args.serve_gauges, seed=1)
         for q in reqs:
-            q.done.wait()
+            q.wait(600)
         out = serve.summarize(reqs)
     finally:
         svc.close()
@@ -901,6 +985,52 @@ def bench_serving(args):
                 "gauges_per_volume": args.serve_gauges, "workers": 3, "budget_gb": 150,
                 "solver": "bicgstab_dd_mix2_hf (reliable 5), clover built on the GPU per kappa"})
     return out
+
+
+def bench_plain_tuned(args, w, U, C, b, stream, world):
+    """The plain solver (bicgstab_dd_mix) in the autotuner's configuration
+    for it (block grid, sweep counts, CTA size; qws_b200/tuning.json), on the
+    workload's fields and source: `steps` timed solves after `warmup`."""
+    import torch
+
+    import qws_b200
+    from qws_b200 import autotune
+
+    t = autotune.lookup(w["L"], "plain", 1)
+    if not t:
+        return {"value": None, "note": "no cached plain tuning for this lattice"}
+    lat = qws_b200.Lattice(w["L"], t["NB"], tbc=w["tbc"], kappa=w["kappa"], stream=stream)
+    try:
+        lat.load_fields(U, C)
+        lat.set_hop_threads(t["hop_threads"])
+        with torch.cuda.stream(stream):
+            bd, x = lat.to_device(b), lat.empty("f64")
+
+            def solve():
+                x.zero_()
+                return lat.bicgstab_dd_mix(x, bd, w["tol"], w["maxiter"], w["tol_s"],
+                                           w["maxiter_s"], t["nsap"], t["nm"])
+
+            for _ in range(max(1, args.warmup)):
+                solve()
+            torch.cuda.synchronize()
+            barrier(world)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                st = solve()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = allreduce_max(e0.elapsed_time(e1), world)
+            true = lat.true_residual(x, bd)
+    finally:
+        lat.close()
+        torch.cuda.empty_cache()
+    return {"value": world * args.steps / (ms * 1e-3), "unit": "solves/s",
+            "config": {"block_grid": t["NB"], "nsap": t["nsap"], "nm": t["nm"],
+                       "hop_threads": t["hop_threads"]},
+            "true_rel_resid": true, "outer_iters": st["outer_iters"],
+            "inner_iters": st["inner_iters"]}
 
 
 def cpu_baseline(w, x_gpu, digests, gpu_solve):
@@ -977,6 +1107,8 @@ def main():
                     help="workers of the 48 uneven-volume solves sub-result (0: skip)")
     ap.add_argument("--batch48", type=int, default=4,
                     help="right-hand sides of the 48^3x96 multi-RHS precision-form run")
+    ap.add_argument("--reps48", type=int, default=5,
+                    help="timed solves per 48^3x96 measurement (at least 5)")
     ap.add_argument("--tune", default="cache", choices=["cache", "retune", "off"],
                     help="precision-form configuration: the autotuner's cached choice "
                          "(tuning on a miss), a fresh tuning run, or the reference partition")

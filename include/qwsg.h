@@ -72,6 +72,12 @@ int qwsg_create_batch(qwsg_lattice** out, qwsg_lattice* parent, int nrhs);
  * every operator and solver on the handle then applies kappas[r] and its
  * clover to RHS r.  Call again to change the kappas. */
 int qwsg_batch_set_kappas(qwsg_lattice* batch, const double* kappas, double csw);
+/* a stopping tolerance for every RHS of a multi-RHS handle (no counterpart in
+ * the reference, whose solvers take one tol): the FP64 outer solvers
+ * (qwsg_bicgstab_dd_mix, qwsg_bicgstab_dd_mix2_hf) stop RHS r at tols[r]
+ * (and restart it from its true residual until that is below tols[r]) in
+ * place of their tol argument.  NULL restores the tol argument for all RHS. */
+int qwsg_batch_set_tols(qwsg_lattice* batch, const double* tols);
 int qwsg_nrhs(const qwsg_lattice* lat, int* nrhs);
 /* per-RHS results of the last multi-RHS solve: stats of the DD solvers,
  * iteration counts of the inner solvers (either pointer may be NULL) */
@@ -146,6 +152,13 @@ int qwsg_bicgstab_precdd_s(qwsg_lattice* lat, float* x, const float* b, double t
  * x holds the initial guess on entry.  stats may be NULL. */
 int qwsg_bicgstab_dd_mix(qwsg_lattice* lat, double* x, const double* b, double tol, int maxiter,
                          double tol_s, int maxiter_s, int nsap, int nm, qwsg_solve_stats* stats);
+/* Fault injection on the host, for tests (no counterpart in the reference):
+ * from now on the single-RHS FP64 outer loop of this handle
+ * (qwsg_bicgstab_dd_mix, qwsg_bicgstab_dd_mix2_hf) takes the reduction
+ * <r0, q> as exactly zero at outer iteration outer_iter, so the reference's
+ * breakdown guard (alpha = 0 when |<r0, q>| == 0, bicgstab_dd_mix.cc:192)
+ * decides that step.  0 turns it off.  Nothing on the GPU is disturbed. */
+int qwsg_inject_breakdown(qwsg_lattice* lat, int outer_iter);
 /* |b - D x| / |b| in FP64 (one value per RHS on a multi-RHS handle) */
 int qwsg_true_residual(qwsg_lattice* lat, const double* x, const double* b, double* rel);
 

@@ -688,6 +688,12 @@ int approx_inv(orc_lat* l, double* x, const double* b, double tol_s, int maxiter
 
 extern "C" {
 
+// A breakdown planted for tests: at outer iteration g_breakdown_at (0: never)
+// the outer loop takes <r0, q> as exactly zero, so the reference's guard
+// (alpha = 0 when |<r0, q>| == 0, bicgstab_dd_mix.cc:192) decides the step.
+static int g_breakdown_at = 0;
+void orc_plant_breakdown(int outer_iter) { g_breakdown_at = outer_iter; }
+
 // bicgstab_dd_mix_ (bicgstab_dd_mix.cc:105-388): flexible BiCGStab in FP64
 // with the single-precision SAP-preconditioned solve as variable
 // preconditioner; iter runs 1..maxiter-1.
@@ -712,6 +718,7 @@ void orc_bicgstab_dd_mix(orc_lat* l, double* x, const double* b, double tol, int
     inner += approx_inv(l, u.data(), p.data(), tol_s, maxiter_s, nsap, nm);
     orc_ddd_d(l, q.data(), u.data());
     ctmp = cdot(r0.data(), q.data(), n);
+    if (iter == g_breakdown_at) ctmp = 0;
     alpha = rho0 / ctmp;
     if (std::abs(ctmp) == 0) alpha = 0;
     double ar = alpha.real(), ai = alpha.imag();

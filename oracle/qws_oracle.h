@@ -82,6 +82,11 @@ void orc_bicgstab_dd_mix(orc_lat*, double* x, const double* b, double tol,
                          int maxiter, double tol_s, int maxiter_s, int nsap,
                          int nm, double* stats, double* hist);
 
+/* test hook: the outer loop of orc_bicgstab_dd_mix takes <r0, q> as zero at
+ * outer iteration `outer_iter` (0: never), exercising the reference's
+ * breakdown guard (bicgstab_dd_mix.cc:192) */
+void orc_plant_breakdown(int outer_iter);
+
 /* ---- half-precision solver pair, restated in FP32 ----------------------- */
 /* assign_mult_mSAP_s_h_ (prec_ddd_s_h.h:63-231) is prec_s_ with nsap-1 sweeps;
  * the flexible inner solver (bicgstab_precdd_s_h.cc:83-369) with that M and the

@@ -118,6 +118,7 @@ def load_oracle():
     lib.orc_gen_clover.restype = ctypes.c_int
     lib.orc_gen_clover.argtypes = [_dp, _dp, _ip, ctypes.c_double, ctypes.c_double]
     lib.orc_gen_source.argtypes = [_dp, _ip, ctypes.c_ulonglong, ctypes.c_int, ctypes.c_int]
+    lib.orc_plant_breakdown.argtypes = [ctypes.c_int]
     lib.orc_norm2_d.restype = ctypes.c_double
     lib.orc_norm2_d.argtypes = [_dp, ctypes.c_long]
     lib.orc_norm2_s.restype = ctypes.c_double

@@ -59,6 +59,8 @@ def load_library(path: str | os.PathLike | None = None):
         "qwsg_create_batch": [ctypes.POINTER(vp), vp, c_int],
         "qwsg_nrhs": [vp, ip],
         "qwsg_batch_set_kappas": [vp, vp, c_double],
+        "qwsg_batch_set_tols": [vp, vp],
+        "qwsg_inject_breakdown": [vp, c_int],
         "qwsg_batch_stats": [vp, ctypes.POINTER(SolveStats), ip],
         "qwsg_build_clover": [vp, c_double],
         "qwsg_set_graphs": [vp, c_int],
@@ -525,6 +527,11 @@ class Lattice:
         _check(self.lib.qwsg_true_residual(self.h, _ptr(x), _ptr(b), r))
         return r[0] if self.nr == 1 else list(r)
 
+    def inject_breakdown(self, outer_iter):
+        """Test hook (host side): the outer loop takes <r0, q> as zero at
+        outer iteration outer_iter (0: off); qwsg_inject_breakdown."""
+        _check(self.lib.qwsg_inject_breakdown(self.h, int(outer_iter)))
+
     def set_graphs(self, enable=True):
         _check(self.lib.qwsg_set_graphs(self.h, 1 if enable else 0))
 
@@ -589,6 +596,18 @@ class BatchLattice(Lattice):
         assert k.size == self.nr
         _check(self.lib.qwsg_batch_set_kappas(self.h, ctypes.c_void_p(k.ctypes.data), float(csw)))
         self.kappas = k.copy()
+
+    def set_tols(self, tols):
+        """A stopping tolerance per RHS for the FP64 outer solvers
+        (qwsg_batch_set_tols); None: the solver's tol argument for all."""
+        if tols is None:
+            _check(self.lib.qwsg_batch_set_tols(self.h, None))
+            self.tols = None
+            return
+        t = np.ascontiguousarray(tols, np.float64)
+        assert t.size == self.nr
+        _check(self.lib.qwsg_batch_set_tols(self.h, ctypes.c_void_p(t.ctypes.data)))
+        self.tols = t.copy()
 
     def load_fields(self, *a, **k):
         raise QwsgError("fields belong to the parent lattice")

@@ -243,6 +243,28 @@ int qwsg_batch_set_kappas(qwsg_lattice* l, const double* kappas, double csw) {
   });
 }
 
+int qwsg_batch_set_tols(qwsg_lattice* l, const double* tols) {
+  return guarded([&] {
+    check_ctx(l);
+    Ctx& c = *l->c;
+    if (!tols) {
+      c.rhs_tols.clear();
+      return;
+    }
+    for (int r = 0; r < c.G.nr; r++)
+      if (!std::isfinite(tols[r])) throw Error(1, "qwsg_batch_set_tols: tolerance must be finite");
+    c.rhs_tols.assign(tols, tols + c.G.nr);
+  });
+}
+
+int qwsg_inject_breakdown(qwsg_lattice* l, int outer_iter) {
+  return guarded([&] {
+    check_ctx(l);
+    if (outer_iter < 0) throw Error(1, "qwsg_inject_breakdown: outer_iter must be >= 0");
+    l->c->breakdown_at = outer_iter;
+  });
+}
+
 int qwsg_nrhs(const qwsg_lattice* l, int* nrhs) {
   return guarded([&] {
     if (!l || !l->c) throw Error(4, "lattice handle is NULL");

@@ -14,6 +14,8 @@
 // Gauss-Jordan inversion with partial pivoting, as on the host.
 #include <cmath>
 
+#include <type_traits>
+
 #include "ctx.h"
 
 namespace qwsg {
@@ -277,18 +279,20 @@ void set_rhs_kappas(Ctx& c, const double* kappas, double csw) {
     QWSG_CUDA(cudaStreamSynchronize(c.st));
     c.clear_graphs();
   }
-  if (!c.Cdr) {
-    QWSG_CUDA(cudaMalloc(&c.Cdr, sizeof(double) * n));
-    QWSG_CUDA(cudaMalloc(&c.Csr, sizeof(float) * n));
-    QWSG_CUDA(cudaMalloc(&c.Chr, sizeof(__half) * n));
-    QWSG_CUDA(cudaMalloc(&c.kap_d, sizeof(double) * Ctx::kMaxRhs));
-    QWSG_CUDA(cudaMalloc(&c.kap_s, sizeof(float) * Ctx::kMaxRhs));
-    c.owned.push_back(c.Cdr);
-    c.owned.push_back(c.Csr);
-    c.owned.push_back(c.Chr);
-    c.owned.push_back(c.kap_d);
-    c.owned.push_back(c.kap_s);
-  }
+  // each plane set on its own: one that failed to allocate is retried by the
+  // next call, and no launch below runs before all of them exist
+  auto want = [&](auto** p, size_t bytes) {
+    if (*p) return;
+    void* q = nullptr;
+    QWSG_CUDA(cudaMalloc(&q, bytes));
+    c.owned.push_back(q);
+    *p = static_cast<std::remove_reference_t<decltype(**p)>*>(q);
+  };
+  want(&c.Cdr, sizeof(double) * n);
+  want(&c.Csr, sizeof(float) * n);
+  want(&c.Chr, sizeof(__half) * n);
+  want(&c.kap_d, sizeof(double) * Ctx::kMaxRhs);
+  want(&c.kap_s, sizeof(float) * Ctx::kMaxRhs);
   for (int r = 0; r < c.G.nr; r++)
     build_into(c, c.Ud, c.Cdr, c.Csr, csw * kappas[r], c.G.lgnr, r, spad(c.G));
   clover_s2h_entries(c.G, c.Chr, c.Csr, c.st);

@@ -141,6 +141,12 @@ struct Ctx {
   // per-RHS kappa on a multi-RHS handle (set_rhs_kappas): clover planes per
   // (site, RHS) entry in FP64/FP32/FP16 and the kappas; empty: the parent's
   std::vector<double> rhs_kappas;
+  // per-RHS stopping tolerance of the FP64 outer solvers (qwsg_batch_set_tols);
+  // empty: the tolerance argument of the call for every RHS
+  std::vector<double> rhs_tols;
+  // fault injection on the host (qwsg_inject_breakdown): the FP64 outer loop
+  // takes <r0, q> as zero at this outer iteration (0: never)
+  int breakdown_at = 0;
   double* Cdr = nullptr;
   float* Csr = nullptr;
   __half* Chr = nullptr;

@@ -167,16 +167,20 @@ void down(Ctx& c, void* host, const R* planes, int dom, int vlen) {
 void sync_eo(Ctx& c) {
   sync_fields(c);
   const size_t n = (size_t)72 * c.G.pad;
-  if (!g.eUd) {
-    QWSG_CUDA(cudaMalloc(&g.eUd, sizeof(double) * n));
-    QWSG_CUDA(cudaMalloc(&g.eCd, sizeof(double) * n));
-    QWSG_CUDA(cudaMalloc(&g.eUs, sizeof(float) * n));
-    QWSG_CUDA(cudaMalloc(&g.eCs, sizeof(float) * n));
-    for (int i = 0; i < 4; i++) {
-      g.ed[i] = c.alloc_spinor<double>();
-      g.es[i] = c.alloc_spinor<float>();
+  // every buffer on its own (a failed allocation is retried by the next call)
+  for (double** p : {&g.eUd, &g.eCd})
+    if (!*p) {
+      QWSG_CUDA(cudaMalloc(p, sizeof(double) * n));
+      g.eo_dirty = true;
     }
-    g.eo_dirty = true;
+  for (float** p : {&g.eUs, &g.eCs})
+    if (!*p) {
+      QWSG_CUDA(cudaMalloc(p, sizeof(float) * n));
+      g.eo_dirty = true;
+    }
+  for (int i = 0; i < 4; i++) {
+    if (!g.ed[i]) g.ed[i] = c.alloc_spinor<double>();
+    if (!g.es[i]) g.es[i] = c.alloc_spinor<float>();
   }
   if (g.eo_dirty || g.always_upload) {
     const size_t V = (size_t)c.G.V;

@@ -118,7 +118,7 @@ __device__ __forceinline__ void do_hop(const HopArgs<T>& a, const Site& s, int g
   }
   int gn;
   if (!face) {
-    gn = g + DIR * a.G.str[MU];
+    gn = g + rot_step(a.G, MU, s.lc[MU], DIR);
   } else {
     int ncol;
     gn = nbr_across(a.G, s, MU, DIR, &ncol);

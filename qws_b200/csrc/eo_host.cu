@@ -17,10 +17,11 @@ namespace qwsg {
 }
 
 void Ctx::ensure_eo() {
-  if (!eo_d[0]) {
-    for (int i = 0; i < 6; i++) eo_d[i] = alloc_spinor<double>();
-    for (int i = 0; i < 2; i++) eo_s[i] = alloc_spinor<float>();
-  }
+  // each buffer on its own (a failed allocation is retried by the next call)
+  for (int i = 0; i < 6; i++)
+    if (!eo_d[i]) eo_d[i] = alloc_spinor<double>();
+  for (int i = 0; i < 2; i++)
+    if (!eo_s[i]) eo_s[i] = alloc_spinor<float>();
 }
 
 template <typename R>

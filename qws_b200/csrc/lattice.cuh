@@ -64,6 +64,7 @@ struct Geom {
   int tbc;     // +1 periodic / -1 antiperiodic in t (fbc_f[3], qws.cc:298-310)
   int pad;     // plane stride in elements
   int str[4];  // in-block strides of x, y, z, t (block_local)
+  int rot;     // the fastest in-block direction (str 1), stored rotated by one
   // right-hand sides per spinor field (a power of two, 1..32).  Spinor
   // fields interleave them RHS-minor: RHS r of site g is entry
   // (g << lgnr) + r of planes with stride pad << lgnr, so the threads of one
@@ -96,11 +97,34 @@ struct Site {
 // nearest they can be and stay in L2 between the launches' reads; the
 // second largest is fastest, so every block face but that direction's is a
 // run of whole rows and the face kernels read whole sectors.
+//
+// Along the fastest direction a row is stored rotated by one -- in-block
+// coordinates B-1, 0, 1, ..., B-2 -- so that the row's two face sites (0 and
+// B-1) are adjacent: the face kernels, which visit only face sites, then read
+// them as one 32-byte sector instead of two sectors that each hold one site.
+// Interior hops along that direction keep stride 1 except the step between
+// B-2 and B-1 (see rot_step).
+__host__ __device__ __forceinline__ int rot_pos(const Geom& G, int mu, int l) {
+  return mu == G.rot ? (l + 1 == G.B[mu] ? 0 : l + 1) : l;
+}
+__host__ __device__ __forceinline__ int rot_coord(const Geom& G, int mu, int p) {
+  return mu == G.rot ? (p == 0 ? G.B[mu] - 1 : p - 1) : p;
+}
 __host__ __device__ __forceinline__ int block_local(const Geom& G, const int lc[4]) {
-  return lc[0] * G.str[0] + lc[1] * G.str[1] + lc[2] * G.str[2] + lc[3] * G.str[3];
+  return rot_pos(G, 0, lc[0]) * G.str[0] + rot_pos(G, 1, lc[1]) * G.str[1] +
+         rot_pos(G, 2, lc[2]) * G.str[2] + rot_pos(G, 3, lc[3]) * G.str[3];
+}
+// offset of the interior hop from in-block coordinate l to l + dir along mu
+__host__ __device__ __forceinline__ int rot_step(const Geom& G, int mu, int l, int dir) {
+  int d = dir * G.str[mu];
+  if (mu == G.rot) {
+    if (dir > 0 && l == G.B[mu] - 2) d -= G.B[mu];  // B-2 -> B-1: back to the row's start
+    if (dir < 0 && l == G.B[mu] - 1) d += G.B[mu];  // B-1 -> B-2: to the row's end
+  }
+  return d;
 }
 
-__device__ __forceinline__ void decode_site(const Geom& G, int g, Site& s) {
+__host__ __device__ __forceinline__ void decode_site(const Geom& G, int g, Site& s) {
   s.col = g >= G.Vh;
   int rem = g - s.col * G.Vh;
   int k = fdiv(rem, G.fVb);
@@ -108,7 +132,7 @@ __device__ __forceinline__ void decode_site(const Geom& G, int g, Site& s) {
 #pragma unroll
   for (int mu = 0; mu < 4; mu++) {
     const int q = fdiv(t, G.fstr[mu]);
-    s.lc[mu] = q - fdiv(q, G.fB[mu]) * G.B[mu];
+    s.lc[mu] = rot_coord(G, mu, q - fdiv(q, G.fB[mu]) * G.B[mu]);
   }
   int q = fdiv(k, G.fnbh0);
   int r = k - q * G.nbh0;

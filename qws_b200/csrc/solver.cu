@@ -7,6 +7,7 @@
 // lattice.  The SAP sweep is written once for every storage format (FP32,
 // FP16 with per-site scales).
 #include <algorithm>
+#include <initializer_list>
 #include <cmath>
 #include <cstring>
 
@@ -233,6 +234,7 @@ Ctx::Ctx(const int L[4], const int NB[4], int tbc, int nrhs) {
       G.str[order[k]] = stride;
       stride *= G.B[order[k]];
     }
+    G.rot = order[0];
   }
   for (int mu = 0; mu < 4; mu++) G.fstr[mu] = make_fastdiv(G.str[mu]);
   for (int mu = 0; mu < 4; mu++) G.fB[mu] = make_fastdiv(G.B[mu]);
@@ -316,64 +318,45 @@ __half* Ctx::alloc_spinor_h() {
   return (__half*)p;
 }
 
-void Ctx::ensure_sap() {
-  if (!sap_s) {
-    sap_s = alloc_spinor<float>();
-    sap_a = alloc_spinor<float>();
-    sap_t = alloc_spinor<float>();
-  }
+// Each buffer is allocated on its own when it is missing: an allocation
+// that fails (out of device memory) throws with that buffer and the ones
+// after it still null, and the next call allocates exactly those, so no
+// launch ever sees a buffer of a set that is missing.
+template <typename R>
+static void alloc_missing(Ctx& c, std::initializer_list<R**> ps) {
+  for (R** p : ps)
+    if (!*p) *p = c.alloc_spinor<R>();
 }
+
+void Ctx::ensure_sap() { alloc_missing<float>(*this, {&sap_s, &sap_a, &sap_t}); }
 // (the FP32 SAP buffers are allocated by the FP32 SAP itself: the
 // precision form's inner solve does not need them)
-void Ctx::ensure_inner() {
-  if (!in_q) {
-    in_q = alloc_spinor<float>();
-    in_r = alloc_spinor<float>();
-    in_p = alloc_spinor<float>();
-    in_t = alloc_spinor<float>();
-    in_r0 = alloc_spinor<float>();
-  }
-}
+void Ctx::ensure_inner() { alloc_missing<float>(*this, {&in_q, &in_r, &in_p, &in_t, &in_r0}); }
 void Ctx::ensure_outer() {
   ensure_inner();
-  if (!out_q) {
-    out_q = alloc_spinor<double>();
-    out_r = alloc_spinor<double>();
-    out_p = alloc_spinor<double>();
-    out_t = alloc_spinor<double>();
-    out_u = alloc_spinor<double>();
-    out_r0 = alloc_spinor<double>();
-    ai_b = alloc_spinor<float>();
-    ai_t = alloc_spinor<float>();
-    ai_x = alloc_spinor<float>();
-  }
+  alloc_missing<double>(*this, {&out_q, &out_r, &out_p, &out_t, &out_u, &out_r0});
+  alloc_missing<float>(*this, {&ai_b, &ai_t, &ai_x});
 }
 void Ctx::ensure_hp() {
   ensure_inner();
   ensure_fields_h();
-  if (!h_s) {
-    h_s = alloc_spinor_h();
-    h_a = alloc_spinor_h();
-    h_t = alloc_spinor_h();
-    h_b = alloc_spinor_h();
-    in_w = alloc_spinor<float>();
-  }
+  for (__half** p : {&h_s, &h_a, &h_t, &h_b})
+    if (!*p) *p = alloc_spinor_h();
+  alloc_missing<float>(*this, {&in_w});
 }
 void Ctx::ensure_fields_d() {
-  if (!Ud) {
-    QWSG_CUDA(cudaMalloc(&Ud, sizeof(double) * 72 * (size_t)G.pad));
-    QWSG_CUDA(cudaMalloc(&Cd, sizeof(double) * 72 * (size_t)G.pad));
-    QWSG_CUDA(cudaMemsetAsync(Ud, 0, sizeof(double) * 72 * (size_t)G.pad, st));
-    QWSG_CUDA(cudaMemsetAsync(Cd, 0, sizeof(double) * 72 * (size_t)G.pad, st));
-  }
+  for (double** p : {&Ud, &Cd})
+    if (!*p) {
+      QWSG_CUDA(cudaMalloc(p, sizeof(double) * 72 * (size_t)G.pad));
+      QWSG_CUDA(cudaMemsetAsync(*p, 0, sizeof(double) * 72 * (size_t)G.pad, st));
+    }
 }
 void Ctx::ensure_fields_s() {
-  if (!Us) {
-    QWSG_CUDA(cudaMalloc(&Us, sizeof(float) * 72 * (size_t)G.pad));
-    QWSG_CUDA(cudaMalloc(&Cs, sizeof(float) * 72 * (size_t)G.pad));
-    QWSG_CUDA(cudaMemsetAsync(Us, 0, sizeof(float) * 72 * (size_t)G.pad, st));
-    QWSG_CUDA(cudaMemsetAsync(Cs, 0, sizeof(float) * 72 * (size_t)G.pad, st));
-  }
+  for (float** p : {&Us, &Cs})
+    if (!*p) {
+      QWSG_CUDA(cudaMalloc(p, sizeof(float) * 72 * (size_t)G.pad));
+      QWSG_CUDA(cudaMemsetAsync(*p, 0, sizeof(float) * 72 * (size_t)G.pad, st));
+    }
   fields_h_valid = false;  // the FP16 copies follow the FP32 fields
   links12_valid = false;   // so does the 12-real link copy
 }
@@ -452,10 +435,11 @@ void Ctx::ensure_fields_h() {
     return;
   }
   if (!Us) throw Error(4, "gauge/clover fields not loaded");
-  if (!Uh) {
-    QWSG_CUDA(cudaMalloc(&Uh, sizeof(__half) * 72 * (size_t)G.pad));
-    QWSG_CUDA(cudaMalloc(&Ch, sizeof(__half) * 72 * (size_t)G.pad));
-  }
+  for (__half** p : {&Uh, &Ch})
+    if (!*p) {
+      QWSG_CUDA(cudaMalloc(p, sizeof(__half) * 72 * (size_t)G.pad));
+      fields_h_valid = false;
+    }
   if (!fields_h_valid) {
     fields_s2h(G, Uh, Us, Ch, Cs, st);
     check_launch("fields_s2h");
@@ -547,23 +531,30 @@ template void dslash_outer<double>(Ctx&, double*, const double*, int, int, doubl
 
 // face-site lists, built once on the host from the block geometry
 void Ctx::ensure_face_lists() {
-  if (face_list[0]) return;
+  if (face_list[0] && face_list[1]) return;
   std::vector<int> lst[2];
   for (int g = 0; g < G.V; g++) {
     int col = g >= G.Vh;
     const int t = (g - col * G.Vh) % G.Vb;
     bool face = false;
     for (int mu = 0; mu < 4; mu++) {  // block_local
-      const int l = (t / G.str[mu]) % G.B[mu];
+      const int l = rot_coord(G, mu, (t / G.str[mu]) % G.B[mu]);
       face |= (l == 0) || (l == G.B[mu] - 1);
     }
     if (face) lst[col].push_back(g);
   }
   for (int c2 = 0; c2 < 2; c2++) {
+    if (face_list[c2]) continue;  // made by an earlier call that failed on the other
+    int* d = nullptr;
+    QWSG_CUDA(cudaMalloc(&d, sizeof(int) * (lst[c2].size() + 1)));
+    cudaError_t e = cudaMemcpy(d, lst[c2].data(), sizeof(int) * lst[c2].size(),
+                               cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      cudaFree(d);
+      QWSG_CUDA(e);
+    }
     n_face[c2] = (int)lst[c2].size();
-    QWSG_CUDA(cudaMalloc(&face_list[c2], sizeof(int) * (lst[c2].size() + 1)));
-    QWSG_CUDA(cudaMemcpy(face_list[c2], lst[c2].data(), sizeof(int) * lst[c2].size(),
-                         cudaMemcpyHostToDevice));
+    face_list[c2] = d;
   }
 }
 
@@ -958,6 +949,7 @@ static int outer_loop(Ctx& c, double* x, const double* b, double tol, int iter_b
     blas_cdot<double>(G, r0, q, c.d_res, c.rb, c.st);
     h = c.fetch(2);
     ctmp = std::complex<double>(h[0], h[1]);
+    if (iter == c.breakdown_at && iter > 0) ctmp = 0;  // injected on the host (tests)
     alpha = rho0 / ctmp;
     if (std::abs(ctmp) == 0) alpha = 0;
     blas_bicg_update<double>(G, x, r, u, q, alpha.real(), alpha.imag(), nullptr, c.d_res, c.rb,

@@ -165,7 +165,8 @@ int approx_inv(Ctx& c, double* x, const double* b, double tol_s, int maxiter_s, 
 }
 
 // the flexible FP64 outer BiCGStab on all RHS, iter in [iter_begin, iter_end);
-// conv[r]: the reference's conviter of each RHS (iter_end when not reached)
+// conv[r]: the reference's conviter of each RHS (iter_end when not reached).
+// RHS r stops at its own tolerance when the handle has per-RHS ones.
 void outer_loop(Ctx& c, double* x, const double* b, double tol, int iter_begin, int iter_end,
                 double tol_s, int maxiter_s, int nsap, int nm, bool hf, const bool* active_in,
                 int* conv, long* inner_out, double* rel_out) {
@@ -188,6 +189,8 @@ void outer_loop(Ctx& c, double* x, const double* b, double tol, int iter_begin, 
     conv[k] = iter_end;
     nact += act[k];
   }
+  double tolk[kMax];  // each RHS's own stopping tolerance
+  for (int k = 0; k < nr; k++) tolk[k] = c.rhs_tols.empty() ? tol : c.rhs_tols[k];
   long inner = 0;
   for (int iter = iter_begin; iter < iter_end && nact > 0; iter++) {
     inner += approx_inv(c, u, p, tol_s, maxiter_s, nsap, nm, hf, act);
@@ -211,7 +214,7 @@ void outer_loop(Ctx& c, double* x, const double* b, double tol, int iter_begin, 
       if (!act[k]) continue;
       rnorm[k] = h[4 * k];
       if (!std::isfinite(rnorm[k])) throw Error(3, "solver: non-finite residual norm");
-      if (std::sqrt(rnorm[k] / bnorm[k]) < tol) {
+      if (std::sqrt(rnorm[k] / bnorm[k]) < tolk[k]) {
         conv[k] = iter;
         act[k] = false;
         nact--;
@@ -239,7 +242,7 @@ void outer_loop(Ctx& c, double* x, const double* b, double tol, int iter_begin, 
       rnorm[k] = h[4 * k];
       if (!std::isfinite(rnorm[k])) throw Error(3, "solver: non-finite residual norm");
       rho[k] = cd(h[4 * k + 1], h[4 * k + 2]);
-      if (std::sqrt(rnorm[k] / bnorm[k]) < tol) {
+      if (std::sqrt(rnorm[k] / bnorm[k]) < tolk[k]) {
         conv[k] = iter;
         act[k] = false;
         nact--;
@@ -334,7 +337,7 @@ void bicgstab_dd_mix2_hf_mrhs(Ctx& c, double* x, const double* b, double tol, in
     if (reliable <= 0) break;
     true_residual_mrhs(c, x, b, truerel);
     for (int k = 0; k < nr; k++) {
-      if (act[k] && truerel[k] < tol) act[k] = false;
+      if (act[k] && truerel[k] < (c.rhs_tols.empty() ? tol : c.rhs_tols[k])) act[k] = false;
       left += act[k];
     }
     if (left == 0) break;

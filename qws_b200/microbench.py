@@ -10,8 +10,9 @@ spinors read and written once, links and clover once per site).
 
 Kernels: jinv (one Richardson step on one colour), dslash_s / dslash_d (full
 D in FP32 / FP64), block_s (block-interior D on one colour), face_s (face hops
-of one colour), prec (the whole SAP preconditioner prec_ddd_s_), prec_h (the
-FP16-storage SAP).  --nrhs N runs the launch on a multi-RHS handle (N
+of one colour), jinv_h / face_h (the FP16-storage Richardson step and face
+hops through the single-operator entry points, conversions included), prec
+(the whole SAP preconditioner prec_ddd_s_), prec_h (the FP16-storage SAP).  --nrhs N runs the launch on a multi-RHS handle (N
 right-hand sides per launch; spinor bytes count N times, links and clover
 once).
 """
@@ -75,6 +76,10 @@ def main():
             fn, nbytes = (lambda: lat.ddd_in(bs, 0, out=out_s)), (V // 2) * (2 * sp32 + lc32)
         elif k == "face_s":
             fn, nbytes = (lambda: lat.ddd_out(bs, 0, 0.1, out=out_s)), None
+        elif k == "jinv_h":  # FP16 storage: with the conversions of the single-op entry point
+            fn, nbytes = (lambda: lat.jinv_h(bs, 0, 1, out=out_s)), None
+        elif k == "face_h":
+            fn, nbytes = (lambda: lat.ddd_out_h(bs, 0, 0.1, out=out_s)), None
         elif k == "prec":
             fn, nbytes = (lambda: lat.prec_ddd(bs, 4, 2, out=out_s)), None
         elif k == "prec_h":

@@ -4,12 +4,24 @@ Requests (gauge field, kappa, csw, source, tolerance) arrive at any time.
 The service keeps gauge fields resident on the device, builds each
 request's clover term there (qwsg_build_clover), admits work against an
 HBM budget, merges compatible pending requests -- same lattice, gauge
-field, csw and tolerance; each keeps its own kappa, whose clover term is
-built on the GPU for its RHS (qwsg_batch_set_kappas) -- into one multi-RHS
-solve (qwsg_create_batch), and runs several solves at once on separate CUDA
+field and csw; each keeps its own kappa, whose clover term is built on the
+GPU for its RHS (qwsg_batch_set_kappas), and its own tolerance, at which its
+RHS stops (qwsg_batch_set_tols) -- into one multi-RHS solve
+(qwsg_create_batch), and runs several solves at once on separate CUDA
 streams, so requests that arrive while others are on the GPU start as soon
-as a worker slot and memory are free.  Every result carries its own latency
-(completion minus arrival); `summarize` gives p50/p99 and solves/s.
+as a worker slot and memory are free.  Requests for a field that is busy
+wait for its running solve and join the next batch on it together with
+every compatible request that arrived meanwhile.  Every result carries its
+own latency (completion minus arrival); `summarize` gives p50/p99 and
+solves/s.
+
+Failures are reported on the request (`error`), never by the service
+stopping: a request that cannot fit the HBM budget fails at once
+(MemoryError); one whose `deadline_s` passes before it starts fails with
+DeadlineExceeded; `Service.cancel` withdraws a request that has not started
+(Cancelled); a solver error -- a non-finite residual from a NaN or infinite
+source, say -- fails the requests of that solve, and the field and the
+service stay usable.
 
 The solver is the precision form (bicgstab_dd_mix2_hf: FP64 outer with
 reliable restarts, flexible FP32 inner, FP16-storage SAP).  A request's
@@ -34,7 +46,12 @@ import numpy as np
 # bytes per padded site of the pieces a job holds on the device
 _FIELD_BYTES = 72 * (8 + 4 + 2) * 2 + 4 * 12 * 4  # gauge + clover, FP64/FP32/FP16
 #                                                   copies; 12-real FP32 links
-_WORK_BYTES_PER_RHS = 9 * 24 * 8 + 9 * 24 * 4 + 4 * 52  # FP64, FP32, FP16 work spinors
+_WORK_BYTES_PER_RHS = (6 * 192      # FP64 outer work spinors
+                       + 9 * 96     # FP32: inner solver 5, approximate inverse 3, flexible w
+                       + 4 * 52     # FP16-storage SAP spinors
+                       + 3 * 96     # FP32 SAP buffers (when the FP32 SAP runs on the handle)
+                       + 3 * 192)   # the job's x and b, and the library's staging buffer
+_HANDLE_BYTES = 16 << 20            # reduction and coefficient buffers, face lists
 
 
 def _pad(V):
@@ -49,8 +66,12 @@ _RHS_CLOVER_BYTES = 72 * (8 + 4 + 2)  # per-RHS clover planes of a merged solve
 
 
 def work_bytes(L, nr):
+    """device bytes of an nr-RHS work handle on lattice L: the solver's work
+    spinors, the job's own x and b (kept on the handle, so they are counted
+    here and not left in torch's cache), the library's staging buffer, the
+    per-RHS clover planes of a merged solve, and the handle's small buffers"""
     per = _WORK_BYTES_PER_RHS + (_RHS_CLOVER_BYTES if nr > 1 else 0)
-    return per * _pad(int(np.prod(L))) * nr
+    return per * _pad(int(np.prod(L))) * nr + _HANDLE_BYTES
 
 
 def stream_priority(L):
@@ -77,6 +98,9 @@ class Request:
     # where the solution goes: None -> a new host array; or a C-contiguous
     # FP64 [V, 24] array of the caller's (page-locked: faster download)
     out: np.ndarray | None = None
+    # the request fails with DeadlineExceeded if it has not started this many
+    # seconds after it arrived (None: no deadline)
+    deadline_s: float | None = None
     rid: int = -1
     t_arrival: float = 0.0
     # filled in by the service
@@ -95,8 +119,15 @@ class Request:
 
     def key(self):
         """Requests with the same key merge into one multi-RHS solve (each
-        keeps its own kappa: per-RHS clover terms, qwsg_batch_set_kappas)."""
-        return (self.L, self.gauge, self.csw, self.tol)
+        keeps its own kappa, per-RHS clover terms, qwsg_batch_set_kappas, and
+        its own tolerance, qwsg_batch_set_tols)."""
+        return (self.L, self.gauge, self.csw)
+
+    def wait(self, timeout):
+        """Block until the request is finished; TimeoutError after `timeout` s."""
+        if not self.done.wait(timeout):
+            raise TimeoutError(f"request {self.rid} not finished after {timeout} s")
+        return self
 
     @property
     def latency(self):
@@ -137,9 +168,19 @@ class _Resident:
 
     def close(self):
         for w in self.work.values():
-            w.close()
+            close_work(w)
         self.work.clear()
         self.lat.close()
+
+
+def close_work(w):
+    """Free a work handle and its job buffers, and give torch's cached blocks
+    back to the device so the library's own allocations can use them."""
+    import torch
+
+    w.job_b = w.job_x = None
+    w.close()
+    torch.cuda.empty_cache()
 
 
 class _Placeholder:
@@ -219,6 +260,17 @@ class Service:
             self.cv.notify_all()
         return req
 
+    def cancel(self, req: Request) -> bool:
+        """Withdraw a request that has not started: it finishes at once with
+        error "Cancelled".  False if it has started (a running solve is not
+        interrupted) or is already finished."""
+        with self.cv:
+            if req in self.pending:
+                self._reject(req, "Cancelled")
+                self.cv.notify_all()
+                return True
+            return False
+
     def close(self):
         with self.cv:
             self.stop = True
@@ -256,7 +308,7 @@ class Service:
             for nr in list(r.work):
                 if self.used + need <= self.budget:
                     return True
-                r.work.pop(nr).close()
+                close_work(r.work.pop(nr))
                 self.used -= work_bytes(r.L, nr)
         for r in idle:
             if self.used + need <= self.budget:
@@ -266,6 +318,13 @@ class Service:
             self.used -= r.bytes
             self.evicted += 1
         return self.used + need <= self.budget
+
+    def _expire(self):
+        """Fail the pending requests whose deadline has passed (cv held)."""
+        now = time.monotonic()
+        for q in [q for q in self.pending
+                  if q.deadline_s is not None and now - q.t_arrival > q.deadline_s]:
+            self._reject(q, f"DeadlineExceeded: not started within {q.deadline_s} s")
 
     def _reject(self, q, why):
         self.pending.remove(q)
@@ -284,6 +343,7 @@ class Service:
         takes free memory gives it back when it ends.  A request that cannot
         fit the budget at all fails at once.  Called with cv held; reserves
         the memory and the resident field."""
+        self._expire()
         tried = set()
         blocked = False
         for r in list(self.pending):
@@ -332,6 +392,8 @@ class Service:
             while True:
                 if self.stop and not self.pending:
                     return
+                if self.idle_workers == 0:
+                    self._expire()
                 job = self._pick() if self.idle_workers > 0 and self.pending else None
                 if job is None:
                     self.cv.wait(0.02)
@@ -387,10 +449,18 @@ class Service:
         B = res.work.get(nr)
         if B is None:  # work buffers of an nr-RHS solve on this field, kept for reuse
             B = res.lat.batch(nr, stream=res.stream)
-            B.set_graphs(self.graphs)
+            try:
+                B.set_graphs(self.graphs)
+                with torch.cuda.stream(res.stream):
+                    B.job_b, B.job_x = B.empty("f64"), B.empty("f64")
+            except Exception:
+                B.job_b = B.job_x = None
+                B.close()
+                raise
             res.work[nr] = B
-        if nr > 1:  # every request its own kappa: per-RHS clover terms
+        if nr > 1:  # every request its own kappa (per-RHS clover terms) and tolerance
             B.set_kappas([q.kappa for q in group], r0.csw)
+            B.set_tols([q.tol for q in group])
         res.stream.synchronize()
         t2 = time.monotonic()
         s = self.solver
@@ -411,10 +481,12 @@ class Service:
                         torch.from_numpy(P[k]).copy_(torch.from_numpy(
                             np.ascontiguousarray(q.source, np.float64).reshape(P[k].shape)))
                 S = P
-            bd = B.to_device(S)
-            xd = B.empty("f64")
-            st = B.bicgstab_dd_mix2_hf(xd, bd, r0.tol, s["maxiter"], s["tol_s"], s["maxiter_s"],
-                                       cfg["nsap"], cfg["nm"], reliable=s["reliable"])
+            bd = B.to_device(S, out=B.job_b)
+            xd = B.job_x
+            xd.zero_()
+            st = B.bicgstab_dd_mix2_hf(xd, bd, max(q.tol for q in group), s["maxiter"],
+                                       s["tol_s"], s["maxiter_s"], cfg["nsap"], cfg["nm"],
+                                       reliable=s["reliable"])
             truer = B.true_residual(xd, bd)
             if nr == 1 and r0.out is not None:
                 X = B.to_host(xd, out=r0.out)
@@ -495,12 +567,19 @@ def seeded_gauge(seed0=1000, n_smear=5, alpha=0.36, device=True):
 
 
 def poisson_workload(service, rate, window, volumes, weights, n_gauges, kappa_range=(0.130, 0.137),
-                     csw=1.7, tols=(1e-8, 1e-10, 1e-12), seed=0, sources_per_volume=2):
+                     csw=1.7, tols=(1e-8, 1e-10, 1e-12), seed=0, sources_per_volume=2,
+                     deadline_s=None, scratch_out=False):
     """Poisson arrivals at `rate` per second for `window` seconds.  Each
     request draws a volume (with `weights`), a gauge id, kappa uniform in
     kappa_range, a tolerance and a Gaussian or point source.  Sources come from
     a small pool of page-locked host arrays made before the window opens, so
-    the feeder keeps up with the arrival times.  Returns the submitted requests (wait on req.done)."""
+    the feeder keeps up with the arrival times.  scratch_out: every request
+    of a volume writes its solution into one shared page-locked array that
+    nobody reads (a load generator that keeps thousands of 48^3x96 solutions,
+    2 GB each, would run the host out of memory; concurrent writes into it
+    are harmless because the array is discarded).  Each result's true
+    residual is computed on the device before the download either way.
+    Returns the submitted requests (wait on req.done)."""
     import qws_b200
 
     import torch
@@ -511,6 +590,8 @@ def poisson_workload(service, rate, window, volumes, weights, n_gauges, kappa_ra
         return p
 
     rng = np.random.default_rng(seed)
+    sinks = {L: torch.empty((int(np.prod(L)), 24), dtype=torch.float64, pin_memory=True).numpy()
+             for L in volumes} if scratch_out else {}
     pool = {}
     for L in volumes:
         pool[L] = [pinned(qws_b200.gen_source(L, 5000 + k, "gauss")) for k in range(sources_per_volume)]
@@ -530,7 +611,8 @@ def poisson_workload(service, rate, window, volumes, weights, n_gauges, kappa_ra
         L = tuple(volumes[vi])
         req = Request(L=L, gauge=int(rng.integers(n_gauges)),
                       kappa=float(rng.uniform(*kappa_range)), csw=csw,
-                      tol=float(rng.choice(tols)), source=pool[L][int(rng.integers(len(pool[L])))])
+                      tol=float(rng.choice(tols)), source=pool[L][int(rng.integers(len(pool[L])))],
+                      deadline_s=deadline_s, out=sinks.get(L))
         delay = t0 + ta - time.monotonic()
         if delay > 0:
             time.sleep(delay)
@@ -549,19 +631,44 @@ def main():
     ap.add_argument("--workers", type=int, default=3)
     ap.add_argument("--max-batch", type=int, default=16)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--deadline", type=float, default=None,
+                    help="a request not started this many seconds after arrival fails "
+                         "(load shedding when the arrival rate exceeds what the GPU sustains)")
+    ap.add_argument("--warm", action="store_true",
+                    help="make every (volume, gauge field) resident before the window opens")
     a = ap.parse_args()
     vols = [tuple(int(v) for v in s.split("x")) for s in a.volumes.split(",")]
     weights = [float(w) for w in a.weights.split(",")]
     svc = Service(seeded_gauge(), budget_bytes=a.budget_gb * 1e9, workers=a.workers,
                   max_batch=a.max_batch)
     try:
-        reqs = poisson_workload(svc, a.rate, a.window, vols, weights, a.gauges, seed=a.seed)
+        warm_s = 0.0
+        if a.warm:
+            import qws_b200
+
+            t0 = time.monotonic()
+            warm = [svc.submit(Request(L=L, gauge=g, kappa=0.1335, csw=1.7, tol=1e-8,
+                                       source=qws_b200.gen_source(L, 4000 + g, "gauss")))
+                    for L in vols for g in range(a.gauges)]
+            for q in warm:
+                q.wait(600)
+            warm_s = time.monotonic() - t0
+        merged0 = svc.merged
+        t0 = time.monotonic()
+        reqs = poisson_workload(svc, a.rate, a.window, vols, weights, a.gauges, seed=a.seed,
+                                deadline_s=a.deadline, scratch_out=True)
         for q in reqs:
-            q.done.wait()
-        out = summarize(reqs)
+            q.wait(3600)
+        out = summarize(reqs, t0, max(q.t_done for q in reqs))
+        ok = [q for q in reqs if q.error is None]
         out.update({"rate": a.rate, "window_s": a.window, "requests": len(reqs),
-                    "merged": svc.merged, "workers": a.workers, "budget_gb": a.budget_gb,
-                    "gauges_per_volume": a.gauges})
+                    "merged": svc.merged - merged0, "workers": a.workers,
+                    "budget_gb": a.budget_gb, "gauges_per_volume": a.gauges,
+                    "deadline_s": a.deadline, "warmup_s": round(warm_s, 2),
+                    "shed": sum((q.error or "").startswith("DeadlineExceeded") for q in reqs),
+                    "batch_sizes": {str(b): sum(q.batch == b for q in ok)
+                                    for b in sorted({q.batch for q in ok})},
+                    "fields_evicted": svc.evicted})
         print(json.dumps(out), flush=True)
     finally:
         svc.close()

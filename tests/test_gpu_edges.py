@@ -113,3 +113,67 @@ def test_rejected(L, NB, nr):
             lat.batch(nr).close()
         finally:
             lat.close()
+
+
+def test_forced_breakdown_matches_oracle():
+    """<r0, q> = 0 at the first outer iteration, planted on the host in both
+    the GPU solver (qwsg_inject_breakdown) and the oracle: the reference's
+    guard (alpha = 0, bicgstab_dd_mix.cc:192) keeps x and r for that half
+    step, the omega half step goes on, and both still converge with the same
+    outer count (+-1) to the same solution."""
+    import qws_b200
+    from qwsref import load_oracle
+
+    L, NB = (8, 4, 4, 8), (2, 1, 1, 1)
+    U, C = fields(L)
+    b = qws_b200.gen_source(L, 9)
+    o = Oracle(L, NB, tbc=-1, kappa=KAPPA)
+    o.set_fields(U, C)
+    lib = load_oracle()
+    lib.orc_plant_breakdown(1)
+    try:
+        xo, so, _ = o.bicgstab_dd_mix(b, np.zeros_like(b), 1e-12, 30, 1e-6, 50, 4, 2)
+    finally:
+        lib.orc_plant_breakdown(0)
+    xo_clean, so_clean, _ = o.bicgstab_dd_mix(b, np.zeros_like(b), 1e-12, 30, 1e-6, 50, 4, 2)
+    lat = qws_b200.Lattice(L, NB, tbc=-1, kappa=KAPPA)
+    try:
+        lat.load_fields(U, C)
+        bd, x = lat.to_device(b), lat.empty("f64")
+        lat.inject_breakdown(1)
+        st = lat.bicgstab_dd_mix(x, bd, 1e-12, 30, 1e-6, 50, 4, 2)
+        lat.inject_breakdown(0)
+        assert abs(st["outer_iters"] - so[0]) <= 1
+        assert so[0] >= so_clean[0]  # the lost half step costs iterations, not the answer
+        assert np.isfinite(lat.to_host(x)).all()
+        assert lat.true_residual(x, bd) < 1e-11
+        assert rel(lat.to_host(x), xo) < 1e-10
+    finally:
+        lat.close()
+
+
+def test_nan_source_fails_cleanly():
+    """A source holding a NaN makes the residual non-finite: the solve
+    returns error code 3 (no NaN solution is handed back as a result), and
+    the handle and the device stay usable for the next solve."""
+    import qws_b200
+
+    L, NB = (8, 4, 4, 8), (2, 1, 1, 1)
+    U, C = fields(L)
+    b = qws_b200.gen_source(L, 9)
+    lat = qws_b200.Lattice(L, NB, tbc=-1, kappa=KAPPA)
+    try:
+        lat.load_fields(U, C)
+        bad = b.copy()
+        bad[5, 3] = np.nan
+        x = lat.empty("f64")
+        with pytest.raises(qws_b200.QwsgError, match="non-finite"):
+            lat.bicgstab_dd_mix(x, lat.to_device(bad), 1e-10, 30, 1e-6, 50, 4, 2)
+        with pytest.raises(qws_b200.QwsgError, match="non-finite"):
+            lat.bicgstab_dd_mix2_hf(x, lat.to_device(bad), 1e-10, 30, 1e-6, 50, 4, 2, reliable=3)
+        x.zero_()
+        bd = lat.to_device(b)
+        st = lat.bicgstab_dd_mix(x, bd, 1e-10, 30, 1e-6, 50, 4, 2)
+        assert st["outer_iters"] < 30 and lat.true_residual(x, bd) < 1e-10
+    finally:
+        lat.close()

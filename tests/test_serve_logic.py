@@ -1,8 +1,10 @@
 """The solve service's scheduling on CPU (no GPU work): compatible pending
-requests merge into a power-of-two batch of at most max_batch, the oldest
-request goes first, a busy field holds back its requests, and admission
-evicts idle work buffers, then idle fields, least recently used first,
-never the field the job needs."""
+requests (same lattice, gauge field, csw; any kappa and tolerance) merge
+into a power-of-two batch of at most max_batch, the oldest request goes
+first, a busy field holds back its requests, and admission evicts idle work
+buffers, then idle fields, least recently used first, never the field the
+job needs.  Requests past their deadline and cancelled requests finish with
+an error instead of running; waiting on a request has a timeout."""
 import threading
 
 import numpy as np
@@ -48,8 +50,9 @@ L1, L2 = (8, 8, 8, 8), (16, 16, 16, 32)
 
 def test_merge_power_of_two_and_order():
     svc = make_service(1e12, max_batch=4)
-    a = [req(L1, 0, 0.13 + 0.001 * k) for k in range(5)]  # kappas differ: still compatible
-    b = req(L1, 0, 0.12, tol=1e-8)
+    # kappas and tolerances differ: still compatible (per-RHS kappa and tol)
+    a = [req(L1, 0, 0.13 + 0.001 * k, tol=(1e-8, 1e-10, 1e-12)[k % 3]) for k in range(5)]
+    b = req(L1, 1, 0.12, tol=1e-8)  # another gauge field
     svc.pending = [b] + a
     res, group = svc._pick()
     assert group == [b]                      # the oldest request first
@@ -186,3 +189,42 @@ def test_summarize_phases_errors_and_volumes():
     assert st["requests_with_field_load"] == 1 and st["above_tol"] == 0
     assert st["by_volume"]["8x8x8x8"][0] == 2 and st["by_volume"]["16x16x16x32"] == [1, 500.0, 300.0]
     assert st["phases_ms"]["queue"][0] == 10.0
+
+
+def test_deadline_expires_before_start():
+    svc = make_service(1e12)
+    svc.residents[(L1, 0)] = FakeResident(L1, 0, 1.0, busy=True)
+    late = req(L1, 0, 0.13)
+    late.deadline_s = 0.5
+    late.t_arrival = -10.0  # arrived long ago, its field still busy
+    ok = req(L2, 1, 0.13)
+    ok.deadline_s = 3600.0
+    svc.pending = [late, ok]
+    import time as _t
+    ok.t_arrival = _t.monotonic()
+    res, group = svc._pick()
+    assert group == [ok]
+    assert late.done.is_set() and late.error.startswith("DeadlineExceeded")
+    assert late in svc.completed and svc.pending == []
+
+
+def test_cancel_pending_only():
+    svc = make_service(1e12)
+    a, b = req(L1, 0, 0.13), req(L1, 0, 0.13)
+    svc.pending = [a, b]
+    assert svc.cancel(a)
+    assert a.done.is_set() and a.error == "Cancelled" and svc.pending == [b]
+    assert not svc.cancel(a)  # already finished
+    res, group = svc._pick()
+    assert group == [b]
+    assert not svc.cancel(b)  # started: a running solve is not interrupted
+
+
+def test_wait_times_out():
+    import pytest
+
+    q = req(L1, 0, 0.13)
+    with pytest.raises(TimeoutError):
+        q.wait(0.01)
+    q.done.set()
+    assert q.wait(0.01) is q
