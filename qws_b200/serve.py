@@ -205,8 +205,14 @@ class Service:
 
     def __init__(self, gauge_source, budget_bytes=150e9, workers=3, max_batch=16,
                  block_grid=None, maxiter=100, tol_s=1e-6, maxiter_s=50, nsap=None, nm=None,
-                 reliable=5, graphs=True):
+                 reliable=5, graphs=True, lifo_after_s=None):
         self.gauge_source = gauge_source
+        # adaptive LIFO: once the oldest pending request has waited longer
+        # than this (s), the newest pending requests are served first -- under
+        # overload the oldest are the ones a deadline sheds, and serving them
+        # first would make every served request wait about as long (None:
+        # always in arrival order)
+        self.lifo_after_s = lifo_after_s
         # CUDA graphs of the SAP sequences are captured per (buffers, kappa);
         # they pay off when requests repeat a kappa
         self.graphs = bool(graphs)
@@ -346,7 +352,11 @@ class Service:
         self._expire()
         tried = set()
         blocked = False
-        for r in list(self.pending):
+        order = list(self.pending)
+        if (self.lifo_after_s is not None and order and
+                time.monotonic() - order[0].t_arrival > self.lifo_after_s):
+            order.reverse()
+        for r in order:
             if r.key() in tried:
                 continue
             tried.add(r.key())
@@ -358,7 +368,7 @@ class Service:
             res = self.residents.get((r.L, r.gauge))
             if res is not None and res.busy:
                 continue
-            group = [q for q in self.pending if q.key() == r.key()]
+            group = [q for q in order if q.key() == r.key()]
             nr = 1
             while nr * 2 <= min(len(group), self.max_batch, 32):
                 nr *= 2
@@ -634,13 +644,18 @@ def main():
     ap.add_argument("--deadline", type=float, default=None,
                     help="a request not started this many seconds after arrival fails "
                          "(load shedding when the arrival rate exceeds what the GPU sustains)")
+    ap.add_argument("--lifo-after", type=float, default=None,
+                    help="serve the newest requests first once the oldest has waited this "
+                         "long (default with --deadline: min(2 s, deadline/4); else never)")
     ap.add_argument("--warm", action="store_true",
                     help="make every (volume, gauge field) resident before the window opens")
     a = ap.parse_args()
     vols = [tuple(int(v) for v in s.split("x")) for s in a.volumes.split(",")]
     weights = [float(w) for w in a.weights.split(",")]
     svc = Service(seeded_gauge(), budget_bytes=a.budget_gb * 1e9, workers=a.workers,
-                  max_batch=a.max_batch)
+                  max_batch=a.max_batch,
+                  lifo_after_s=(a.lifo_after if a.lifo_after is not None else
+                                (None if a.deadline is None else min(2.0, a.deadline / 4))))
     try:
         warm_s = 0.0
         if a.warm:
@@ -664,7 +679,8 @@ def main():
         out.update({"rate": a.rate, "window_s": a.window, "requests": len(reqs),
                     "merged": svc.merged - merged0, "workers": a.workers,
                     "budget_gb": a.budget_gb, "gauges_per_volume": a.gauges,
-                    "deadline_s": a.deadline, "warmup_s": round(warm_s, 2),
+                    "deadline_s": a.deadline, "lifo_after_s": svc.lifo_after_s,
+                    "warmup_s": round(warm_s, 2),
                     "shed": sum((q.error or "").startswith("DeadlineExceeded") for q in reqs),
                     "batch_sizes": {str(b): sum(q.batch == b for q in ok)
                                     for b in sorted({q.batch for q in ok})},

@@ -38,6 +38,7 @@ def make_service(budget, max_batch=16):
     svc.pending, svc.residents, svc.used, svc.merged, svc.evicted = [], {}, 0.0, 0, 0
     svc.completed = []
     svc.cv = threading.Condition()
+    svc.lifo_after_s = None
     return svc
 
 
@@ -228,3 +229,25 @@ def test_wait_times_out():
         q.wait(0.01)
     q.done.set()
     assert q.wait(0.01) is q
+
+
+def test_adaptive_lifo_under_overload():
+    """Once the oldest pending request has waited longer than lifo_after_s,
+    the newest compatible requests are served first (the oldest are the
+    ones a deadline sheds); before that, arrival order."""
+    import time as _t
+
+    svc = make_service(1e12, max_batch=2)
+    svc.lifo_after_s = 1.0
+    now = _t.monotonic()
+    reqs = [req(L1, 0, 0.13) for _ in range(4)]
+    for k, q in enumerate(reqs):
+        q.t_arrival = now - 0.1 * (4 - k)  # all recent: arrival order
+    svc.pending = list(reqs)
+    res, group = svc._pick()
+    assert group == reqs[:2]
+    res.busy = False
+    svc.pending = list(reqs)
+    reqs[0].t_arrival = now - 5.0  # the oldest has waited long: newest first
+    res, group = svc._pick()
+    assert group == [reqs[3], reqs[2]]
