@@ -101,3 +101,29 @@ def test_oracle_generator_bit_equal(Lg, n_smear, csw, kappa):
     for kind, arg in (("gauss", 0), ("z2", 0), ("point", 7)):
         np.testing.assert_array_equal(bits(qws_b200.gen_source(Lg, 12, kind, arg)),
                                       bits(qwsref.gen_source(Lg, 12, kind, arg)))
+
+
+def test_reference_solution_fixture():
+    """tests/golden/ref_solutions_48c96.npz (made by make_ref_solutions.py from
+    the reference's own 48^3x96 solves): both kappas, 1024 distinct sites in
+    range, finite values, iteration counts and residuals of a converged
+    1e-10 solve, and the same gauge field and source digests for both."""
+    import json
+    from pathlib import Path
+
+    z = np.load(Path(__file__).parent / "golden" / "ref_solutions_48c96.npz")
+    meta = json.loads(str(z["meta"]))
+    V = 48 * 48 * 48 * 96
+    sites = z["sites"]
+    assert len(sites) == 1024 and len(set(sites.tolist())) == 1024
+    assert sites.min() >= 0 and sites.max() < V and (np.diff(sites) > 0).all()
+    assert set(meta) == {"0.1365", "0.1355"}
+    for k, m in meta.items():
+        x = z[f"x_{k}"]
+        assert x.shape == (1024, 24) and np.isfinite(x).all()
+        assert m["true_rel_resid"] < 1e-10 and m["outer_iters"] >= 1
+        # the sample carries its share of |x|^2
+        share = float(np.sum(x * x)) / float(z[f"xnorm2_{k}"])
+        assert 0.2 * 1024 / V < share < 5 * 1024 / V
+    a, b = meta["0.1365"]["field_sha256"], meta["0.1355"]["field_sha256"]
+    assert a["gauge"] == b["gauge"] and a["source"] == b["source"] and a["clover"] != b["clover"]
