@@ -356,6 +356,97 @@ struct OpS2D {
   }
 };
 
+// complex float arithmetic of the inner loop's scalars, each product and
+// sum rounded on its own (no contraction), as the host loop computes them;
+// the quotient is formed in FP64 and rounded once
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+  return make_float2(__fsub_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)),
+                     __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+__device__ __forceinline__ float2 cdivf(float2 a, float2 b) {
+  const double den = (double)b.x * b.x + (double)b.y * b.y;
+  return make_float2((float)(((double)a.x * b.x + (double)a.y * b.y) / den),
+                     (float)(((double)a.y * b.x - (double)a.x * b.y) / den));
+}
+__device__ __forceinline__ float cabsf2(float2 a) { return hypotf(a.x, a.y); }
+
+__global__ void k_inner_scalars(InnerScalars* s, const double* __restrict__ res, int phase,
+                                double tol) {
+  const bool done = s->done != 0;
+  switch (phase) {
+    case 0: {
+      const float bn = (float)res[0];
+      s->bnorm = bn;
+      s->rnorm = bn;
+      s->rho0r = bn;
+      s->rho0i = 0;
+      s->done = bn == 0;
+      s->iters = 0;
+      s->bad = 0;
+      s->iter = 0;
+      for (int k = 0; k < 12; k++) s->cf[k] = 0;
+      break;
+    }
+    case 1: {  // alpha = rho0 / <r0, q>, zero when |<r0, q>| <= 1e-15
+      float2 a = make_float2(0, 0);
+      if (!done) {
+        const float2 ct = make_float2((float)res[0], (float)res[1]);
+        a = cdivf(make_float2(s->rho0r, s->rho0i), ct);
+        if (cabsf2(ct) <= 1e-15f) a = make_float2(0, 0);
+      }
+      s->ar = a.x;
+      s->ai = a.y;
+      s->cf[0] = a.x;
+      s->cf[1] = a.y;
+      break;
+    }
+    case 2:
+    case 4: {
+      float2 beta = make_float2(0, 0), w = make_float2(0, 0);
+      if (!done) {
+        const float rn = (float)res[0];
+        s->rnorm = rn;
+        if (!isfinite(rn)) {
+          s->bad = 1;
+          s->done = 1;
+        } else if ((double)sqrtf(rn / s->bnorm) < tol) {
+          s->done = 1;
+          s->iters = s->iter + 1;
+        } else if (phase == 4) {  // beta = alpha rho / (rho0 omega); rho0 = rho
+          const float2 rho = make_float2((float)res[1], (float)res[2]);
+          w = make_float2(s->wr, s->wi);
+          beta = cdivf(cmulf(make_float2(s->ar, s->ai), rho),
+                       cmulf(make_float2(s->rho0r, s->rho0i), w));
+          s->rho0r = rho.x;
+          s->rho0i = rho.y;
+          if (cabsf2(w) == 0 || cabsf2(rho) == 0) beta = make_float2(0, 0);
+        }
+      }
+      if (phase == 4) {
+        s->cf[8] = beta.x;
+        s->cf[9] = beta.y;
+        s->cf[10] = w.x;
+        s->cf[11] = w.y;
+        s->iter++;
+      }
+      break;
+    }
+    case 3: {  // omega = <t, r> / |t|^2, zero when |t|^2 <= 1e-30
+      float2 w = make_float2(0, 0);
+      if (!done) {
+        const float r0 = (float)res[0], r1 = (float)res[1], r2 = (float)res[2];
+        w = make_float2(r1 / r0, r2 / r0);
+        if (r0 <= 1e-30f) w = make_float2(0, 0);
+      }
+      s->wr = w.x;
+      s->wi = w.y;
+      s->cf[4] = w.x;
+      s->cf[5] = w.y;
+      break;
+    }
+  }
+}
+
 int grid_for(const Geom& G, const RedBuf* rb) {
   int b = ((G.V << G.lgnr) + kThreads - 1) / kThreads;
   int cap = rb ? rb->nblk : 148 * 8;
@@ -454,6 +545,11 @@ void blas_d2s(const Geom& G, float* y, const double* x, double s, cudaStream_t s
 void blas_s2d(const Geom& G, double* y, const float* x, double s, cudaStream_t st,
               const double* cf) {
   run<float, 0>(G, OpS2D{y, x, s, cf}, nullptr, nullptr, st);
+}
+
+void inner_scalars(InnerScalars* s, const double* res, int phase, double tol, cudaStream_t st) {
+  count_launch();
+  k_inner_scalars<<<1, 1, 0, st>>>(s, res, phase, tol);
 }
 
 #define QWSG_INST(R)                                                                         \

@@ -62,6 +62,11 @@ struct Ctx {
   RedBuf rb{};
   double* d_res = nullptr;
   double* h_res = nullptr;  // pinned
+  // device-side scalars of the single-RHS flexible inner solve, and their
+  // pinned host copy (ensure_hp)
+  InnerScalars* d_isc = nullptr;
+  InnerScalars* h_isc = nullptr;
+  const InnerScalars* fetch_inner();
 
   // work buffers, allocated on first use
   float* sap_s = nullptr;
@@ -189,9 +194,10 @@ struct Ctx {
     const void* b;
     int nsap, nm;
     double kappa;
+    double tol = 0;  // the stopping tolerance a captured solver step compares with
     bool operator==(const GraphKey& o) const {
       return op == o.op && a == o.a && b == o.b && nsap == o.nsap && nm == o.nm &&
-             kappa == o.kappa;
+             kappa == o.kappa && tol == o.tol;
     }
   };
   struct GraphEntry {

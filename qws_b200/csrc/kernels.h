@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <cstddef>
 
 #include "lattice.cuh"
 
@@ -145,6 +146,28 @@ void fields_s2h(const Geom& G, __half* Uh, const float* Us, __half* Ch, const fl
                 cudaStream_t st);
 // FP16 copy of per-RHS FP32 clover planes (entries of a multi-RHS handle)
 void clover_s2h_entries(const Geom& G, __half* Ch, const float* Cs, cudaStream_t st);
+// Device-side scalars of the flexible inner BiCGStab of one right-hand side
+// (bicgstab_precdd_s_h.cc:83-369): the loop's reductions land in res, a
+// one-thread kernel turns them into the next update's coefficients, kept
+// in cf in the layout the update kernels read as a per-RHS table (alpha at
+// 0-1, omega at 4-5, beta and omega of the p update at 8-11), and decides
+// convergence, so the host reads back one small record per half iteration
+// instead of every reduction.  done: converged (or b = 0) -- the remaining
+// updates of the iteration use zero coefficients; iters: the iteration the
+// residual fell below tol; bad: a non-finite residual.
+struct InnerScalars {
+  double cf[12];
+  float bnorm, rnorm, rho0r, rho0i, ar, ai, wr, wi;
+  int done, iters, bad, iter;
+};
+// phase 0: after r = b (res[0] = |b|^2); 1: after <r0, q>; 2: after the alpha
+// update (res[0] = |r|^2); 3: after |t|^2, <t, r>; 4: after the omega update
+// (|r|^2, <r0, r>), which also sets beta
+void inner_scalars(InnerScalars* s, const double* res, int phase, double tol, cudaStream_t st);
+inline double* inner_coefs(InnerScalars* s, int k) {  // device address of cf + k
+  return reinterpret_cast<double*>(reinterpret_cast<char*>(s) + offsetof(InnerScalars, cf)) + k;
+}
+
 // y = (float)(x * s)   /   y = (double)x * s   (cf: per-RHS s, cf[4*rhs])
 void blas_d2s(const Geom& G, float* y, const double* x, double s, cudaStream_t st,
               const double* cf = nullptr);

@@ -294,6 +294,7 @@ Ctx::~Ctx() {
   cudaFree(rb.counter);
   cudaFree(d_res);
   cudaFreeHost(h_res);
+  if (h_isc) cudaFreeHost(h_isc);
   if (own_stream && st) cudaStreamDestroy(st);
 }
 
@@ -343,6 +344,13 @@ void Ctx::ensure_hp() {
   for (__half** p : {&h_s, &h_a, &h_t, &h_b})
     if (!*p) *p = alloc_spinor_h();
   alloc_missing<float>(*this, {&in_w});
+  if (!d_isc) {
+    void* q = nullptr;
+    QWSG_CUDA(cudaMalloc(&q, sizeof(InnerScalars)));
+    owned.push_back(q);
+    d_isc = static_cast<InnerScalars*>(q);
+  }
+  if (!h_isc) QWSG_CUDA(cudaMallocHost(&h_isc, sizeof(InnerScalars)));
 }
 void Ctx::ensure_fields_d() {
   for (double** p : {&Ud, &Cd})
@@ -445,6 +453,12 @@ void Ctx::ensure_fields_h() {
     check_launch("fields_s2h");
     fields_h_valid = true;
   }
+}
+
+const InnerScalars* Ctx::fetch_inner() {
+  QWSG_CUDA(cudaMemcpyAsync(h_isc, d_isc, sizeof(InnerScalars), cudaMemcpyDeviceToHost, st));
+  QWSG_CUDA(cudaStreamSynchronize(st));
+  return h_isc;
 }
 
 const double* Ctx::fetch(int n) {
@@ -642,6 +656,14 @@ static void graphed(Ctx& c, const Ctx::GraphKey& k, F&& body) {
     body();
     return;
   }
+  // inside a capture that is already running (a solver step that contains
+  // this sequence): the launches become part of that graph
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  QWSG_CUDA(cudaStreamIsCapturing(c.st, &cs));
+  if (cs == cudaStreamCaptureStatusActive) {
+    body();
+    return;
+  }
   for (auto& e : c.graphs)
     if (e.key == k) {
       QWSG_CUDA(cudaGraphLaunch(e.exec, c.st));
@@ -666,6 +688,31 @@ static void graphed(Ctx& c, const Ctx::GraphKey& k, F&& body) {
   }
   cudaGraph_t g = nullptr;
   QWSG_CUDA(cudaStreamEndCapture(c.st, &g));
+  // the same step with other scalar arguments (kappa, tolerance): the launch
+  // sequence is the same, so update the instantiated graph in place -- far
+  // cheaper than instantiating one (a service sees a new kappa in nearly
+  // every request); launches already enqueued keep their arguments
+  for (size_t i = 0; i < c.graphs.size(); i++) {
+    auto& en = c.graphs[i];
+    if (en.key.op == k.op && en.key.a == k.a && en.key.b == k.b && en.key.nsap == k.nsap &&
+        en.key.nm == k.nm) {
+      cudaGraphExecUpdateResultInfo info{};
+      if (cudaGraphExecUpdate(en.exec, g, &info) == cudaSuccess) {
+        cudaGraphDestroy(g);
+        en.key = k;
+        QWSG_CUDA(cudaGraphLaunch(en.exec, c.st));
+        c.n_graph_launches++;
+        return;
+      }
+      // not updatable: drop that graph (after its pending launches) and
+      // instantiate a new one below
+      (void)cudaGetLastError();
+      QWSG_CUDA(cudaStreamSynchronize(c.st));
+      cudaGraphExecDestroy(en.exec);
+      c.graphs.erase(c.graphs.begin() + i);
+      break;
+    }
+  }
   cudaGraphExec_t exec = nullptr;
   cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
   cudaGraphDestroy(g);
@@ -716,11 +763,9 @@ void prec_s(Ctx& c, float* out, const float* in, int nsap, int nm) {
 // is stored with per-site scales instead of the reference's one global
 // scale (assign_q_s2h, qws_h.cc:175-207), arithmetic is FP32, and the sweep
 // count is the reference's half-precision one (isap = 1 .. nsap-1).
-void prec_s_h(Ctx& c, float* out, const float* in, int nsap, int nm) {
-  if (nsap > 10 || nm > 10)
-    throw Error(2, "assign_mult_mSAP_s_h_: nsap and nm must be <= 10 (prec_ddd_s_h.h:100-101)");
-  c.ensure_hp();
-  c.ensure_face_lists();
+// the launches alone (buffers, face lists and fields already in place), for
+// callers that capture them inside a larger step
+static void prec_s_h_seq(Ctx& c, float* out, const float* in, int nsap, int nm) {
   graphed(c, {2, out, in, nsap, nm, c.kappa}, [&] {
     spinor_s2h(c.G, c.h_b, in, c.st);
     spinor_h2h(c.G, c.h_s, c.h_b, c.st);
@@ -729,6 +774,14 @@ void prec_s_h(Ctx& c, float* out, const float* in, int nsap, int nm) {
     spinor_h2s(c.G, out, c.h_a, c.st);
     c.n_prec_s_h++;
   });
+}
+
+void prec_s_h(Ctx& c, float* out, const float* in, int nsap, int nm) {
+  if (nsap > 10 || nm > 10)
+    throw Error(2, "assign_mult_mSAP_s_h_: nsap and nm must be <= 10 (prec_ddd_s_h.h:100-101)");
+  c.ensure_hp();
+  c.ensure_face_lists();
+  prec_s_h_seq(c, out, in, nsap, nm);
   c.check_launch("prec_s_h");
 }
 
@@ -842,63 +895,59 @@ int bicgstab_precdd_s(Ctx& c, float* x, const float* b, double tol, int maxiter,
 // bicgstab_precdd_s_h_ (bicgstab_precdd_s_h.cc:83-369): flexible BiCGStab,
 // w = M p, q = D w, x += alpha w (and likewise for the omega step), with the
 // FP16-storage SAP as M and the FP32 D (assign_mult_wd_s_, prec_ddd_s_h.h:233).
+// The scalars live on the device (InnerScalars, inner_scalars): each half
+// iteration -- SAP, D, the reduction, the scalar update, the vector update
+// and its norms -- is one CUDA graph replay, after which the host reads
+// back one small record (convergence, a non-finite residual) instead of
+// every reduction.  The arithmetic and its order are the host loop's.
 int bicgstab_precdd_s_h(Ctx& c, float* x, const float* b, double tol, int maxiter, int nsap,
                         int nm, double* final_rel) {
+  if (nsap > 10 || nm > 10)
+    throw Error(2, "assign_mult_mSAP_s_h_: nsap and nm must be <= 10 (prec_ddd_s_h.h:100-101)");
   c.ensure_hp();
+  c.ensure_face_lists();  // built before any capture
+  c.ensure_links12();
   const Geom& G = c.G;
   float *q = c.in_q, *r = c.in_r, *p = c.in_p, *t = c.in_t, *r0 = c.in_r0, *w = c.in_w;
+  InnerScalars* S = c.d_isc;
   blas_zero<float>(G, x, 0, G.V, c.st);
   blas_bicg_init<float>(G, b, nullptr, r, p, r0, c.d_res, c.rb, c.st);
-  const double* h = c.fetch(2);
-  const float bnorm = (float)h[0];
-  if (bnorm == 0) {  // b = 0: x = 0 (zeroed above)
+  inner_scalars(S, c.d_res, 0, tol, c.st);
+  const InnerScalars* h = c.fetch_inner();
+  if (h->done) {  // b = 0: x = 0 (zeroed above)
     if (final_rel) *final_rel = 0;
     return 0;
   }
-  std::complex<float> rho0(bnorm, 0), rho, beta, omega, alpha, ctmp;
-  float rnorm = bnorm;
-  int done = maxiter;
   for (int iter = 0; iter < maxiter; iter++) {
     c.n_inner_iter++;
-    prec_s_h(c, w, p, nsap, nm);
-    dslash_full_s(c, q, w);
-    blas_cdot<float>(G, r0, q, c.d_res, c.rb, c.st);
-    h = c.fetch(2);
-    ctmp = std::complex<float>((float)h[0], (float)h[1]);
-    alpha = rho0 / ctmp;
-    if (std::abs(ctmp) <= 1e-15f) alpha = 0;
-    blas_bicg_update<float>(G, x, r, w, q, alpha.real(), alpha.imag(), nullptr, c.d_res, c.rb,
-                            c.st);
-    rnorm = (float)c.fetch(1)[0];
-    if (!std::isfinite(rnorm)) throw Error(3, "solver: non-finite residual norm");
-    if (std::sqrt(rnorm / bnorm) < tol) {
-      done = iter + 1;
-      break;
-    }
-    prec_s_h(c, w, r, nsap, nm);
-    dslash_full_s(c, t, w);
-    blas_norm_cdot<float>(G, t, r, c.d_res, c.rb, c.st);
-    h = c.fetch(3);
-    const float redu0 = (float)h[0], redu1 = (float)h[1], redu2 = (float)h[2];
-    omega = std::complex<float>(redu1 / redu0, redu2 / redu0);
-    if (redu0 <= 1e-30f) omega = 0;
-    blas_bicg_update<float>(G, x, r, w, t, omega.real(), omega.imag(), r0, c.d_res, c.rb, c.st);
-    h = c.fetch(3);
-    rnorm = (float)h[0];
-    if (!std::isfinite(rnorm)) throw Error(3, "solver: non-finite residual norm");
-    rho = std::complex<float>((float)h[1], (float)h[2]);
-    if (std::sqrt(rnorm / bnorm) < tol) {
-      done = iter + 1;
-      break;
-    }
-    beta = alpha * rho / (rho0 * omega);
-    rho0 = rho;
-    if (std::abs(omega) == 0 || std::abs(rho0) == 0) beta = 0;
-    blas_bicg_p<float>(G, p, r, q, beta.real(), beta.imag(), omega.real(), omega.imag(), c.st);
+    graphed(c, {5, x, r0, nsap, nm, c.kappa, tol}, [&] {
+      prec_s_h_seq(c, w, p, nsap, nm);
+      dslash_full_s(c, q, w);
+      blas_cdot<float>(G, r0, q, c.d_res, c.rb, c.st);
+      inner_scalars(S, c.d_res, 1, tol, c.st);
+      blas_bicg_update<float>(G, x, r, w, q, 0, 0, nullptr, c.d_res, c.rb, c.st,
+                              inner_coefs(S, 0));
+      inner_scalars(S, c.d_res, 2, tol, c.st);
+    });
+    h = c.fetch_inner();
+    if (h->bad) throw Error(3, "solver: non-finite residual norm");
+    if (h->done) break;
+    graphed(c, {6, x, r0, nsap, nm, c.kappa, tol}, [&] {
+      prec_s_h_seq(c, w, r, nsap, nm);
+      dslash_full_s(c, t, w);
+      blas_norm_cdot<float>(G, t, r, c.d_res, c.rb, c.st);
+      inner_scalars(S, c.d_res, 3, tol, c.st);
+      blas_bicg_update<float>(G, x, r, w, t, 0, 0, r0, c.d_res, c.rb, c.st, inner_coefs(S, 4));
+      inner_scalars(S, c.d_res, 4, tol, c.st);
+      blas_bicg_p<float>(G, p, r, q, 0, 0, 0, 0, c.st, inner_coefs(S, 8));
+    });
+    h = c.fetch_inner();
+    if (h->bad) throw Error(3, "solver: non-finite residual norm");
+    if (h->done) break;
   }
-  if (final_rel) *final_rel = std::sqrt((double)rnorm / (double)bnorm);
+  if (final_rel) *final_rel = std::sqrt((double)h->rnorm / (double)h->bnorm);
   c.check_launch("bicgstab_precdd_s_h");
-  return done;
+  return h->done ? h->iters : maxiter;
 }
 
 // approx_inv_dirac_op (bicgstab_dd_mix.cc:76-102) with the renormalising

@@ -12,7 +12,9 @@ Kernels: jinv (one Richardson step on one colour), dslash_s / dslash_d (full
 D in FP32 / FP64), block_s (block-interior D on one colour), face_s (face hops
 of one colour), jinv_h / face_h (the FP16-storage Richardson step and face
 hops through the single-operator entry points, conversions included), prec
-(the whole SAP preconditioner prec_ddd_s_), prec_h (the FP16-storage SAP).  --nrhs N runs the launch on a multi-RHS handle (N
+(the whole SAP preconditioner prec_ddd_s_), prec_h (the FP16-storage SAP),
+solve_hf (a whole precision-form solve to 1e-10; --new-kappa rebuilds the
+clover term for another kappa before each, as a serving loop sees them).  --nrhs N runs the launch on a multi-RHS handle (N
 right-hand sides per launch; spinor bytes count N times, links and clover
 once).
 """
@@ -38,6 +40,9 @@ def main():
     ap.add_argument("--kappa", type=float, default=0.1365)
     ap.add_argument("--csw", type=float, default=1.7)
     ap.add_argument("--nrhs", type=int, default=1)
+    ap.add_argument("--new-kappa", action="store_true",
+                    help="solve_hf: a different kappa (clover rebuilt on the GPU) before every "
+                         "solve, as a serving loop sees them")
     ap.add_argument("--links18", action="store_true",
                     help="FP32 kernels read 18-real links even for SU(3) fields")
     a = ap.parse_args()
@@ -80,6 +85,18 @@ def main():
             fn, nbytes = (lambda: lat.jinv_h(bs, 0, 1, out=out_s)), None
         elif k == "face_h":
             fn, nbytes = (lambda: lat.ddd_out_h(bs, 0, 0.1, out=out_s)), None
+        elif k == "solve_hf":  # one precision-form solve to 1e-10 from x = 0
+            xs = lat.empty("f64")
+            state = {"n": 0}
+
+            def fn():
+                if a.new_kappa:
+                    state["n"] += 1
+                    lat.set_kappa(a.kappa - 1e-4 * (state["n"] % 50))
+                    lat.build_clover(a.csw)
+                xs.zero_()
+                lat.bicgstab_dd_mix2_hf(xs, bd, 1e-10, 100, 1e-6, 50, 4, 2, reliable=5)
+            nbytes = None
         elif k == "prec":
             fn, nbytes = (lambda: lat.prec_ddd(bs, 4, 2, out=out_s)), None
         elif k == "prec_h":

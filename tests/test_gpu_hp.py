@@ -141,3 +141,35 @@ def test_fp16_storage_of_vanishing_sites():
         assert rel(h, f) < 1e-2
     finally:
         lat.close()
+
+
+def test_graphs_updated_for_a_new_kappa_match_direct_launches():
+    """The precision form's inner solve replays each half iteration as a
+    captured CUDA graph with its scalars on the device; when kappa changes
+    the graphs are captured again and updated in place.  After such a
+    change the solve is bit-for-bit the one direct launches give, and the
+    device-side iteration count equals the host-side one."""
+    import qws_b200
+
+    L, NB = (8, 8, 8, 8), (2, 2, 2, 2)
+    U, _ = qws_b200.gen_gauge(L, 5, 2, 0.36)
+    b = qws_b200.gen_source(L, 6)
+    res = {}
+    for graphs in (True, False):
+        lat = qws_b200.Lattice(L, NB, tbc=-1, kappa=0.130)
+        try:
+            lat.load_gauge(U)
+            lat.set_graphs(graphs)
+            bd, x = lat.to_device(b), lat.empty("f64")
+            for kappa in (0.130, 0.1345, 0.132):  # the second and third update the graphs
+                lat.set_kappa(kappa)
+                lat.build_clover(1.7)
+                x.zero_()
+                st = lat.bicgstab_dd_mix2_hf(x, bd, 1e-10, 50, 1e-6, 50, 4, 2, reliable=5)
+            res[graphs] = (lat.to_host(x), st, lat.true_residual(x, bd))
+        finally:
+            lat.close()
+    (xg, sg, tg), (xd, sd, td) = res[True], res[False]
+    np.testing.assert_array_equal(xg, xd)
+    assert sg["inner_iters"] == sd["inner_iters"] and sg["outer_iters"] == sd["outer_iters"]
+    assert tg < 1e-10
