@@ -903,12 +903,13 @@ def bench_uneven(args):
     """48 independent solves, volumes drawn uniformly from 8^4, 12^3x24,
     16^3x32 and 24^3x48, each on its own seeded gauge field (generated on the
     GPU), csw 1.7, kappa 0.1365, Gaussian sources, 1e-10, precision form.
-    All 48 are submitted at once to the solve service, whose workers run
-    them concurrently on separate CUDA streams (the small lattices fill a
-    fraction of the SMs each); a cold pass makes the fields resident, the
-    timed warm pass solves the same requests on resident fields.  The same
-    warm pass with one worker (solves one after another) is the reference
-    point for the overlap."""
+    All 48 are submitted at once to the solve service, run three ways:
+    `workers_N`, N workers solving concurrently on separate CUDA streams
+    (the small lattices fill a fraction of the SMs each); `workers_1`, one
+    after another; `group`, one worker running all 48 as one group solve
+    (qws_b200.group_solve: every kernel step one launch over all lattices at
+    that step).  A cold pass makes the fields resident, the timed warm pass
+    solves the same requests on resident fields."""
     import qws_b200
     from qws_b200 import serve
 
@@ -917,35 +918,49 @@ def bench_uneven(args):
     picks = [vols[int(rng.integers(len(vols)))] for _ in range(48)]
     src = {L: qws_b200.gen_source(L, 77, "gauss") for L in vols}
     out = {"solves": 48, "volumes": {"x".join(map(str, L)): picks.count(L) for L in vols}}
-    for workers in (args.uneven_workers, 1):
+    modes = [(f"workers_{args.uneven_workers}", args.uneven_workers, 1), ("workers_1", 1, 1),
+             ("group", 1, 48)]
+    for name, workers, group in modes:
         svc = serve.Service(serve.seeded_gauge(), budget_bytes=150e9, workers=workers,
-                            max_batch=1)
+                            max_batch=1, group=group)
         try:
             def run():
                 t0 = time.monotonic()
-                reqs = [svc.submit(serve.Request(L=L, gauge=i, kappa=0.1365, csw=1.7, tol=1e-10,
-                                                 source=src[L])) for i, L in enumerate(picks)]
+                reqs = svc.submit_all([serve.Request(L=L, gauge=i, kappa=0.1365, csw=1.7,
+                                                     tol=1e-10, source=src[L])
+                                       for i, L in enumerate(picks)])
                 for q in reqs:
                     q.wait(600)
                 t1 = time.monotonic()
                 st = serve.summarize(reqs, t0, t1)
-                return st, t1 - t0
+                return st, t1 - t0, reqs
 
-            cold, cold_s = run()
-            warm, warm_s = run()
+            cold, cold_s, _ = run()
+            rounds0, launches0 = svc.group_rounds, list(svc.group_launches)
+            phase0 = list(svc.group_phase_s)
+            warm, warm_s, reqs = run()
         finally:
             svc.close()
-        out[f"workers_{workers}"] = {
+        out[name] = {
             "solves_per_s": warm["solves_per_s"], "wall_s": warm_s, "cold_wall_s": cold_s,
             "p50_ms": warm["p50_ms"], "max_true_rel_resid": warm["max_true_rel_resid"],
             "errors": warm["errors"] + cold["errors"], "above_tol": warm["above_tol"]}
-    c, one = out[f"workers_{args.uneven_workers}"], out["workers_1"]
-    out["value"] = c["solves_per_s"]
+        if group > 1:
+            out[name]["group_sizes"] = sorted({q.group for q in reqs if q.error is None})
+            out[name]["host_rounds"] = svc.group_rounds - rounds0
+            out[name]["launches"] = svc.group_launches[0] - launches0[0]
+            out[name]["launches_if_alone"] = svc.group_launches[1] - launches0[1]
+            out[name]["phases_s"] = {k: round(svc.group_phase_s[i] - phase0[i], 4) for i, k in
+                                     enumerate(("setup", "group_solve", "results"))}
+    c, one, g = out[f"workers_{args.uneven_workers}"], out["workers_1"], out["group"]
+    out["value"] = max(c["solves_per_s"], g["solves_per_s"])
     out["unit"] = "solves/s"
     out["speedup_vs_one_at_a_time"] = c["solves_per_s"] / one["solves_per_s"]
+    out["group_vs_streams"] = g["solves_per_s"] / c["solves_per_s"]
     out["method"] = ("qws_b200.serve.Service: one resident field per gauge, clover built on the "
-                     "GPU, bicgstab_dd_mix2_hf per request on the worker's stream; the "
-                     "wall-clock span from submission to the last result")
+                     "GPU, bicgstab_dd_mix2_hf per request (workers_N: on the worker's stream; "
+                     "group: all requests of the pass in one group solve); the wall-clock "
+                     "span from submission to the last result")
     return out
 
 

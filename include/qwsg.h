@@ -194,6 +194,39 @@ int qwsg_bicgstab_dd_mix2_hf(qwsg_lattice* lat, double* x, const double* b, doub
                              double tol_s, int maxiter_s, int nsap, int nm, int reliable,
                              qwsg_solve_stats* stats);
 
+/* ---- group solves: several lattices in common launches ---------------- */
+/* No counterpart in the reference, whose bicgstab_dd_mix2_hf_
+ * (bicgstab_dd_mix2_hf.cc:110) solves one lattice per call.  Each item is
+ * one qwsg_bicgstab_dd_mix2_hf solve on its own one-RHS lattice handle (any
+ * volume, block grid, fields, kappa and solver parameters; every handle at
+ * most once).  The solves run together: each kernel step is one launch over
+ * all lattices at that step, so small lattices share the GPU instead of
+ * paying a launch and a mostly idle GPU each.  Every item's solution and
+ * statistics are those its own qwsg_bicgstab_dd_mix2_hf call gives.  x holds
+ * the initial guess on entry.  Work runs on `stream` (NULL: the first
+ * item's handle's stream) after each handle's own stream is drained.
+ * status: 0 or the error code of that item's solve -- the other items carry
+ * on; the call returns the first non-zero status (qwsg_last_error names the
+ * item).  stats may be NULL. */
+typedef struct {
+  qwsg_lattice* lat;
+  double* x;
+  const double* b;
+  double tol;
+  int maxiter;
+  double tol_s;
+  int maxiter_s, nsap, nm, reliable;
+  qwsg_solve_stats stats; /* out */
+  int status;             /* out */
+} qwsg_group_item;
+typedef struct {
+  long rounds;           /* host read-back points of the group */
+  long merged_launches;  /* kernel launches issued */
+  long member_launches;  /* launches the items' own solves would have issued */
+} qwsg_group_stats;
+int qwsg_group_bicgstab_dd_mix2_hf(qwsg_group_item* items, int n, void* stream,
+                                   qwsg_group_stats* stats);
+
 /* ---- synthetic fields (host, OpenMP; conventions in qws_b200/csrc/fields.cu) */
 /* seeded SU(3) links, n_smear APE-style projected averaging steps with
  * weight alpha; writes the average plaquette (Re tr / 3) to *plaq */

@@ -36,6 +36,21 @@ class SolveStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class GroupItem(ctypes.Structure):
+    _fields_ = [("lat", ctypes.c_void_p), ("x", ctypes.c_void_p), ("b", ctypes.c_void_p),
+                ("tol", ctypes.c_double), ("maxiter", ctypes.c_int), ("tol_s", ctypes.c_double),
+                ("maxiter_s", ctypes.c_int), ("nsap", ctypes.c_int), ("nm", ctypes.c_int),
+                ("reliable", ctypes.c_int), ("stats", SolveStats), ("status", ctypes.c_int)]
+
+
+class GroupStats(ctypes.Structure):
+    _fields_ = [("rounds", ctypes.c_long), ("merged_launches", ctypes.c_long),
+                ("member_launches", ctypes.c_long)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 def load_library(path: str | os.PathLike | None = None):
     """Load libqws_b200.so (build it with `python -m qws_b200.build`)."""
     global _lib
@@ -119,6 +134,8 @@ def load_library(path: str | os.PathLike | None = None):
                                      ctypes.POINTER(c_double)],
         "qwsg_bicgstab_dd_mix2_hf": [vp, vp, vp, c_double, c_int, c_double, c_int, c_int, c_int,
                                      c_int, ctypes.POINTER(SolveStats)],
+        "qwsg_group_bicgstab_dd_mix2_hf": [ctypes.POINTER(GroupItem), c_int, vp,
+                                           ctypes.POINTER(GroupStats)],
         "qwsg_counters": [vp] + [ctypes.POINTER(ctypes.c_long)] * 5,
         "qwsg_kernel_timing": [vp, c_int],
         "qwsg_kernel_stats": [vp, ip, vp, vp, vp],
@@ -184,6 +201,43 @@ def gen_source(L, seed=2, kind="gauss", arg=0):
     k = {"gauss": 0, "point": 1, "z2": 2}[kind]
     _check(lib.qwsg_gen_source(S.ctypes.data_as(ctypes.c_void_p), _L4(L), int(seed), k, int(arg)))
     return S
+
+
+def group_solve(solves, stream=None, check=True):
+    """Solve several lattices together (qwsg_group_bicgstab_dd_mix2_hf): each
+    kernel step is one launch over all of them.  solves: dicts with keys
+    lattice (a one-RHS Lattice), x, b (device tensors; x holds the initial
+    guess), tol, maxiter, tol_s, maxiter_s and optionally nsap (4), nm (2),
+    reliable (0).  Returns (per-solve stats dicts with a 'status' key, group
+    stats).  check: raise on the first failed solve, else report statuses."""
+    lib = load_library()
+    n = len(solves)
+    items = (GroupItem * max(n, 1))()
+    for i, s in enumerate(solves):
+        lat = s["lattice"]
+        if lat.nr != 1:
+            raise QwsgError("group_solve: one-RHS lattices only")
+        items[i].lat = lat.h
+        items[i].x = _ptr(s["x"]).value
+        items[i].b = _ptr(s["b"]).value
+        items[i].tol = float(s["tol"])
+        items[i].maxiter = int(s["maxiter"])
+        items[i].tol_s = float(s["tol_s"])
+        items[i].maxiter_s = int(s["maxiter_s"])
+        items[i].nsap = int(s.get("nsap", 4))
+        items[i].nm = int(s.get("nm", 2))
+        items[i].reliable = int(s.get("reliable", 0))
+    gs = GroupStats()
+    st = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+    rc = lib.qwsg_group_bicgstab_dd_mix2_hf(items, n, st, ctypes.byref(gs))
+    if check:
+        _check(rc)
+    out = []
+    for i in range(n):
+        d = items[i].stats.as_dict()
+        d["status"] = items[i].status
+        out.append(d)
+    return out, gs.as_dict()
 
 
 def launch_count():

@@ -67,7 +67,8 @@ __device__ __forceinline__ void dd_add(double& hi, double& lo, double bhi, doubl
 // block to finish sums every (r, k) over the blocks in block order in
 // double-double and writes res[r*4 + k].
 template <int NR>
-__device__ void finish_reduction(const double (&v)[8], int nr, RedBuf rb, double* res) {
+__device__ void finish_reduction(const double (&v)[8], int nr, const RedBuf& rb, double* res,
+                                 int blk, int nblk) {
   __shared__ double sh[kThreads / 32][32][NR > 0 ? NR : 1];
   __shared__ bool last;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -83,14 +84,14 @@ __device__ void finish_reduction(const double (&v)[8], int nr, RedBuf rb, double
     for (int k = 0; k < NR; k++) {
       double x = 0;
       for (int w = 0; w < kThreads / 32; w++) x += sh[w][threadIdx.x][k];
-      rb.partial[((size_t)blockIdx.x * 32 + threadIdx.x) * 4 + k] = x;
+      rb.partial[((size_t)blk * 32 + threadIdx.x) * 4 + k] = x;
     }
     __threadfence();
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned done = atomicAdd(rb.counter, 1u);
-    last = (done == gridDim.x - 1);
+    last = (done == (unsigned)nblk - 1);
   }
   __syncthreads();
   if (!last) return;
@@ -98,7 +99,7 @@ __device__ void finish_reduction(const double (&v)[8], int nr, RedBuf rb, double
   for (int pr = warp; pr < nr * NR; pr += kThreads / 32) {
     const int r = pr / NR, k = pr - r * NR;
     double hi = 0, lo = 0;
-    for (int b = lane; b < (int)gridDim.x; b += 32) {
+    for (int b = lane; b < nblk; b += 32) {
       double x = *((volatile double*)&rb.partial[((size_t)b * 32 + r) * 4 + k]);
       dd_add(hi, lo, x, 0.0);
     }
@@ -122,15 +123,40 @@ __device__ __forceinline__ R coef(const double* cf, int r, int k, R v) {
 
 // ---- per-site operations ---------------------------------------------------
 // every (site, rhs) entry; op(G, entry, rhs, acc)
-template <typename R, int NR, typename Op>
-__global__ void __launch_bounds__(kThreads) k_sites(Geom G, Op op, RedBuf rb, double* res) {
+// block blk of nblk (grid stride nblk * kThreads)
+template <int NR, typename Op>
+__device__ __forceinline__ void sites_body(const Geom& G, const Op& op, const RedBuf& rb,
+                                           double* res, int blk, int nblk) {
   double acc[8];
 #pragma unroll
   for (int k = 0; k < 8; k++) acc[k] = 0;
   const int n = G.V << G.lgnr;
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x)
+  for (int e = blk * kThreads + threadIdx.x; e < n; e += nblk * kThreads)
     op(G, e, e & (G.nr - 1), acc);
-  if constexpr (NR > 0) finish_reduction<NR>(acc, G.nr, rb, res);
+  if constexpr (NR > 0) finish_reduction<NR>(acc, G.nr, rb, res, blk, nblk);
+}
+template <typename R, int NR, typename Op>
+__global__ void __launch_bounds__(kThreads) k_sites(Geom G, Op op, RedBuf rb, double* res) {
+  sites_body<NR>(G, op, rb, res, blockIdx.x, gridDim.x);
+}
+
+// one launch over several lattices (group solves): each member runs the
+// blocks of its own launch -- the same grid stride, partials and final sum,
+// so its results are those of its own launch
+template <typename Op>
+struct SitesArgs {
+  Geom G;
+  Op op;
+  RedBuf rb;
+  double* res;
+};
+template <typename R, int NR, typename Op>
+__global__ void __launch_bounds__(kThreads)
+    k_sites_multi(const SitesArgs<Op>* __restrict__ args, const int* __restrict__ starts, int n) {
+  __shared__ SitesArgs<Op> sa;
+  const int l = group_member(starts, n, blockIdx.x);
+  group_load_args(sa, args + l);
+  sites_body<NR>(sa.G, sa.op, sa.rb, sa.res, blockIdx.x - starts[l], starts[l + 1] - starts[l]);
 }
 
 template <typename R>
@@ -370,8 +396,8 @@ __device__ __forceinline__ float2 cdivf(float2 a, float2 b) {
 }
 __device__ __forceinline__ float cabsf2(float2 a) { return hypotf(a.x, a.y); }
 
-__global__ void k_inner_scalars(InnerScalars* s, const double* __restrict__ res, int phase,
-                                double tol) {
+__device__ void inner_scalars_body(InnerScalars* s, const double* __restrict__ res, int phase,
+                                   double tol) {
   const bool done = s->done != 0;
   switch (phase) {
     case 0: {
@@ -447,15 +473,58 @@ __global__ void k_inner_scalars(InnerScalars* s, const double* __restrict__ res,
   }
 }
 
+__global__ void k_inner_scalars(InnerScalars* s, const double* __restrict__ res, int phase,
+                                double tol) {
+  inner_scalars_body(s, res, phase, tol);
+}
+struct InnerScalarsArgs {
+  InnerScalars* s;
+  const double* res;
+  double tol;
+  int phase;
+  int pad_;
+};
+__global__ void k_inner_scalars_multi(const InnerScalarsArgs* __restrict__ a, int n) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l < n) inner_scalars_body(a[l].s, a[l].res, a[l].phase, a[l].tol);
+}
+
 int grid_for(const Geom& G, const RedBuf* rb) {
   int b = ((G.V << G.lgnr) + kThreads - 1) / kThreads;
   int cap = rb ? rb->nblk : 148 * 8;
   return b < cap ? b : cap;
 }
 
+// merge one per-site launch of each group member (each with the block
+// count of its own launch)
+template <typename R, int NR, typename Op>
+void merge_sites(const GroupRec* const* recs, int n, GroupBatch& b) {
+  std::vector<SitesArgs<Op>> args(n);
+  std::vector<int> starts(n + 1);
+  int blocks = 0;
+  for (int l = 0; l < n; l++) {
+    args[l] = group_arg<SitesArgs<Op>>(recs[l]);
+    starts[l] = blocks;
+    blocks += grid_for(args[l].G, args[l].rb.partial ? &args[l].rb : nullptr);
+  }
+  starts[n] = blocks;
+  const size_t oa = b.put(args.data(), sizeof(SitesArgs<Op>) * n), os = b.put_starts(starts);
+  b.launches.push_back([=](const unsigned char* dev, cudaStream_t st) {
+    count_launch();
+    k_sites_multi<R, NR, Op><<<blocks, kThreads, 0, st>>>(
+        reinterpret_cast<const SitesArgs<Op>*>(dev + oa), reinterpret_cast<const int*>(dev + os),
+        n);
+  });
+}
+
 template <typename R, int NR, typename Op>
 void run(const Geom& G, Op op, RedBuf* rb, double* res, cudaStream_t st) {
   RedBuf dummy{nullptr, nullptr, 0};
+  if (g_group_rec) {
+    if (G.nr != 1) group_unrecorded_launch();
+    group_record(&merge_sites<R, NR, Op>, SitesArgs<Op>{G, op, rb ? *rb : dummy, res});
+    return;
+  }
   count_launch();
   k_sites<R, NR, Op><<<grid_for(G, rb), kThreads, 0, st>>>(G, op, rb ? *rb : dummy, res);
 }
@@ -478,11 +547,67 @@ __global__ void k_zero(Geom G, R* y, int e0, int n) {
   for (int j = 0; j < 6; j++) st4<R>(y, sp, e, j, {0, 0, 0, 0});
 }
 
+// copy (x set) or zero (x null) of entries [e0, e0 + n) for several lattices
+template <typename R>
+struct CopyArgs {
+  Geom G;
+  R* y;
+  const R* x;
+  int e0, n;
+};
+template <typename R>
+__global__ void k_copy_multi(const CopyArgs<R>* __restrict__ args, const int* __restrict__ starts,
+                             int n) {
+  __shared__ CopyArgs<R> sa;
+  const int l = group_member(starts, n, blockIdx.x);
+  group_load_args(sa, args + l);
+  const int i = (blockIdx.x - starts[l]) * blockDim.x + threadIdx.x;
+  if (i >= sa.n) return;
+  const int e = sa.e0 + i, sp = spad(sa.G);
+  if (sa.x) {
+#pragma unroll
+    for (int j = 0; j < 6; j++) st4<R>(sa.y, sp, e, j, ld4<R>(sa.x, sp, e, j));
+  } else {
+#pragma unroll
+    for (int j = 0; j < 6; j++) st4<R>(sa.y, sp, e, j, {0, 0, 0, 0});
+  }
+}
+template <typename R>
+void merge_copy(const GroupRec* const* recs, int n, GroupBatch& b) {
+  std::vector<CopyArgs<R>> args(n);
+  std::vector<int> starts(n + 1);
+  int blocks = 0;
+  for (int l = 0; l < n; l++) {
+    args[l] = group_arg<CopyArgs<R>>(recs[l]);
+    starts[l] = blocks;
+    blocks += (args[l].n + 255) / 256;
+  }
+  starts[n] = blocks;
+  if (blocks == 0) return;
+  const size_t oa = b.put(args.data(), sizeof(CopyArgs<R>) * n), os = b.put_starts(starts);
+  b.launches.push_back([=](const unsigned char* dev, cudaStream_t st) {
+    count_launch();
+    k_copy_multi<R><<<blocks, 256, 0, st>>>(reinterpret_cast<const CopyArgs<R>*>(dev + oa),
+                                            reinterpret_cast<const int*>(dev + os), n);
+  });
+}
+void merge_inner_scalars(const GroupRec* const* recs, int n, GroupBatch& b) {
+  std::vector<InnerScalarsArgs> args(n);
+  for (int l = 0; l < n; l++) args[l] = group_arg<InnerScalarsArgs>(recs[l]);
+  const size_t oa = b.put(args.data(), sizeof(InnerScalarsArgs) * n);
+  b.launches.push_back([=](const unsigned char* dev, cudaStream_t st) {
+    count_launch();
+    k_inner_scalars_multi<<<(n + 31) / 32, 32, 0, st>>>(
+        reinterpret_cast<const InnerScalarsArgs*>(dev + oa), n);
+  });
+}
+
 }  // namespace
 
 template <typename R>
 void blas_copy(const Geom& G, R* y, const R* x, int site0, int n, cudaStream_t st) {
   const int ne = n << G.lgnr;
+  if (group_record(&merge_copy<R>, CopyArgs<R>{G, y, x, site0 << G.lgnr, ne})) return;
   if (ne > 0) {
     count_launch();
     k_copy<R><<<(ne + 255) / 256, 256, 0, st>>>(G, y, x, site0 << G.lgnr, ne);
@@ -491,6 +616,7 @@ void blas_copy(const Geom& G, R* y, const R* x, int site0, int n, cudaStream_t s
 template <typename R>
 void blas_zero(const Geom& G, R* y, int site0, int n, cudaStream_t st) {
   const int ne = n << G.lgnr;
+  if (group_record(&merge_copy<R>, CopyArgs<R>{G, y, nullptr, site0 << G.lgnr, ne})) return;
   if (ne > 0) {
     count_launch();
     k_zero<R><<<(ne + 255) / 256, 256, 0, st>>>(G, y, site0 << G.lgnr, ne);
@@ -548,6 +674,7 @@ void blas_s2d(const Geom& G, double* y, const float* x, double s, cudaStream_t s
 }
 
 void inner_scalars(InnerScalars* s, const double* res, int phase, double tol, cudaStream_t st) {
+  if (group_record(&merge_inner_scalars, InnerScalarsArgs{s, res, tol, phase, 0})) return;
   count_launch();
   k_inner_scalars<<<1, 1, 0, st>>>(s, res, phase, tol);
 }

@@ -704,6 +704,47 @@ int qwsg_bicgstab_dd_mix2_hf(qwsg_lattice* l, double* x, const double* b, double
     if (st) copy_stats(s, st);
   });
 }
+int qwsg_group_bicgstab_dd_mix2_hf(qwsg_group_item* items, int n, void* stream,
+                                   qwsg_group_stats* gst) {
+  return guarded([&] {
+    if (n < 0 || (n > 0 && !items)) throw Error(1, "group solve: no items");
+    if (n == 0) return;
+    std::vector<GroupItem> v(n);
+    for (int i = 0; i < n; i++) {
+      qwsg_group_item& it = items[i];
+      check_ctx(it.lat);
+      need_fields(*it.lat->c, true);
+      need_fields(*it.lat->c, false);
+      if (!it.x || !it.b) throw Error(1, "group solve: x and b must be set");
+      v[i] = GroupItem{it.lat->c, it.x, it.b, it.tol, it.maxiter, it.tol_s, it.maxiter_s,
+                       it.nsap, it.nm, it.reliable, SolveStats{}, -1, std::string()};
+    }
+    cudaStream_t st = stream ? (cudaStream_t)stream : v[0].c->st;
+    GroupStats gs{};
+    std::string first_error;
+    try {
+      group_bicgstab_dd_mix2_hf(v, st, &gs);
+    } catch (...) {
+      for (int i = 0; i < n; i++) items[i].status = v[i].status < 0 ? 3 : v[i].status;
+      throw;
+    }
+    int code = 0;
+    for (int i = 0; i < n; i++) {
+      items[i].status = v[i].status;
+      copy_stats(v[i].stats, &items[i].stats);
+      if (v[i].status != 0 && code == 0) {
+        code = v[i].status;
+        first_error = "group solve, item " + std::to_string(i) + ": " + v[i].error;
+      }
+    }
+    if (gst) {
+      gst->rounds = gs.rounds;
+      gst->merged_launches = gs.merged_launches;
+      gst->member_launches = gs.member_launches;
+    }
+    if (code) throw Error(code, first_error);
+  });
+}
 int qwsg_set_parities(qwsg_lattice* l, int pce, int pco) {
   return guarded([&] {
     check_ctx(l);

@@ -217,34 +217,77 @@ __global__ void k_nat2pl_clover(Geom G, R* dst, const Rin* __restrict__ nat) {
 inline int nb(long n) { return (int)((n + 127) / 128); }
 
 // spinor precision conversions: one thread per (site, rhs) entry
-__global__ void k_s2h(Geom G, __half* dst, const float* __restrict__ src) {
-  int e = blockIdx.x * blockDim.x + threadIdx.x;
+enum { CONV_S2H = 0, CONV_H2S = 1, CONV_H2H = 2 };
+template <int K>
+__device__ __forceinline__ void conv_entry(const Geom& G, void* dst, const void* src, int e) {
   if (e >= (G.V << G.lgnr)) return;
   const int sp = spad(G);
-  float v[24];
-  IO<float>::load_spinor(src, sp, e, v);
-  IO<H16>::store_spinor(dst, sp, e, v);
-}
-
-__global__ void k_h2s(Geom G, float* dst, const __half* __restrict__ src) {
-  int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (G.V << G.lgnr)) return;
-  const int sp = spad(G);
-  float v[24];
-  IO<H16>::load_spinor(src, sp, e, v);
-  IO<float>::store_spinor(dst, sp, e, v);
-}
-
-__global__ void k_h2h(Geom G, __half* dst, const __half* __restrict__ src) {
-  int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (G.V << G.lgnr)) return;
-  const size_t sp = spad(G);
-  // the IO<H16> spinor layout: three 16-byte planes, then the scale plane
-  const uint4* s = reinterpret_cast<const uint4*>(src);
-  uint4* d = reinterpret_cast<uint4*>(dst);
+  if (K == CONV_S2H) {
+    float v[24];
+    IO<float>::load_spinor(static_cast<const float*>(src), sp, e, v);
+    IO<H16>::store_spinor(static_cast<__half*>(dst), sp, e, v);
+  } else if (K == CONV_H2S) {
+    float v[24];
+    IO<H16>::load_spinor(static_cast<const __half*>(src), sp, e, v);
+    IO<float>::store_spinor(static_cast<float*>(dst), sp, e, v);
+  } else {
+    // the IO<H16> spinor layout: three 16-byte planes, then the scale plane
+    const size_t p = sp;
+    const uint4* s = static_cast<const uint4*>(src);
+    uint4* d = static_cast<uint4*>(dst);
 #pragma unroll
-  for (int j = 0; j < 3; j++) d[j * sp + e] = s[j * sp + e];
-  reinterpret_cast<float*>(d + 3 * sp)[e] = reinterpret_cast<const float*>(s + 3 * sp)[e];
+    for (int j = 0; j < 3; j++) d[j * p + e] = s[j * p + e];
+    reinterpret_cast<float*>(d + 3 * p)[e] = reinterpret_cast<const float*>(s + 3 * p)[e];
+  }
+}
+__global__ void k_s2h(Geom G, __half* dst, const float* __restrict__ src) {
+  conv_entry<CONV_S2H>(G, dst, src, blockIdx.x * blockDim.x + threadIdx.x);
+}
+__global__ void k_h2s(Geom G, float* dst, const __half* __restrict__ src) {
+  conv_entry<CONV_H2S>(G, dst, src, blockIdx.x * blockDim.x + threadIdx.x);
+}
+__global__ void k_h2h(Geom G, __half* dst, const __half* __restrict__ src) {
+  conv_entry<CONV_H2H>(G, dst, src, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// the same conversions for several lattices in one launch (group solves;
+// one RHS each)
+struct ConvArgs {
+  Geom G;
+  void* dst;
+  const void* src;
+};
+template <int K>
+__global__ void k_conv_multi(const ConvArgs* __restrict__ args, const int* __restrict__ starts,
+                             int n) {
+  __shared__ ConvArgs sa;
+  const int l = group_member(starts, n, blockIdx.x);
+  group_load_args(sa, args + l);
+  conv_entry<K>(sa.G, sa.dst, sa.src, (blockIdx.x - starts[l]) * blockDim.x + threadIdx.x);
+}
+template <int K>
+void merge_conv(const GroupRec* const* recs, int n, GroupBatch& b) {
+  std::vector<ConvArgs> args(n);
+  std::vector<int> starts(n + 1);
+  int blocks = 0;
+  for (int l = 0; l < n; l++) {
+    args[l] = group_arg<ConvArgs>(recs[l]);
+    starts[l] = blocks;
+    blocks += (args[l].G.V + 127) / 128;
+  }
+  starts[n] = blocks;
+  const size_t oa = b.put(args.data(), sizeof(ConvArgs) * n), os = b.put_starts(starts);
+  b.launches.push_back([=](const unsigned char* dev, cudaStream_t st) {
+    count_launch();
+    k_conv_multi<K><<<blocks, 128, 0, st>>>(reinterpret_cast<const ConvArgs*>(dev + oa),
+                                            reinterpret_cast<const int*>(dev + os), n);
+  });
+}
+template <int K>
+bool record_conv(const Geom& G, void* dst, const void* src) {
+  if (!g_group_rec) return false;
+  if (G.nr != 1) group_unrecorded_launch();
+  return group_record(&merge_conv<K>, ConvArgs{G, dst, src});
 }
 
 // the same three conversions for FP16 fields of two or more RHS (IOP
@@ -387,6 +430,7 @@ void links_compress12(const Geom& G, float* U12, const float* Us, cudaStream_t s
 // FP16 spinors of one RHS use IO<H16>, of two or more the IOP layout of the
 // paired hop kernels
 void spinor_s2h(const Geom& G, __half* dst, const float* src, cudaStream_t st) {
+  if (record_conv<CONV_S2H>(G, dst, src)) return;
   count_launch();
   if (G.nr >= 2)
     k_s2h_pair<<<nb(G.V << (G.lgnr - 1)), 128, 0, st>>>(G, dst, src);
@@ -394,6 +438,7 @@ void spinor_s2h(const Geom& G, __half* dst, const float* src, cudaStream_t st) {
     k_s2h<<<nb(G.V), 128, 0, st>>>(G, dst, src);
 }
 void spinor_h2s(const Geom& G, float* dst, const __half* src, cudaStream_t st) {
+  if (record_conv<CONV_H2S>(G, dst, src)) return;
   count_launch();
   if (G.nr >= 2)
     k_h2s_pair<<<nb(G.V << (G.lgnr - 1)), 128, 0, st>>>(G, dst, src);
@@ -401,6 +446,7 @@ void spinor_h2s(const Geom& G, float* dst, const __half* src, cudaStream_t st) {
     k_h2s<<<nb(G.V), 128, 0, st>>>(G, dst, src);
 }
 void spinor_h2h(const Geom& G, __half* dst, const __half* src, cudaStream_t st) {
+  if (record_conv<CONV_H2H>(G, dst, src)) return;
   count_launch();
   if (G.nr >= 2)
     k_h2h_pair<<<nb(G.V << (G.lgnr - 1)), 128, 0, st>>>(G, dst, src);

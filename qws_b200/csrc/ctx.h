@@ -23,6 +23,8 @@ struct Error : std::runtime_error {
       throw ::qwsg::Error(3, std::string(#call) + ": " + cudaGetErrorString(e_));           \
   } while (0)
 
+struct GroupMember;
+
 struct SolveStats {
   int outer_iters = 0;
   long inner_iters = 0;
@@ -209,6 +211,10 @@ struct Ctx {
   bool use_graphs = true;
   long n_graph_launches = 0;
   void clear_graphs();
+
+  // set while this lattice takes part in a group solve (group.cu): its
+  // read-backs wait for the group's merged launches
+  GroupMember* gm = nullptr;
 };
 
 // kernel kinds for timing
@@ -269,6 +275,31 @@ void bicgstab_dd_mix(Ctx& c, double* x, const double* b, double tol, int maxiter
                      int maxiter_s, int nsap, int nm, SolveStats* stats, double* hist,
                      int hist_len);
 double true_residual(Ctx& c, const double* x, const double* b);
+
+// group solve (group.cu): bicgstab_dd_mix2_hf on each item's lattice (one
+// RHS, one kappa each; any volumes, block grids and solver parameters), with
+// the kernels of all of them merged into common launches on stream st.
+// status: 0, or the error code of that lattice's solve (error: its message);
+// the other lattices carry on.  Throws only on a failure of the group itself.
+struct GroupItem {
+  Ctx* c;
+  double* x;  // initial guess in, solution out (device planes)
+  const double* b;
+  double tol;
+  int maxiter;
+  double tol_s;
+  int maxiter_s, nsap, nm, reliable;
+  SolveStats stats;
+  int status;
+  std::string error;
+};
+struct GroupStats {
+  long rounds;           // read-back points of the group (host synchronisations)
+  long merged_launches;  // launches issued
+  long member_launches;  // launches the lattices' own solves would have issued
+};
+void group_bicgstab_dd_mix2_hf(std::vector<GroupItem>& items, cudaStream_t st, GroupStats* gs);
+void group_park(GroupMember& me, const void* dev, void* host, size_t bytes);
 
 // multi-RHS forms (solver_mrhs.cu) on a context with G.nr right-hand sides:
 // per-RHS scalars and convergence, one launch per operator for all RHS.

@@ -174,9 +174,8 @@ struct MinCtas {
 };
 
 template <typename T, typename P, int SEL, int EPI, bool PRK>
-__device__ __forceinline__ void hop_site(const HopArgs<T>& a) {
+__device__ __forceinline__ void hop_site_at(const HopArgs<T>& a, const int i) {
   using V = typename P::V;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int ll = P::lanes_log(a.G);
   if (i >= (a.nsites << ll)) return;
   // consecutive threads: the right-hand sides (or RHS pairs) of one site,
@@ -230,6 +229,11 @@ __device__ __forceinline__ void hop_site(const HopArgs<T>& a) {
   P::store(a.out, pd, e, o);
 }
 
+template <typename T, typename P, int SEL, int EPI, bool PRK>
+__device__ __forceinline__ void hop_site(const HopArgs<T>& a) {
+  hop_site_at<T, P, SEL, EPI, PRK>(a, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // the same body with and without the 64-register bound (an explicit
 // minimum of one CTA per SM would let the compiler spend every register)
 // PRK: per-RHS kappa (clover planes and kappa per RHS, multi-RHS handles only)
@@ -246,6 +250,30 @@ __global__ void __launch_bounds__(256, 4) k_hop_r64(const HopArgs<T> a) {
 template <int SEL, int EPI, bool PRK>
 __global__ void __launch_bounds__(256) k_hop_pair(const HopArgs<H16> a) {
   hop_site<H16, TwoRhs, SEL, EPI, PRK>(a);
+}
+
+// Several lattices in one launch (a group solve; one right-hand side each):
+// block b runs threads [(b - starts[l]) * blockDim, ...) of member l's own
+// launch, with l's arguments copied into shared memory first, so every
+// member runs exactly the code and arithmetic of its own launch.
+template <typename T, int SEL, int EPI>
+__device__ __forceinline__ void hop_multi_body(const HopArgs<T>* __restrict__ args,
+                                               const int* __restrict__ starts, int n) {
+  __shared__ HopArgs<T> sa;
+  const int l = group_member(starts, n, blockIdx.x);
+  group_load_args(sa, args + l);
+  hop_site_at<T, OneRhs<T>, SEL, EPI, false>(sa, (blockIdx.x - starts[l]) * blockDim.x +
+                                                     threadIdx.x);
+}
+template <typename T, int SEL, int EPI>
+__global__ void __launch_bounds__(256) k_hop_multi(const HopArgs<T>* __restrict__ args,
+                                                   const int* __restrict__ starts, int n) {
+  hop_multi_body<T, SEL, EPI>(args, starts, n);
+}
+template <typename T, int SEL, int EPI>
+__global__ void __launch_bounds__(256, 4) k_hop_multi_r64(const HopArgs<T>* __restrict__ args,
+                                                          const int* __restrict__ starts, int n) {
+  hop_multi_body<T, SEL, EPI>(args, starts, n);
 }
 
 template <typename T, int SEL, int EPI, bool PRK>
@@ -275,8 +303,51 @@ static void launch(const HopArgs<T>& a, cudaStream_t st) {
     launch_v<T, SEL, EPI, false>(a, st);
 }
 
+// merge one hop launch of each group member: 128-thread blocks (a thread's
+// work does not depend on the CTA size), each member's sites in its own
+// blocks; the FP16 block kernels keep their 64-register bound (the FP32
+// ones would spill in the multi-lattice form)
+template <typename T, int SEL, int EPI>
+static void merge_hop(const GroupRec* const* recs, int n, GroupBatch& b) {
+  constexpr int threads = 128;
+  std::vector<HopArgs<T>> args(n);
+  std::vector<int> starts(n + 1);
+  int blocks = 0;
+  for (int l = 0; l < n; l++) {
+    args[l] = group_arg<HopArgs<T>>(recs[l]);
+    starts[l] = blocks;
+    blocks += args[l].nsites > 0 ? (args[l].nsites + threads - 1) / threads : 0;
+  }
+  starts[n] = blocks;
+  if (blocks == 0) return;
+  const size_t oa = b.put(args.data(), sizeof(HopArgs<T>) * n), os = b.put_starts(starts);
+  b.launches.push_back([=](const unsigned char* dev, cudaStream_t st) {
+    count_launch();
+    const auto* A = reinterpret_cast<const HopArgs<T>*>(dev + oa);
+    const auto* S = reinterpret_cast<const int*>(dev + os);
+    if constexpr (std::is_same<T, H16>::value && MinCtas<T, SEL>::value == 4)
+      k_hop_multi_r64<T, SEL, EPI><<<blocks, threads, 0, st>>>(A, S, n);
+    else
+      k_hop_multi<T, SEL, EPI><<<blocks, threads, 0, st>>>(A, S, n);
+  });
+}
+
 template <typename T>
 void launch_hop(int sel, int epi, const HopArgs<T>& a, cudaStream_t st) {
+  if (g_group_rec) {  // a group solve: one right-hand side, one kappa per lattice
+    if (a.G.nr != 1 || (a.Cr && a.kap)) group_unrecorded_launch();
+#define QWSG_CASE(S, E)                           \
+  if (sel == S && epi == E) {                     \
+    group_record(&merge_hop<T, S, E>, a);         \
+    return;                                       \
+  }
+    QWSG_CASE(HOP_ALL, EPI_D)
+    QWSG_CASE(HOP_INNER, EPI_D)
+    QWSG_CASE(HOP_OUTER, EPI_ADD)
+    QWSG_CASE(HOP_INNER, EPI_JINV)
+    QWSG_CASE(HOP_INNER, EPI_SAPE)
+#undef QWSG_CASE
+  }
 #define QWSG_CASE(S, E)              \
   if (sel == S && epi == E) {        \
     launch<T, S, E>(a, st);          \

@@ -4,15 +4,101 @@
 
 #include <atomic>
 #include <cstddef>
+#include <cstring>
+#include <functional>
+#include <vector>
 
 #include "lattice.cuh"
 
 namespace qwsg {
 
+// ---------------------------------------------------------------------------
+// Group solves (group.cu): several lattices, each solved by its own host
+// thread running the unchanged one-lattice solver, with every kernel launch
+// recorded instead of issued.  At each point where a solver reads a result
+// back, the launches the lattices recorded since their last read-back are
+// merged position by position into one launch over all of them.  A record
+// holds the launch's argument block and the function that merges it.
+// ---------------------------------------------------------------------------
+struct GroupRec;
+struct GroupBatch;
+using GroupMergeFn = void (*)(const GroupRec* const* recs, int n, GroupBatch& b);
+struct GroupRec {
+  GroupMergeFn merge;  // also the launch's identity: the same function merges
+  alignas(16) unsigned char data[512];
+};
+struct GroupRecorder {
+  std::vector<GroupRec> recs;
+};
+// the recorder of the calling thread (null outside a group solve)
+extern thread_local GroupRecorder* g_group_rec;
+template <typename A>
+inline bool group_record(GroupMergeFn f, const A& a) {
+  static_assert(sizeof(A) <= sizeof(GroupRec::data), "group record too large");
+  if (!g_group_rec) return false;
+  g_group_rec->recs.emplace_back();
+  GroupRec& r = g_group_rec->recs.back();
+  r.merge = f;
+  std::memcpy(r.data, &a, sizeof(A));
+  return true;
+}
+template <typename A>
+inline const A& group_arg(const GroupRec* r) {
+  return *reinterpret_cast<const A*>(r->data);
+}
+// One round's merged launches: argument tables staged on the host, uploaded
+// in one copy, then the launches run with the device address of the copy.
+struct GroupBatch {
+  std::vector<unsigned char> host;
+  std::vector<std::function<void(const unsigned char* dev, cudaStream_t st)>> launches;
+  size_t put(const void* p, size_t n) {  // 16-byte aligned offset of the copy
+    const size_t off = (host.size() + 15) & ~size_t(15);
+    host.resize(off + n);
+    std::memcpy(host.data() + off, p, n);
+    return off;
+  }
+  // block starts of a merged launch: starts[l] = first block of member l,
+  // starts[n] = the total; returns the offset of the table
+  size_t put_starts(const std::vector<int>& starts) {
+    return put(starts.data(), sizeof(int) * starts.size());
+  }
+};
+[[noreturn]] void group_unrecorded_launch();
+
 // kernels launched by this library in this process (host-side count; a CUDA
-// graph replay adds the launches it captured)
+// graph replay adds the launches it captured).  Every launcher counts its
+// launch; one reached while the thread records for a group solve is a launch
+// the group cannot merge, which is an error.
 extern std::atomic<long> g_kernel_launches;
-inline void count_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
+inline void count_launch() {
+  if (g_group_rec) group_unrecorded_launch();
+  g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
+
+#ifdef __CUDACC__
+// the member whose blocks include block b of a merged launch: the largest l
+// with starts[l] <= b (members without blocks have starts[l] == starts[l+1])
+__device__ __forceinline__ int group_member(const int* __restrict__ starts, int n, int b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(starts + mid) <= b)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+// copy a member's argument block into shared memory (all threads take part)
+template <typename A>
+__device__ __forceinline__ void group_load_args(A& dst, const A* __restrict__ src) {
+  static_assert(sizeof(A) % sizeof(int) == 0, "argument block size");
+  const int* s = reinterpret_cast<const int*>(src);
+  int* d = reinterpret_cast<int*>(&dst);
+  for (int k = threadIdx.x; k < (int)(sizeof(A) / sizeof(int)); k += blockDim.x) d[k] = s[k];
+  __syncthreads();
+}
+#endif
 
 enum { HOP_INNER = 1, HOP_OUTER = 2, HOP_ALL = 3 };
 enum { EPI_D = 0, EPI_ADD = 1, EPI_JINV = 2, EPI_SAPE = 3 };

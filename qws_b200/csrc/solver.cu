@@ -456,12 +456,20 @@ void Ctx::ensure_fields_h() {
 }
 
 const InnerScalars* Ctx::fetch_inner() {
+  if (gm) {
+    group_park(*gm, d_isc, h_isc, sizeof(InnerScalars));
+    return h_isc;
+  }
   QWSG_CUDA(cudaMemcpyAsync(h_isc, d_isc, sizeof(InnerScalars), cudaMemcpyDeviceToHost, st));
   QWSG_CUDA(cudaStreamSynchronize(st));
   return h_isc;
 }
 
 const double* Ctx::fetch(int n) {
+  if (gm) {
+    group_park(*gm, d_res, h_res, sizeof(double) * n);
+    return h_res;
+  }
   QWSG_CUDA(cudaMemcpyAsync(h_res, d_res, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
   QWSG_CUDA(cudaStreamSynchronize(st));
   return h_res;
@@ -651,8 +659,9 @@ static void graphed(Ctx& c, const Ctx::GraphKey& k, F&& body) {
   // the link form is settled before a capture (its check reads back a result)
   // and a change of form drops the graphs captured with the other one
   c.ensure_links12();
+  // (a group solve records the launches one by one to merge them)
   if (c.timing || !c.use_graphs || c.st == nullptr || c.st == cudaStreamLegacy ||
-      c.st == cudaStreamPerThread) {
+      c.st == cudaStreamPerThread || g_group_rec) {
     body();
     return;
   }

@@ -114,6 +114,7 @@ class Request:
     t_clover: float = 0.0
     t_solve: float = 0.0
     batch: int = 0
+    group: int = 0                # requests in the group solve that ran it (1: alone)
     error: str | None = None
     done: threading.Event = field(default_factory=threading.Event)
 
@@ -205,8 +206,18 @@ class Service:
 
     def __init__(self, gauge_source, budget_bytes=150e9, workers=3, max_batch=16,
                  block_grid=None, maxiter=100, tol_s=1e-6, maxiter_s=50, nsap=None, nm=None,
-                 reliable=5, graphs=True, lifo_after_s=None):
+                 reliable=5, graphs=True, lifo_after_s=None, group=1):
         self.gauge_source = gauge_source
+        # group > 1: a worker takes up to this many one-request jobs (any
+        # volumes) at once and runs them as one group solve, every kernel
+        # step one launch over all of them (qws_b200.group_solve); merging
+        # into multi-RHS solves is then off (max_batch 1)
+        self.group = max(1, int(group))
+        if self.group > 1:
+            max_batch = 1
+        self.group_rounds = 0
+        self.group_launches = [0, 0]  # launches issued, launches the solves alone would issue
+        self.group_phase_s = [0.0, 0.0, 0.0]  # jobs' set-up, group solve, jobs' results
         # adaptive LIFO: once the oldest pending request has waited longer
         # than this (s), the newest pending requests are served first -- under
         # overload the oldest are the ones a deadline sheds, and serving them
@@ -265,6 +276,17 @@ class Service:
             self.pending.append(req)
             self.cv.notify_all()
         return req
+
+    def submit_all(self, reqs) -> list:
+        """Submit several requests at once: the scheduler sees them together
+        (a group service then starts them as one group)."""
+        with self.cv:
+            for req in reqs:
+                req.rid = next(self.ids)
+                req.t_arrival = time.monotonic()
+                self.pending.append(req)
+            self.cv.notify_all()
+        return list(reqs)
 
     def cancel(self, req: Request) -> bool:
         """Withdraw a request that has not started: it finishes at once with
@@ -397,6 +419,21 @@ class Service:
             return res, group
         return None
 
+    def _next_job(self):
+        """The next job for an idle worker: (resident, requests), or with
+        group > 1 a list of every such job that can start now, up to `group`
+        of them, for one group solve.  Called with cv held."""
+        job = self._pick()
+        if job is None or self.group <= 1:
+            return job
+        jobs = [job]
+        while len(jobs) < self.group and self.pending:
+            j = self._pick()
+            if j is None:
+                break
+            jobs.append(j)
+        return jobs
+
     def _scheduler(self):
         with self.cv:
             while True:
@@ -404,7 +441,7 @@ class Service:
                     return
                 if self.idle_workers == 0:
                     self._expire()
-                job = self._pick() if self.idle_workers > 0 and self.pending else None
+                job = self._next_job() if self.idle_workers > 0 and self.pending else None
                 if job is None:
                     self.cv.wait(0.02)
                     continue
@@ -417,27 +454,98 @@ class Service:
             job = self.jobs.get()
             if job is None:
                 return
-            res, group = job
+            jobs = job if isinstance(job, list) else [job]
             try:
-                self._run(res, group)
+                if isinstance(job, list):
+                    self._run_group(jobs)
+                else:
+                    self._run(*job)
             except Exception as e:  # reported on the requests, the service goes on
-                for q in group:
-                    q.error = f"{type(e).__name__}: {e}"
-                    q.t_done = time.monotonic()
+                for _, group in jobs:
+                    for q in group:
+                        if q.t_done == 0.0:
+                            q.error = f"{type(e).__name__}: {e}"
+                            q.t_done = time.monotonic()
             with self.cv:
-                live = self.residents.get((res.L, res.gid))
-                if live is not None:
-                    live.busy = False
-                    live.last_used = time.monotonic()
-                for q in group:
-                    self.completed.append(q)
-                    q.done.set()
+                for res, group in jobs:
+                    live = self.residents.get((res.L, res.gid))
+                    if live is not None:
+                        live.busy = False
+                        live.last_used = time.monotonic()
+                    for q in group:
+                        self.completed.append(q)
+                        q.done.set()
                 self.idle_workers += 1
                 self.cv.notify_all()
 
     def _run(self, res, group):
+        p = self._stage(res, group)
+        s = self.solver
+        with self._torch.cuda.stream(p["res"].stream):
+            p["stats"] = p["B"].bicgstab_dd_mix2_hf(
+                p["xd"], p["bd"], max(q.tol for q in group), s["maxiter"], s["tol_s"],
+                s["maxiter_s"], p["cfg"]["nsap"], p["cfg"]["nm"], reliable=s["reliable"])
+        self._finish(p)
+
+    def _run_group(self, jobs):
+        """Several one-request jobs (any volumes) as one group solve
+        (qws_b200.group_solve): each kernel step is one launch over all of
+        them.  A request whose solve fails gets its error; the others finish."""
+        import qws_b200
+
+        def stage(job):
+            res, group = job
+            try:
+                return self._stage(res, group)
+            except Exception as e:
+                for q in group:
+                    q.error = f"{type(e).__name__}: {e}"
+                    q.t_done = time.monotonic()
+                return None
+
+        # the jobs' own host work (field set-up, uploads; downloads) on a
+        # pool of threads, as separate workers would do it
+        t0 = time.monotonic()
+        staged = [p for p in self._pool_map(stage, jobs) if p is not None]
+        if not staged:
+            return
+        solves = [dict(lattice=p["B"], x=p["xd"], b=p["bd"], tol=p["group"][0].tol,
+                       nsap=p["cfg"]["nsap"], nm=p["cfg"]["nm"], **self.solver) for p in staged]
+        t1 = time.monotonic()
+        st, gs = qws_b200.group_solve(solves, check=False)
+        t2 = time.monotonic()
+        self.group_rounds += gs["rounds"]
+        self.group_launches[0] += gs["merged_launches"]
+        self.group_launches[1] += gs["member_launches"]
+        done = []
+        for p, s in zip(staged, st):
+            if s["status"] != 0:
+                for q in p["group"]:
+                    q.error = f"QwsgError: solve failed in its group (qwsg error {s['status']})"
+                    q.t_done = time.monotonic()
+                continue
+            p["stats"] = s
+            p["group_size"] = len(staged)
+            done.append(p)
+        self._pool_map(self._finish, done)
+        t3 = time.monotonic()
+        for k, dt in enumerate((t1 - t0, t2 - t1, t3 - t2)):
+            self.group_phase_s[k] += dt
+
+    def _pool_map(self, fn, items):
+        if len(items) <= 1:
+            return [fn(x) for x in items]
+        from concurrent.futures import ThreadPoolExecutor
+
+        with ThreadPoolExecutor(max_workers=min(16, len(items))) as ex:
+            return list(ex.map(fn, items))
+
+    def _stage(self, res, group):
+        """Make the field resident, build the clover term(s), take the work
+        handle and upload the source(s): everything of a job before its solve."""
         import torch
 
+        self._torch = torch
         t0 = time.monotonic()
         for q in group:
             q.t_start = t0
@@ -473,7 +581,6 @@ class Service:
             B.set_tols([q.tol for q in group])
         res.stream.synchronize()
         t2 = time.monotonic()
-        s = self.solver
         with torch.cuda.stream(res.stream):
             S = np.ascontiguousarray(group[0].source, np.float64) if nr == 1 else None
             if S is None or not torch.from_numpy(S).is_pinned():
@@ -494,10 +601,24 @@ class Service:
             bd = B.to_device(S, out=B.job_b)
             xd = B.job_x
             xd.zero_()
-            st = B.bicgstab_dd_mix2_hf(xd, bd, max(q.tol for q in group), s["maxiter"],
-                                       s["tol_s"], s["maxiter_s"], cfg["nsap"], cfg["nm"],
-                                       reliable=s["reliable"])
-            truer = B.true_residual(xd, bd)
+        return {"res": res, "group": group, "cfg": cfg, "made": made, "B": B, "bd": bd,
+                "xd": xd, "t0": t0, "t1": t1, "t2": t2, "group_size": 1}
+
+    def _finish(self, p):
+        """True residuals, download, per-request results of a solved job."""
+        res, group, B, bd, xd = p["res"], p["group"], p["B"], p["bd"], p["xd"]
+        nr = len(group)
+        r0 = group[0]
+        torch = self._torch
+        with torch.cuda.stream(res.stream):
+            per = B.batch_stats()[0] if nr > 1 else [p["stats"]]
+            # the solver's own final true residual (reliable restarts
+            # compute it), else one more D application
+            if all(s.get("rel_resid_true", -1.0) >= 0 for s in per):
+                truer = [s["rel_resid_true"] for s in per]
+                truer = truer[0] if nr == 1 else truer
+            else:
+                truer = B.true_residual(xd, bd)
             if nr == 1 and r0.out is not None:
                 X = B.to_host(xd, out=r0.out)
             else:
@@ -512,10 +633,9 @@ class Service:
                 B.to_host(xd, out=P)
                 X = np.empty_like(P)
                 torch.from_numpy(X).copy_(torch.from_numpy(P))
-            per = B.batch_stats()[0] if nr > 1 else [st]
-            del bd, xd
         truer = [truer] if nr == 1 else truer
         t3 = time.monotonic()
+        t0, t1, t2 = p["t0"], p["t1"], p["t2"]
         for k, q in enumerate(group):
             if nr > 1 and q.out is not None:
                 q.out[...] = X[k]
@@ -523,7 +643,8 @@ class Service:
             q.stats = {"outer_iters": per[k]["outer_iters"], "true_rel_resid": truer[k],
                        "inner_iters": per[k]["inner_iters"]}
             q.batch = nr
-            q.t_resident, q.t_clover, q.t_solve = (t1 - t0) if made else 0.0, t2 - t1, t3 - t2
+            q.group = p["group_size"]
+            q.t_resident, q.t_clover, q.t_solve = (t1 - t0) if p["made"] else 0.0, t2 - t1, t3 - t2
             q.t_done = t3
 
 

@@ -39,6 +39,10 @@ def make_service(budget, max_batch=16):
     svc.completed = []
     svc.cv = threading.Condition()
     svc.lifo_after_s = None
+    svc.group = 1
+    svc.group_rounds = 0
+    svc.group_launches = [0, 0]
+    svc.group_phase_s = [0.0, 0.0, 0.0]
     return svc
 
 
@@ -251,3 +255,58 @@ def test_adaptive_lifo_under_overload():
     reqs[0].t_arrival = now - 5.0  # the oldest has waited long: newest first
     res, group = svc._pick()
     assert group == [reqs[3], reqs[2]]
+
+
+def test_group_jobs_take_every_startable_request():
+    """With group > 1 an idle worker takes every job that can start now (one
+    request each: merging into multi-RHS solves is off), up to `group`; a
+    request whose field is busy waits for a later group."""
+    svc = make_service(1e12, max_batch=1)
+    svc.group = 3
+    reqs = [req(L1, g, 0.13) for g in range(4)] + [req(L2, 0, 0.13)]
+    busy = FakeResident(L1, 1, 0.0, busy=True)
+    svc.residents[(L1, 1)] = busy
+    svc.pending = list(reqs)
+    jobs = svc._next_job()
+    assert [g for _, g in jobs] == [[reqs[0]], [reqs[2]], [reqs[3]]]
+    jobs = svc._next_job()
+    assert [g for _, g in jobs] == [[reqs[4]]]
+    assert svc.pending == [reqs[1]] and svc._next_job() is None
+    svc.group = 1
+    busy.busy = False
+    res, group = svc._next_job()
+    assert group == [reqs[1]]
+
+
+def test_group_failed_solve_fails_only_its_request(monkeypatch):
+    """A group solve reports a status per request: a failed one gets its
+    error, the others their results."""
+    import qws_b200
+
+    svc = make_service(1e12, max_batch=1)
+    svc.solver = dict(maxiter=10, tol_s=1e-6, maxiter_s=50, reliable=0)
+    reqs = [req(L1, g, 0.13) for g in range(3)]
+    finished = []
+
+    def stage(res, group):
+        return {"res": res, "group": group, "B": object(), "xd": None, "bd": None,
+                "cfg": {"nsap": 4, "nm": 2}}
+
+    def finish(p):
+        for q in p["group"]:
+            q.t_done = 1.0
+        finished.append((p["group"][0], p["group_size"], p["stats"]["status"]))
+
+    def group_solve(solves, check=True):
+        assert not check and len(solves) == 3
+        return ([{"status": 3 if k == 1 else 0, "outer_iters": 1, "inner_iters": 9,
+                  "rel_resid_recursive": 0.0, "rel_resid_true": -1.0} for k in range(3)],
+                {"rounds": 5, "merged_launches": 10, "member_launches": 30})
+
+    monkeypatch.setattr(svc, "_stage", stage, raising=False)
+    monkeypatch.setattr(svc, "_finish", finish, raising=False)
+    monkeypatch.setattr(qws_b200, "group_solve", group_solve)
+    svc._run_group([(FakeResident(L1, g, 0.0), [q]) for g, q in enumerate(reqs)])
+    assert sorted(finished, key=lambda f: reqs.index(f[0])) == [(reqs[0], 3, 0), (reqs[2], 3, 0)]
+    assert reqs[1].error.startswith("QwsgError") and reqs[1].t_done > 0
+    assert reqs[0].error is None and svc.group_rounds == 5
