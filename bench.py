@@ -899,30 +899,18 @@ def bench_precision_48(args, world):
     return out
 
 
-def bench_uneven(args):
-    """48 independent solves, volumes drawn uniformly from 8^4, 12^3x24,
-    16^3x32 and 24^3x48, each on its own seeded gauge field (generated on the
-    GPU), csw 1.7, kappa 0.1365, Gaussian sources, 1e-10, precision form.
-    All 48 are submitted at once to the solve service, run three ways:
-    `workers_N`, N workers solving concurrently on separate CUDA streams
-    (the small lattices fill a fraction of the SMs each); `workers_1`, one
-    after another; `group`, one worker running all 48 as one group solve
-    (qws_b200.group_solve: every kernel step one launch over all lattices at
-    that step).  A cold pass makes the fields resident, the timed warm pass
-    solves the same requests on resident fields."""
+def _uneven_pass(args, picks, vols, modes):
+    """Each mode: a service solving the requests for `picks` (one seeded
+    gauge field each) submitted at once; a cold pass makes the fields
+    resident, the timed warm pass solves the same requests again."""
     import qws_b200
     from qws_b200 import serve
 
-    vols = [(8, 8, 8, 8), (12, 12, 12, 24), (16, 16, 16, 32), (24, 24, 24, 48)]
-    rng = np.random.default_rng(4)
-    picks = [vols[int(rng.integers(len(vols)))] for _ in range(48)]
     src = {L: qws_b200.gen_source(L, 77, "gauss") for L in vols}
-    out = {"solves": 48, "volumes": {"x".join(map(str, L)): picks.count(L) for L in vols}}
-    modes = [(f"workers_{args.uneven_workers}", args.uneven_workers, 1), ("workers_1", 1, 1),
-             ("group", 1, 48)]
-    for name, workers, group in modes:
+    out = {"solves": len(picks), "volumes": {"x".join(map(str, L)): picks.count(L) for L in vols}}
+    for name, workers, group, gmax in modes:
         svc = serve.Service(serve.seeded_gauge(), budget_bytes=150e9, workers=workers,
-                            max_batch=1, group=group)
+                            max_batch=1, group=group, group_max_sites=gmax)
         try:
             def run():
                 t0 = time.monotonic()
@@ -937,7 +925,7 @@ def bench_uneven(args):
 
             cold, cold_s, _ = run()
             rounds0, launches0 = svc.group_rounds, list(svc.group_launches)
-            phase0 = list(svc.group_phase_s)
+            phase0, host0 = list(svc.group_phase_s), dict(svc.group_host_s)
             warm, warm_s, reqs = run()
         finally:
             svc.close()
@@ -947,20 +935,58 @@ def bench_uneven(args):
             "errors": warm["errors"] + cold["errors"], "above_tol": warm["above_tol"]}
         if group > 1:
             out[name]["group_sizes"] = sorted({q.group for q in reqs if q.error is None})
+            out[name]["group_max_sites"] = gmax
             out[name]["host_rounds"] = svc.group_rounds - rounds0
             out[name]["launches"] = svc.group_launches[0] - launches0[0]
             out[name]["launches_if_alone"] = svc.group_launches[1] - launches0[1]
             out[name]["phases_s"] = {k: round(svc.group_phase_s[i] - phase0[i], 4) for i, k in
                                      enumerate(("setup", "group_solve", "results"))}
-    c, one, g = out[f"workers_{args.uneven_workers}"], out["workers_1"], out["group"]
-    out["value"] = max(c["solves_per_s"], g["solves_per_s"])
+            out[name]["group_solve_host_s"] = {k[2:]: round(v - host0[k], 4)
+                                               for k, v in svc.group_host_s.items()}
+    return out
+
+
+def bench_uneven(args):
+    """48 independent solves, volumes drawn uniformly from 8^4, 12^3x24,
+    16^3x32 and 24^3x48, each on its own seeded gauge field (generated on the
+    GPU), csw 1.7, kappa 0.1365, Gaussian sources, 1e-10, precision form.
+    All 48 are submitted at once to the solve service, run four ways:
+    `workers_N`, N workers solving concurrently on separate CUDA streams
+    (the small lattices fill a fraction of the SMs each); `workers_1`, one
+    after another; `group`, one worker running all 48 as one group solve
+    (qws_b200.group_solve: every kernel step one launch over all lattices at
+    that step); `group_small`, N workers where the lattices of at most
+    300,000 sites (whose own launches underfill the GPU) form one group solve
+    and the larger ones run on their own streams beside it.  `small_volumes`
+    repeats streams / one at a time / group for 48 solves drawn from 8^4 and
+    12^3x24 only, the launch-bound case."""
+    vols = [(8, 8, 8, 8), (12, 12, 12, 24), (16, 16, 16, 32), (24, 24, 24, 48)]
+    rng = np.random.default_rng(4)
+    picks = [vols[int(rng.integers(len(vols)))] for _ in range(48)]
+    w = args.uneven_workers
+    out = _uneven_pass(args, picks, vols,
+                       [(f"workers_{w}", w, 1, None), ("workers_1", 1, 1, None),
+                        ("group", 1, 48, None), ("group_small", w, 48, 300000)])
+    c, one = out[f"workers_{w}"], out["workers_1"]
+    g, gs = out["group"], out["group_small"]
+    out["value"] = max(c["solves_per_s"], g["solves_per_s"], gs["solves_per_s"])
     out["unit"] = "solves/s"
     out["speedup_vs_one_at_a_time"] = c["solves_per_s"] / one["solves_per_s"]
     out["group_vs_streams"] = g["solves_per_s"] / c["solves_per_s"]
+    out["group_small_vs_streams"] = gs["solves_per_s"] / c["solves_per_s"]
+    svols = vols[:2]
+    rng = np.random.default_rng(5)
+    spicks = [svols[int(rng.integers(len(svols)))] for _ in range(48)]
+    small = _uneven_pass(args, spicks, svols, [(f"workers_{w}", w, 1, None),
+                                               ("workers_1", 1, 1, None), ("group", 1, 48, None)])
+    small["group_vs_streams"] = small["group"]["solves_per_s"] / small[f"workers_{w}"]["solves_per_s"]
+    small["group_vs_one_at_a_time"] = (small["group"]["solves_per_s"] /
+                                       small["workers_1"]["solves_per_s"])
+    out["small_volumes"] = small
     out["method"] = ("qws_b200.serve.Service: one resident field per gauge, clover built on the "
                      "GPU, bicgstab_dd_mix2_hf per request (workers_N: on the worker's stream; "
-                     "group: all requests of the pass in one group solve); the wall-clock "
-                     "span from submission to the last result")
+                     "group: the requests of the pass in one group solve); the wall-clock span "
+                     "from submission to the last result, host sources and solutions included")
     return out
 
 

@@ -223,6 +223,10 @@ typedef struct {
   long rounds;           /* host read-back points of the group */
   long merged_launches;  /* kernel launches issued */
   long member_launches;  /* launches the items' own solves would have issued */
+  /* host seconds spent waiting for the items' solves to reach their next
+   * read-back, merging their launches, issuing launches and copies, and
+   * waiting for the GPU */
+  double t_members, t_merge, t_launch, t_gpu_wait;
 } qwsg_group_stats;
 int qwsg_group_bicgstab_dd_mix2_hf(qwsg_group_item* items, int n, void* stream,
                                    qwsg_group_stats* stats);

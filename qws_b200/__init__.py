@@ -45,7 +45,9 @@ class GroupItem(ctypes.Structure):
 
 class GroupStats(ctypes.Structure):
     _fields_ = [("rounds", ctypes.c_long), ("merged_launches", ctypes.c_long),
-                ("member_launches", ctypes.c_long)]
+                ("member_launches", ctypes.c_long), ("t_members", ctypes.c_double),
+                ("t_merge", ctypes.c_double), ("t_launch", ctypes.c_double),
+                ("t_gpu_wait", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

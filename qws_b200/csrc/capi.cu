@@ -741,6 +741,10 @@ int qwsg_group_bicgstab_dd_mix2_hf(qwsg_group_item* items, int n, void* stream,
       gst->rounds = gs.rounds;
       gst->merged_launches = gs.merged_launches;
       gst->member_launches = gs.member_launches;
+      gst->t_members = gs.t_members;
+      gst->t_merge = gs.t_merge;
+      gst->t_launch = gs.t_launch;
+      gst->t_gpu_wait = gs.t_gpu_wait;
     }
     if (code) throw Error(code, first_error);
   });

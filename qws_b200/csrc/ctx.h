@@ -297,6 +297,9 @@ struct GroupStats {
   long rounds;           // read-back points of the group (host synchronisations)
   long merged_launches;  // launches issued
   long member_launches;  // launches the lattices' own solves would have issued
+  // host seconds: waiting for the members to reach their read-backs, merging,
+  // issuing the launches and copies, waiting for the GPU
+  double t_members, t_merge, t_launch, t_gpu_wait;
 };
 void group_bicgstab_dd_mix2_hf(std::vector<GroupItem>& items, cudaStream_t st, GroupStats* gs);
 void group_park(GroupMember& me, const void* dev, void* host, size_t bytes);

@@ -17,6 +17,7 @@
 // of that member's own launch with its own arguments, so every member's
 // results are bitwise those of its own solve; what changes is that the small
 // lattices no longer pay a launch, and a half-empty GPU, each.
+#include <chrono>
 #include <condition_variable>
 #include <map>
 #include <mutex>
@@ -56,6 +57,10 @@ struct GroupMember {
   bool ran = false;   // its launches ran in the last round
   int held = 0;       // rounds it has been held back in a row
   GroupSig last_sig;  // the launch sequence it ran last
+  // device addresses of the lattice's page-locked read-back buffers (null:
+  // not mapped, read back with a copy call)
+  void* h_res_dev = nullptr;
+  void* h_isc_dev = nullptr;
 };
 
 // called by a member's solver thread at a read-back: hand over the
@@ -101,6 +106,20 @@ void member_thread(GroupMember& me, GroupItem& it, int device) {
   me.g->cv_coord.notify_one();
 }
 
+// the read-backs of one round in one launch: block l copies member l's
+// result words into its page-locked host buffer (reachable from the device
+// through unified addressing), in place of one copy call per member
+struct Readback {
+  const unsigned long long* src;
+  unsigned long long* dst;
+  int words;
+  int pad_;
+};
+__global__ void k_group_readback(const Readback* __restrict__ rb) {
+  const Readback r = rb[blockIdx.x];
+  for (int k = threadIdx.x; k < r.words; k += blockDim.x) r.dst[k] = r.src[k];
+}
+
 // page-locked and device staging of one round's argument tables
 struct Staging {
   unsigned char* host = nullptr;
@@ -133,8 +152,13 @@ struct Staging {
 // and A's members arrive at B's step, after which both merge.  The smaller
 // of the two waits, and no member waits two rounds in a row.  Returns the
 // merged launches issued; marks in `ran` the members to release.
+static double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 long run_round(std::vector<GroupMember>& mem, std::map<GroupSig, GroupSig>& next, Staging& stg,
-               cudaStream_t st, long* member_launches) {
+               cudaStream_t st, long* member_launches, double* t) {
+  const double t0 = now_s();
   std::map<GroupSig, std::vector<int>> sigs;
   std::vector<GroupSig> cur(mem.size());
   for (int l = 0; l < (int)mem.size(); l++) {
@@ -181,6 +205,27 @@ long run_round(std::vector<GroupMember>& mem, std::map<GroupSig, GroupSig>& next
     }
     *member_launches += (long)(gr.sig->size() * gr.ls->size());
   }
+  std::vector<Readback> rbs;
+  std::vector<GroupMember*> copies;
+  for (auto& m : mem)
+    if (!m.left && m.ran && !m.finished && m.rb_bytes) {
+      void* dst = m.rb_host == m.c->h_res ? m.h_res_dev
+                  : m.rb_host == m.c->h_isc ? m.h_isc_dev : nullptr;
+      if (dst && m.rb_bytes % 8 == 0)
+        rbs.push_back({static_cast<const unsigned long long*>(m.rb_dev),
+                       static_cast<unsigned long long*>(dst), (int)(m.rb_bytes / 8), 0});
+      else
+        copies.push_back(&m);
+    }
+  if (!rbs.empty()) {
+    const size_t off = b.put(rbs.data(), sizeof(Readback) * rbs.size());
+    const int nrb = (int)rbs.size();
+    b.launches.push_back([=](const unsigned char* dev, cudaStream_t s2) {
+      count_launch();
+      k_group_readback<<<nrb, 32, 0, s2>>>(reinterpret_cast<const Readback*>(dev + off));
+    });
+  }
+  const double t1 = now_s();
   if (!b.launches.empty()) {
     stg.reserve(b.host.size());
     std::memcpy(stg.host, b.host.data(), b.host.size());
@@ -189,15 +234,19 @@ long run_round(std::vector<GroupMember>& mem, std::map<GroupSig, GroupSig>& next
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) throw Error(3, std::string("group solve launch: ") + cudaGetErrorString(e));
   }
+  for (GroupMember* m : copies)
+    QWSG_CUDA(cudaMemcpyAsync(m->rb_host, m->rb_dev, m->rb_bytes, cudaMemcpyDeviceToHost, st));
   for (int l = 0; l < (int)mem.size(); l++) {
     GroupMember& m = mem[l];
     if (m.left || !m.ran) continue;
     m.rec.recs.clear();
     m.last_sig = std::move(cur[l]);
-    if (!m.finished && m.rb_bytes)
-      QWSG_CUDA(cudaMemcpyAsync(m.rb_host, m.rb_dev, m.rb_bytes, cudaMemcpyDeviceToHost, st));
   }
+  const double t2 = now_s();
   QWSG_CUDA(cudaStreamSynchronize(st));
+  t[0] += t1 - t0;
+  t[1] += t2 - t1;
+  t[2] += now_s() - t2;
   return (long)b.launches.size();
 }
 
@@ -239,11 +288,19 @@ void group_bicgstab_dd_mix2_hf(std::vector<GroupItem>& items, cudaStream_t st, G
     mem[i].g = &g;
     mem[i].c = items[i].c;
     items[i].c->gm = &mem[i];
+    // (page-locked memory is mapped for the device under unified addressing;
+    // where it is not, the read-backs fall back to copies)
+    if (cudaHostGetDevicePointer(&mem[i].h_res_dev, items[i].c->h_res, 0) != cudaSuccess)
+      mem[i].h_res_dev = nullptr;
+    if (cudaHostGetDevicePointer(&mem[i].h_isc_dev, items[i].c->h_isc, 0) != cudaSuccess)
+      mem[i].h_isc_dev = nullptr;
+    (void)cudaGetLastError();
   }
   g.n_live = n;
   Staging stg;
   std::map<GroupSig, GroupSig> next;
   long rounds = 0, merged = 0, member_launches = 0;
+  double t_round[3] = {0, 0, 0}, t_wait = 0;
   std::vector<std::thread> th;
   th.reserve(n);
   for (int i = 0; i < n; i++) th.emplace_back(member_thread, std::ref(mem[i]), std::ref(items[i]), device);
@@ -251,11 +308,13 @@ void group_bicgstab_dd_mix2_hf(std::vector<GroupItem>& items, cudaStream_t st, G
   {
     std::unique_lock<std::mutex> lk(g.m);
     while (g.n_live > 0) {
+      const double w0 = now_s();
       g.cv_coord.wait(lk, [&] { return g.n_parked == g.n_live; });
+      t_wait += now_s() - w0;
       // every live member is parked: their state is ours until released
       lk.unlock();
       try {
-        merged += run_round(mem, next, stg, st, &member_launches);
+        merged += run_round(mem, next, stg, st, &member_launches, t_round);
       } catch (const std::exception& e) {
         fail = e.what();
       }
@@ -294,6 +353,10 @@ void group_bicgstab_dd_mix2_hf(std::vector<GroupItem>& items, cudaStream_t st, G
     gs->rounds = rounds;
     gs->merged_launches = merged;
     gs->member_launches = member_launches;
+    gs->t_members = t_wait;
+    gs->t_merge = t_round[0];
+    gs->t_launch = t_round[1];
+    gs->t_gpu_wait = t_round[2];
   }
   if (!fail.empty()) {
     cudaStreamSynchronize(st);

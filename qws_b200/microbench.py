@@ -17,6 +17,16 @@ solve_hf (a whole precision-form solve to 1e-10; --new-kappa rebuilds the
 clover term for another kappa before each, as a serving loop sees them).  --nrhs N runs the launch on a multi-RHS handle (N
 right-hand sides per launch; spinor bytes count N times, links and clover
 once).
+
+    python -m qws_b200.microbench --kernel solve_group --count 48 \
+        --volumes 8x8x8x8,12x12x12x24,16x16x16x32,24x24x24x48
+
+solve_group: `count` precision-form solves to 1e-10 on lattices drawn from
+`volumes` (each its own seeded gauge field, generated on the GPU; block grid
+and sweep counts from the autotuner's cache for the volume), all fields and
+sources resident: the solves one after another on one stream, then the same
+solves as one group solve (qws_b200.group_solve), each timed with CUDA
+events over `iters` repetitions.
 """
 from __future__ import annotations
 
@@ -45,7 +55,12 @@ def main():
                          "solve, as a serving loop sees them")
     ap.add_argument("--links18", action="store_true",
                     help="FP32 kernels read 18-real links even for SU(3) fields")
+    ap.add_argument("--count", type=int, default=48, help="solve_group: number of solves")
+    ap.add_argument("--volumes", default="8x8x8x8,12x12x12x24,16x16x16x32,24x24x24x48",
+                    help="solve_group: lattice volumes drawn uniformly")
     a = ap.parse_args()
+    if a.kernel == "solve_group":
+        return solve_group(a)
     L = tuple(int(v) for v in a.lattice.split(","))
     NB = tuple(int(v) for v in a.blocks.split(","))
     U, plaq = qws_b200.gen_gauge(L, 11, 5, 0.36)
@@ -126,6 +141,73 @@ def main():
     lat.close()
     if lat is not base:
         base.close()
+
+
+def solve_group(a):
+    import torch
+
+    import qws_b200
+    from qws_b200 import autotune
+
+    vols = [tuple(int(v) for v in s.split("x")) for s in a.volumes.split(",")]
+    rng = np.random.default_rng(4)
+    picks = [vols[int(rng.integers(len(vols)))] for _ in range(a.count)]
+    st = torch.cuda.Stream()
+    solves = []
+    for i, L in enumerate(picks):
+        hit = autotune.lookup(L, "hf", 1) or {}
+        NB = tuple(hit.get("NB", autotune.REFERENCE_NB))
+        lat = qws_b200.Lattice(L, NB, tbc=-1, kappa=a.kappa, stream=st)
+        lat.set_hop_threads(hit.get("hop_threads", 128))
+        lat.gen_gauge_device(1000 + 7919 * i + sum(L), 5, 0.36)
+        lat.build_clover(a.csw)
+        with torch.cuda.stream(st):
+            b = lat.to_device(qws_b200.gen_source(L, 77))
+            x = lat.empty("f64")
+        solves.append(dict(lattice=lat, x=x, b=b, tol=1e-10, maxiter=100, tol_s=1e-6,
+                           maxiter_s=50, nsap=hit.get("nsap", 4), nm=hit.get("nm", 2),
+                           reliable=5))
+    torch.cuda.synchronize()
+
+    def solo():
+        for s in solves:
+            s["x"].zero_()
+            s["lattice"].bicgstab_dd_mix2_hf(s["x"], s["b"], s["tol"], s["maxiter"], s["tol_s"],
+                                             s["maxiter_s"], s["nsap"], s["nm"], s["reliable"])
+
+    def group():
+        for s in solves:
+            s["x"].zero_()
+        return qws_b200.group_solve(solves, stream=st)[1]
+
+    def timed(fn):
+        with torch.cuda.stream(st):
+            for _ in range(a.warmup):
+                fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            out = None
+            for _ in range(a.iters):
+                out = fn()
+            e1.record(st)
+            torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / a.iters, out
+
+    t_solo, _ = timed(solo)
+    x_solo = [s["x"].clone() for s in solves]
+    t_group, gs = timed(group)
+    same = all(torch.equal(s["x"], x0) for s, x0 in zip(solves, x_solo))
+    res = {"kernel": "solve_group", "count": a.count,
+           "volumes": {"x".join(map(str, L)): picks.count(L) for L in vols},
+           "sites": int(sum(np.prod(L) for L in picks)),
+           "solo_ms": t_solo, "group_ms": t_group,
+           "solo_solves_per_s": a.count / (t_solo * 1e-3),
+           "group_solves_per_s": a.count / (t_group * 1e-3),
+           "group_bitwise_equal_solo": same, "group_stats": gs}
+    print(json.dumps(res), flush=True)
+    for s in solves:
+        s["lattice"].close()
 
 
 if __name__ == "__main__":

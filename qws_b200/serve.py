@@ -206,18 +206,24 @@ class Service:
 
     def __init__(self, gauge_source, budget_bytes=150e9, workers=3, max_batch=16,
                  block_grid=None, maxiter=100, tol_s=1e-6, maxiter_s=50, nsap=None, nm=None,
-                 reliable=5, graphs=True, lifo_after_s=None, group=1):
+                 reliable=5, graphs=True, lifo_after_s=None, group=1, group_max_sites=None):
         self.gauge_source = gauge_source
         # group > 1: a worker takes up to this many one-request jobs (any
         # volumes) at once and runs them as one group solve, every kernel
         # step one launch over all of them (qws_b200.group_solve); merging
         # into multi-RHS solves is then off (max_batch 1)
         self.group = max(1, int(group))
+        # only lattices of at most this many sites join a group; a larger one
+        # (whose own launches fill the GPU) runs alone on its worker's stream
+        # while a group runs beside it (None: every lattice joins)
+        self.group_max_sites = float("inf") if group_max_sites is None else int(group_max_sites)
         if self.group > 1:
             max_batch = 1
         self.group_rounds = 0
         self.group_launches = [0, 0]  # launches issued, launches the solves alone would issue
         self.group_phase_s = [0.0, 0.0, 0.0]  # jobs' set-up, group solve, jobs' results
+        # inside the group solves: host time per activity (qwsg_group_stats)
+        self.group_host_s = dict.fromkeys(("t_members", "t_merge", "t_launch", "t_gpu_wait"), 0.0)
         # adaptive LIFO: once the oldest pending request has waited longer
         # than this (s), the newest pending requests are served first -- under
         # overload the oldest are the ones a deadline sheds, and serving them
@@ -361,8 +367,9 @@ class Service:
         self.completed.append(q)
         q.done.set()
 
-    def _pick(self):
-        """The oldest request that can start now, with the compatible pending
+    def _pick(self, accept=None):
+        """The oldest request that can start now (and that `accept` takes,
+        when given), with the compatible pending
         requests merged into its batch (a power of two, at most max_batch, and
         no larger than the memory allows).  Once a request waits for memory
         that only running jobs can give back, later requests start only if
@@ -379,7 +386,7 @@ class Service:
                 time.monotonic() - order[0].t_arrival > self.lifo_after_s):
             order.reverse()
         for r in order:
-            if r.key() in tried:
+            if r.key() in tried or (accept is not None and not accept(r)):
                 continue
             tried.add(r.key())
             if field_bytes(r.L) + work_bytes(r.L, 1) > self.budget:
@@ -426,9 +433,12 @@ class Service:
         job = self._pick()
         if job is None or self.group <= 1:
             return job
+        small = lambda r: int(np.prod(r.L)) <= self.group_max_sites
+        if not small(job[1][0]):
+            return job  # a lattice that fills the GPU by itself: its own stream
         jobs = [job]
         while len(jobs) < self.group and self.pending:
-            j = self._pick()
+            j = self._pick(accept=small)
             if j is None:
                 break
             jobs.append(j)
@@ -517,6 +527,8 @@ class Service:
         self.group_rounds += gs["rounds"]
         self.group_launches[0] += gs["merged_launches"]
         self.group_launches[1] += gs["member_launches"]
+        for k in self.group_host_s:
+            self.group_host_s[k] += gs[k]
         done = []
         for p, s in zip(staged, st):
             if s["status"] != 0:

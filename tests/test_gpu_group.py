@@ -163,5 +163,5 @@ def test_group_rejects_bad_items(lattices):
     finally:
         batch.close()
     # an empty group is a no-op
-    assert qws_b200.group_solve([]) == ([], {"rounds": 0, "merged_launches": 0,
-                                             "member_launches": 0})
+    st, gs = qws_b200.group_solve([])
+    assert st == [] and gs["rounds"] == 0 and gs["merged_launches"] == 0

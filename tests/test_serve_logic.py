@@ -40,9 +40,11 @@ def make_service(budget, max_batch=16):
     svc.cv = threading.Condition()
     svc.lifo_after_s = None
     svc.group = 1
+    svc.group_max_sites = float("inf")
     svc.group_rounds = 0
     svc.group_launches = [0, 0]
     svc.group_phase_s = [0.0, 0.0, 0.0]
+    svc.group_host_s = dict.fromkeys(("t_members", "t_merge", "t_launch", "t_gpu_wait"), 0.0)
     return svc
 
 
@@ -301,7 +303,8 @@ def test_group_failed_solve_fails_only_its_request(monkeypatch):
         assert not check and len(solves) == 3
         return ([{"status": 3 if k == 1 else 0, "outer_iters": 1, "inner_iters": 9,
                   "rel_resid_recursive": 0.0, "rel_resid_true": -1.0} for k in range(3)],
-                {"rounds": 5, "merged_launches": 10, "member_launches": 30})
+                {"rounds": 5, "merged_launches": 10, "member_launches": 30, "t_members": 0.1,
+                 "t_merge": 0.1, "t_launch": 0.1, "t_gpu_wait": 0.1})
 
     monkeypatch.setattr(svc, "_stage", stage, raising=False)
     monkeypatch.setattr(svc, "_finish", finish, raising=False)
@@ -310,3 +313,18 @@ def test_group_failed_solve_fails_only_its_request(monkeypatch):
     assert sorted(finished, key=lambda f: reqs.index(f[0])) == [(reqs[0], 3, 0), (reqs[2], 3, 0)]
     assert reqs[1].error.startswith("QwsgError") and reqs[1].t_done > 0
     assert reqs[0].error is None and svc.group_rounds == 5
+
+
+def test_group_leaves_large_lattices_alone():
+    """With group_max_sites, a lattice above it starts as a job of its own
+    (its own stream) and the group takes only the smaller ones."""
+    svc = make_service(1e12, max_batch=1)
+    svc.group = 8
+    svc.group_max_sites = 20000
+    big = req(L2, 0, 0.13)                     # 131072 sites
+    smalls = [req(L1, g, 0.13) for g in range(3)]
+    svc.pending = [smalls[0], big, smalls[1], smalls[2]]
+    jobs = svc._next_job()
+    assert [g for _, g in jobs] == [[smalls[0]], [smalls[1]], [smalls[2]]]
+    res, group = svc._next_job()
+    assert group == [big]
