@@ -1023,6 +1023,7 @@ def bench_serving(args):
                 "warmup_s": round(warmup_s, 2), "warmup_errors": sum(q.error is not None for q in warm),
                 "warmup_error_kinds": serve.summarize(warm).get("error_kinds", {}),
                 "requests": len(reqs), "merged": svc.merged, "fields_evicted": svc.evicted,
+                "work_handles_moved": svc.handles_moved,
                 "gauges_per_volume": args.serve_gauges, "workers": 3, "budget_gb": 150,
                 "solver": "bicgstab_dd_mix2_hf (reliable 5), clover built on the GPU per kappa"})
     return out

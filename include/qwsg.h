@@ -78,6 +78,14 @@ int qwsg_batch_set_kappas(qwsg_lattice* batch, const double* kappas, double csw)
  * (and restart it from its true residual until that is below tols[r]) in
  * place of their tol argument.  NULL restores the tol argument for all RHS. */
 int qwsg_batch_set_tols(qwsg_lattice* batch, const double* tols);
+/* Re-attach a multi-RHS handle to another lattice of the same extents, block
+ * grid and time boundary (no counterpart in the reference): its work buffers
+ * then serve that lattice's fields and kappa, so a pool of handles per volume
+ * serves many gauge fields without allocating.  Per-RHS kappas and
+ * tolerances are dropped (set them again) and the handle's CUDA graphs
+ * released; the handle's pending work is finished first.  The old parent
+ * is not touched and may already be destroyed. */
+int qwsg_batch_set_parent(qwsg_lattice* batch, qwsg_lattice* parent);
 int qwsg_nrhs(const qwsg_lattice* lat, int* nrhs);
 /* per-RHS results of the last multi-RHS solve: stats of the DD solvers,
  * iteration counts of the inner solvers (either pointer may be NULL) */

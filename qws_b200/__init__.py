@@ -136,6 +136,7 @@ def load_library(path: str | os.PathLike | None = None):
                                      ctypes.POINTER(c_double)],
         "qwsg_bicgstab_dd_mix2_hf": [vp, vp, vp, c_double, c_int, c_double, c_int, c_int, c_int,
                                      c_int, ctypes.POINTER(SolveStats)],
+        "qwsg_batch_set_parent": [vp, vp],
         "qwsg_group_bicgstab_dd_mix2_hf": [ctypes.POINTER(GroupItem), c_int, vp,
                                            ctypes.POINTER(GroupStats)],
         "qwsg_counters": [vp] + [ctypes.POINTER(ctypes.c_long)] * 5,
@@ -644,6 +645,16 @@ class BatchLattice(Lattice):
 
     def set_kappa(self, kappa):
         raise QwsgError("kappa belongs to the parent lattice (or use set_kappas)")
+
+    def set_parent(self, parent):
+        """Serve another lattice of the same extents and block grid with this
+        handle's buffers (qwsg_batch_set_parent); per-RHS kappas and
+        tolerances must be set again."""
+        _check(self.lib.qwsg_batch_set_parent(self.h, parent.h))
+        self.parent = parent
+        self.kappa = parent.kappa
+        self.kappas = None
+        self.tols = None
 
     def set_kappas(self, kappas, csw):
         """A kappa per RHS: clover terms of the parent's gauge field built on

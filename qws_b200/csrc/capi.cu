@@ -232,6 +232,29 @@ int qwsg_create_batch(qwsg_lattice** out, qwsg_lattice* parent, int nrhs) {
   });
 }
 
+int qwsg_batch_set_parent(qwsg_lattice* l, qwsg_lattice* parent) {
+  return guarded([&] {
+    // (the old parent may be gone: nothing of it is touched)
+    if (!l || !l->c || !parent || !parent->c) throw Error(4, "lattice handle is NULL");
+    Ctx& c = *l->c;
+    Ctx& p = *parent->c;
+    if (!c.parent) throw Error(1, "qwsg_batch_set_parent: not a multi-RHS handle");
+    if (p.parent) throw Error(1, "qwsg_batch_set_parent: the parent must be a lattice");
+    for (int mu = 0; mu < 4; mu++)
+      if (p.G.L[mu] != c.G.L[mu] || p.G.NB[mu] != c.G.NB[mu])
+        throw Error(1, "qwsg_batch_set_parent: the lattice must have the same extents and block grid");
+    if (p.G.tbc != c.G.tbc) throw Error(1, "qwsg_batch_set_parent: the time boundary differs");
+    QWSG_CUDA(cudaStreamSynchronize(c.st));  // the handle's running work
+    c.clear_graphs();                        // they hold the old fields' addresses
+    c.rhs_kappas.clear();                    // per-RHS clover terms of the old gauge field
+    c.rhs_tols.clear();
+    c.parent = &p;
+    c.G.hop_threads = p.G.hop_threads;
+    c.links12_valid = false;
+    c.sync_from_parent(false);
+  });
+}
+
 int qwsg_batch_set_kappas(qwsg_lattice* l, const double* kappas, double csw) {
   return guarded([&] {
     check_ctx(l);

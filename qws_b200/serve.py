@@ -251,6 +251,9 @@ class Service:
         self.completed = []
         self.merged = 0
         self.evicted = 0                  # resident fields freed for others
+        self.handles_moved = 0            # work handles taken over by another field
+        self.stall_s = 5.0                # see _stalled
+        self._stall_since = None
         self.stop = False
         self.workers = [threading.Thread(target=self._worker, daemon=True) for _ in range(workers)]
         for t in self.workers:
@@ -323,9 +326,19 @@ class Service:
 
     # ---- scheduling ------------------------------------------------------------
     def _idle(self, keep=None):
+        keep = keep if isinstance(keep, tuple) else (keep,)
         return sorted((r for r in self.residents.values()
-                       if not r.busy and r.lat is not None and r is not keep),
+                       if not r.busy and r.lat is not None and all(r is not k for k in keep)),
                       key=lambda r: r.last_used)
+
+    def _donor(self, L, nr, exclude=None):
+        """An idle resident field of volume L holding a work handle of nr RHS
+        that a job on another field of that volume can take over
+        (qwsg_batch_set_parent), least recently used first."""
+        for r in self._idle(exclude):
+            if r.L == L and nr in r.work:
+                return r
+        return None
 
     def _evict(self, need, keep=None):
         """Free idle work handles, then idle resident fields (least recently
@@ -402,13 +415,23 @@ class Service:
             while nr * 2 <= min(len(group), self.max_batch, 32):
                 nr *= 2
             fit = None
+            donor = None
             while fit is None and nr >= 1:
-                need = (field_bytes(r.L) if res is None else 0) + \
-                    (work_bytes(r.L, nr) if res is None or nr not in res.work else 0)
-                if need == 0 or self.used + need <= self.budget or \
-                        (not blocked and self._evict(need, keep=res)):
-                    fit = need
-                else:
+                have = res is not None and nr in res.work
+                base = field_bytes(r.L) if res is None else 0
+                # the work buffers of an idle field of the same volume serve
+                # as well as new ones (they move to this field); if making
+                # room needs that field evicted, new buffers instead
+                d = None if have else self._donor(r.L, nr, exclude=res)
+                options = [(base, d)] if have or d is not None else []
+                if not have:
+                    options.append((base + work_bytes(r.L, nr), None))
+                for need, d in options:
+                    if need == 0 or self.used + need <= self.budget or \
+                            (not blocked and self._evict(need, keep=(res, d))):
+                        fit, donor = need, d
+                        break
+                if fit is None:
                     nr //= 2
             if fit is None:
                 blocked = True
@@ -418,6 +441,9 @@ class Service:
             if res is None:
                 res = _Placeholder(r.L, r.gauge)
                 self.residents[(r.L, r.gauge)] = res
+            if donor is not None:
+                res.work[nr] = donor.work.pop(nr)
+                self.handles_moved += 1
             res.busy = True
             for q in group:
                 self.pending.remove(q)
@@ -444,6 +470,22 @@ class Service:
             jobs.append(j)
         return jobs
 
+    def _stalled(self, job, now):
+        """Failure detection for admission: with every worker idle nothing
+        can give memory back, so pending requests that still cannot start
+        after `stall_s` never will -- fail them (AdmissionStalled) instead of
+        leaving their callers waiting.  Called with cv held."""
+        if job is not None or not self.pending or self.idle_workers < len(self.workers):
+            self._stall_since = None
+            return
+        if self._stall_since is None:
+            self._stall_since = now
+        elif now - self._stall_since > self.stall_s:
+            for q in list(self.pending):
+                self._reject(q, "AdmissionStalled: no memory can be freed for it while "
+                                "nothing runs")
+            self._stall_since = None
+
     def _scheduler(self):
         with self.cv:
             while True:
@@ -452,6 +494,7 @@ class Service:
                 if self.idle_workers == 0:
                     self._expire()
                 job = self._next_job() if self.idle_workers > 0 and self.pending else None
+                self._stalled(job, time.monotonic())
                 if job is None:
                     self.cv.wait(0.02)
                     continue
@@ -566,6 +609,7 @@ class Service:
         if made:  # first use of this field: make it resident
             U = self.gauge_source(res.L, res.gid)
             live = _Resident(res.L, res.gid, U, cfg["NB"], cfg["hop_threads"], self.graphs)
+            live.work = res.work  # a work handle taken over from another field
             live.busy = True
             with self.cv:
                 self.residents[(res.L, res.gid)] = live
@@ -577,6 +621,9 @@ class Service:
         if nr == 1:
             res.prepare(r0.kappa, r0.csw)  # the field's own clover term
         B = res.work.get(nr)
+        if B is not None and B.parent is not res.lat:  # taken over from another field
+            B.set_parent(res.lat)
+            B.set_stream(res.stream)
         if B is None:  # work buffers of an nr-RHS solve on this field, kept for reuse
             B = res.lat.batch(nr, stream=res.stream)
             try:
@@ -817,7 +864,7 @@ def main():
                     "shed": sum((q.error or "").startswith("DeadlineExceeded") for q in reqs),
                     "batch_sizes": {str(b): sum(q.batch == b for q in ok)
                                     for b in sorted({q.batch for q in ok})},
-                    "fields_evicted": svc.evicted})
+                    "fields_evicted": svc.evicted, "work_handles_moved": svc.handles_moved})
         print(json.dumps(out), flush=True)
     finally:
         svc.close()

@@ -40,6 +40,7 @@ def make_service(budget, max_batch=16):
     svc.cv = threading.Condition()
     svc.lifo_after_s = None
     svc.group = 1
+    svc.handles_moved = 0
     svc.group_max_sites = float("inf")
     svc.group_rounds = 0
     svc.group_launches = [0, 0]
@@ -158,13 +159,15 @@ def test_waiting_request_not_overtaken():
         svc.pending = [waiting, later, ready]
         return svc, warm, waiting, later, ready
 
-    # `later` (a new L1 field) would need `warm` evicted: it waits
-    svc, warm, waiting, later, ready = setup(f2 + w2 + 2 * warm_bytes - 1)
+    # `later` (a new L1 field; it would take over `warm`'s idle work
+    # buffers, so it needs a field's bytes) would need `warm` evicted: it waits
+    f1 = serve.field_bytes(L1)
+    svc, warm, waiting, later, ready = setup(f2 + w2 + warm_bytes + f1 - 1)
     res, group = svc._pick()
     assert group == [ready] and res is warm and not warm.closed
     assert svc.pending == [waiting, later]
     # with room for it in the free budget, `later` starts before `ready`
-    svc, warm, waiting, later, ready = setup(f2 + w2 + 2 * warm_bytes)
+    svc, warm, waiting, later, ready = setup(f2 + w2 + warm_bytes + f1)
     res, group = svc._pick()
     assert group == [later] and not warm.closed
     assert svc.pending == [waiting, ready]
@@ -328,3 +331,77 @@ def test_group_leaves_large_lattices_alone():
     assert [g for _, g in jobs] == [[smalls[0]], [smalls[1]], [smalls[2]]]
     res, group = svc._next_job()
     assert group == [big]
+
+
+def test_idle_work_handle_moves_to_another_field_of_the_volume():
+    """A job on a field without work buffers takes over an idle field's
+    buffers of the same volume and RHS count (no new allocation, no
+    eviction) instead of allocating its own."""
+    fb, wb = serve.field_bytes(L1), serve.work_bytes(L1, 1)
+    svc = make_service(2 * fb + wb)           # room for two fields and one handle
+    donor = FakeResident(L1, 0, 1.0, work=(1,))
+    target = FakeResident(L1, 1, 2.0)
+    svc.residents = {(L1, 0): donor, (L1, 1): target}
+    svc.used = 2 * fb + wb
+    handle = donor.work[1]
+    q = req(L1, 1, 0.13)
+    svc.pending = [q]
+    res, group = svc._pick()
+    assert res is target and group == [q]
+    assert target.work == {1: handle} and donor.work == {}
+    assert not handle.closed and not donor.closed and svc.handles_moved == 1
+    assert svc.used == 2 * fb + wb            # nothing allocated, nothing freed
+    # a field that is not resident yet: the placeholder takes the handle
+    target.busy = False
+    q2 = req(L1, 2, 0.13)
+    svc.budget = 3 * fb + wb
+    svc.pending = [q2]
+    res2, group2 = svc._pick()
+    assert isinstance(res2, serve._Placeholder) and res2.work == {1: handle}
+    assert target.work == {}
+
+
+def test_takeover_that_cannot_fit_falls_back_to_new_buffers():
+    """When room for a new field can only be made by evicting the idle field
+    whose work buffers the job would take over, the job gets new buffers
+    and that field is evicted (nothing running could ever free the memory
+    otherwise, and the request would wait for ever)."""
+    fb, wb = serve.field_bytes(L2), serve.work_bytes(L2, 1)
+    svc = make_service(fb + wb + fb // 2)      # one field and its buffers, not two fields
+    donor = FakeResident(L2, 0, 1.0, work=(1,))
+    svc.residents = {(L2, 0): donor}
+    svc.used = fb + wb
+    q = req(L2, 1, 0.13)
+    svc.pending = [q]
+    res, group = svc._pick()
+    assert group == [q] and isinstance(res, serve._Placeholder)
+    assert donor.closed and (L2, 0) not in svc.residents
+    assert res.work == {} and svc.used == fb + wb and svc.handles_moved == 0
+
+
+def test_stalled_admission_fails_the_requests():
+    """With every worker idle nothing can free memory: requests that still
+    cannot start after stall_s fail with AdmissionStalled (a bug elsewhere
+    must not leave their callers waiting for ever)."""
+    svc = make_service(1e12)
+    svc.workers = [None, None]
+    svc.idle_workers = 2
+    svc.stall_s = 1.0
+    svc._stall_since = None
+    q = req(L1, 0, 0.13)
+    svc.pending = [q]
+    svc._stalled(None, 100.0)
+    assert svc.pending == [q]
+    svc._stalled(None, 100.5)
+    assert svc.pending == [q]
+    svc._stalled(None, 101.5)
+    assert svc.pending == [] and q.error.startswith("AdmissionStalled") and q.done.is_set()
+    # a running job resets the clock
+    q2 = req(L1, 0, 0.13)
+    svc.pending = [q2]
+    svc._stalled(None, 200.0)
+    svc.idle_workers = 1
+    svc._stalled(None, 300.0)
+    svc.idle_workers = 2
+    svc._stalled(None, 300.5)
+    assert svc.pending == [q2]
