@@ -266,7 +266,6 @@ void group_bicgstab_dd_mix2_hf(std::vector<GroupItem>& items, cudaStream_t st, G
   }
   // everything the solve would allocate or build on first use, now (a
   // launch inside the recorded solve must be one the group can merge)
-  std::vector<bool> timing(n);
   for (int i = 0; i < n; i++) {
     Ctx& c = *items[i].c;
     c.ensure_outer();
@@ -275,16 +274,24 @@ void group_bicgstab_dd_mix2_hf(std::vector<GroupItem>& items, cudaStream_t st, G
     c.ensure_links12();
     c.check_launch("group solve set-up");
     QWSG_CUDA(cudaStreamSynchronize(c.st));
-    timing[i] = c.timing;
-    c.timing = false;
-    items[i].status = -1;
-    items[i].error.clear();
   }
   int device = 0;
   QWSG_CUDA(cudaGetDevice(&device));
   GroupState g;
   std::vector<GroupMember> mem(n);
+  std::vector<bool> timing(n);
+  // the lattices leave group mode on every way out
+  auto restore = [&] {
+    for (int i = 0; i < n; i++) {
+      items[i].c->gm = nullptr;
+      items[i].c->timing = timing[i];
+    }
+  };
   for (int i = 0; i < n; i++) {
+    timing[i] = items[i].c->timing;
+    items[i].c->timing = false;
+    items[i].status = -1;
+    items[i].error.clear();
     mem[i].g = &g;
     mem[i].c = items[i].c;
     items[i].c->gm = &mem[i];
@@ -302,8 +309,21 @@ void group_bicgstab_dd_mix2_hf(std::vector<GroupItem>& items, cudaStream_t st, G
   long rounds = 0, merged = 0, member_launches = 0;
   double t_round[3] = {0, 0, 0}, t_wait = 0;
   std::vector<std::thread> th;
-  th.reserve(n);
-  for (int i = 0; i < n; i++) th.emplace_back(member_thread, std::ref(mem[i]), std::ref(items[i]), device);
+  try {
+    th.reserve(n);
+    for (int i = 0; i < n; i++)
+      th.emplace_back(member_thread, std::ref(mem[i]), std::ref(items[i]), device);
+  } catch (...) {  // the threads that started unwind at their first read-back
+    {
+      std::lock_guard<std::mutex> lk(g.m);
+      g.abort = true;
+    }
+    g.cv_work.notify_all();
+    for (auto& t : th) t.join();
+    restore();
+    cudaStreamSynchronize(st);
+    throw Error(3, "group solve: could not start a thread per lattice");
+  }
   std::string fail;
   {
     std::unique_lock<std::mutex> lk(g.m);
@@ -345,10 +365,7 @@ void group_bicgstab_dd_mix2_hf(std::vector<GroupItem>& items, cudaStream_t st, G
     }
   }
   for (auto& t : th) t.join();
-  for (int i = 0; i < n; i++) {
-    items[i].c->gm = nullptr;
-    items[i].c->timing = timing[i];
-  }
+  restore();
   if (gs) {
     gs->rounds = rounds;
     gs->merged_launches = merged;
