@@ -89,9 +89,16 @@ class ClockSampler:
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 9:
-                self.rows.append(parts)
+                self.rows.append((time.monotonic(), parts))
+
+    def mark(self):
+        """Start of the timed region: the sampler runs from before the
+        warm-up (nvidia-smi takes a moment to emit its first sample) and
+        only samples taken after this mark count."""
+        self.t_mark = time.monotonic()
 
     def stop(self):
+        t_end = time.monotonic()
         if self.proc:
             self.proc.terminate()
             try:
@@ -102,7 +109,10 @@ class ClockSampler:
         reasons = set()
         smax = None
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in self.rows:
+        t0 = getattr(self, "t_mark", float("-inf"))
+        for t, r in self.rows:
+            if not t0 <= t <= t_end:
+                continue
             try:
                 sm.append(float(r[1]))
                 smax = float(r[2])
@@ -223,6 +233,8 @@ def bench_ours(args, w, name):
         return lat.bicgstab_dd_mix(xd, bd, w["tol"], w["maxiter"], w["tol_s"], w["maxiter_s"],
                                    w["nsap"], w["nm"])
 
+    clocks = ClockSampler(local)
+    clocks.start()
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             st = solve()
@@ -233,10 +245,9 @@ def bench_ours(args, w, name):
         progress("warm-up done; timed plain solves")
         # ---- device-resident timed region (production configuration: the
         #      SAP launch sequences replayed from CUDA graphs) ------------------
-        clocks = ClockSampler(local)
         barrier(world)
         torch.cuda.synchronize()
-        clocks.start()
+        clocks.mark()
         n_launch0 = qws_b200.launch_count()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -1143,7 +1154,7 @@ def main():
                     help="right-hand sides of the multi-RHS sub-result (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=5.0,
                     help="arrival rate of the serving sub-result (0: skip)")
-    ap.add_argument("--serve-window", type=float, default=10.0)
+    ap.add_argument("--serve-window", type=float, default=30.0)
     ap.add_argument("--serve-gauges", type=int, default=4)
     ap.add_argument("--uneven-workers", type=int, default=8,
                     help="workers of the 48 uneven-volume solves sub-result (0: skip)")
