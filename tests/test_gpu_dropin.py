@@ -72,7 +72,11 @@ def to_s(v):
 
 
 def P(a):
-    return ctypes.c_void_p(a.ctypes.data)
+    """The address of `a` for a C call.  The pointer object holds a
+    reference to `a`, so a temporary argument stays alive through the call
+    (a bare c_void_p(a.ctypes.data) of a temporary points at memory Python
+    frees as soon as this function returns)."""
+    return a.ctypes.data_as(ctypes.c_void_p)
 
 
 def test_globals(qws):
@@ -85,11 +89,13 @@ def test_globals(qws):
 def test_ddd(qws):
     lib, o, b, _ = qws
     out = aligned_empty(b.size, np.float64)
-    lib.ddd_d_(P(out), P(to_d(b)))
+    bd = to_d(b)
+    lib.ddd_d_(P(out), P(bd))
     assert rel(qws_to_nat_spinor(out, L, VLEND), o.ddd_d(b)) < 1e-13
     bs = b.astype(np.float32)
     out = aligned_empty(b.size, np.float32)
-    lib.ddd_s_(P(out), P(to_s(bs)))
+    bq = to_s(bs)
+    lib.ddd_s_(P(out), P(bq))
     assert rel(qws_to_nat_spinor(out, L, VLENS), o.ddd_s(bs)) < 1e-6
 
 
@@ -99,7 +105,8 @@ def test_ddd_in_out_domain0(qws):
     deo = ctypes.byref(ctypes.c_int(0))
     out = aligned_empty(b.size, np.float64)
     out[:] = 0
-    lib.ddd_in_d_(P(out), P(to_d(b)), deo)
+    bd = to_d(b)
+    lib.ddd_in_d_(P(out), P(bd), deo)
     g = GOLD["CASE0"]["norms"]
     val = float(np.sum(out.astype(np.float64) ** 2))
     assert check_sh_ok("ddd_in_d_", val, dict(g)["ddd_in_d_"])
@@ -116,9 +123,10 @@ def test_sap(qws):
     bs = b.astype(np.float32)
     nsap, nm = ctypes.c_int(4), ctypes.c_int(2)
     out = aligned_empty(b.size, np.float32)
-    lib.prec_ddd_s_(P(out), P(to_s(bs)), ctypes.byref(nsap), ctypes.byref(nm))
+    bq = to_s(bs)
+    lib.prec_ddd_s_(P(out), P(bq), ctypes.byref(nsap), ctypes.byref(nm))
     assert rel(qws_to_nat_spinor(out, L, VLENS), o.prec_ddd_s(bs, 4, 2)) < 5e-6
-    lib.prec_s_(P(out), P(to_s(bs)), ctypes.byref(nsap), ctypes.byref(nm))
+    lib.prec_s_(P(out), P(bq), ctypes.byref(nsap), ctypes.byref(nm))
     assert rel(qws_to_nat_spinor(out, L, VLENS), o.prec_s(bs, 4, 2)) < 5e-6
 
 

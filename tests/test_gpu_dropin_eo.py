@@ -34,7 +34,7 @@ def golden(name):
 
 
 def P(a):
-    return ctypes.c_void_p(a.ctypes.data)
+    return a.ctypes.data_as(ctypes.c_void_p)  # (holds a reference to `a`)
 
 
 def I(v):
