@@ -63,9 +63,12 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks/throttle reasons sampled during the timed region.
+    nvidia-smi runs on a pseudo-terminal (so it writes each sample as it
+    takes it instead of buffering them) with its own timestamp per sample;
+    the samples between mark() and stop() are the timed region's."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -73,45 +76,76 @@ class ClockSampler:
         self.gpu = gpu_index
         self.rows = []
         self.proc = None
+        self.t_mark = float("-inf")
 
     def start(self):
         try:
+            import pty
+
+            master, slave = pty.openpty()
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
                  "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                stdout=slave, stderr=subprocess.DEVNULL, close_fds=True)
+            os.close(slave)
+            self.fd = master
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except OSError:
             self.proc = None
 
     def _read(self):
-        for line in self.proc.stdout:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 9:
-                self.rows.append((time.monotonic(), parts))
+        buf = b""
+        while True:
+            try:
+                chunk = os.read(self.fd, 4096)
+            except OSError:  # the terminal closes when nvidia-smi exits
+                break
+            if not chunk:
+                break
+            buf += chunk
+            *lines, buf = buf.split(b"\n")
+            for line in lines:
+                parts = [p.strip() for p in line.decode(errors="replace").split(",")]
+                if len(parts) >= 10:
+                    self.rows.append((self._stamp(parts[0]), parts[1:]))
+
+    @staticmethod
+    def _stamp(text):
+        import datetime
+
+        for fmt in ("%Y/%m/%d %H:%M:%S.%f", "%Y/%m/%d %H:%M:%S"):
+            try:
+                return datetime.datetime.strptime(text, fmt).timestamp()
+            except ValueError:
+                pass
+        return time.time()
 
     def mark(self):
         """Start of the timed region: the sampler runs from before the
-        warm-up (nvidia-smi takes a moment to emit its first sample) and
-        only samples taken after this mark count."""
-        self.t_mark = time.monotonic()
+        warm-up (nvidia-smi takes a moment to emit its first sample)."""
+        self.t_mark = time.time()
 
     def stop(self):
-        t_end = time.monotonic()
+        t_end = time.time()
         if self.proc:
+            time.sleep(0.3)  # the sample in flight
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+            self.t.join(timeout=2)
+            try:
+                os.close(self.fd)
+            except OSError:
+                pass
         sm = []
         reasons = set()
         smax = None
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        t0 = getattr(self, "t_mark", float("-inf"))
         for t, r in self.rows:
-            if not t0 <= t <= t_end:
+            if not self.t_mark <= t <= t_end:
                 continue
             try:
                 sm.append(float(r[1]))
