@@ -119,23 +119,6 @@ void run_hop(Ctx& c, int sel, int epi, const HopArgs<T>& a) {
                     (double)sites * hop_bytes<T>(sel, epi, c.G.nr, a.U12 != nullptr)});
 }
 
-template <typename T>
-const typename Store<T>::type* gauge_of(Ctx& c);
-template <>
-const float* gauge_of<float>(Ctx& c) { return c.Us; }
-template <>
-const double* gauge_of<double>(Ctx& c) { return c.Ud; }
-template <>
-const __half* gauge_of<H16>(Ctx& c) { return c.Uh; }
-template <typename T>
-const typename Store<T>::type* clover_of(Ctx& c);
-template <>
-const float* clover_of<float>(Ctx& c) { return c.Cs; }
-template <>
-const double* clover_of<double>(Ctx& c) { return c.Cd; }
-template <>
-const __half* clover_of<H16>(Ctx& c) { return c.Ch; }
-
 void site_range(const Ctx& c, int col, int& site0, int& n) {
   if (col >= 0) {
     site0 = col * c.G.Vh;
