@@ -248,7 +248,9 @@ __global__ void __launch_bounds__(256, 4) k_hop_r64(const HopArgs<T> a) {
 // The full-lattice operators at a register bound of their own: FP64 at 128
 // registers (4 CTAs of 128 threads per SM instead of 3; 56 bytes spill) and
 // FP32 at 72 with CTAs of 128 (7 CTAs instead of 6): 13 % and 3 % faster
-// at 32^3x64, bit for bit the same results.
+// at 32^3x64; the FP16 face kernel at 72 too (7 instead of 6, ~5 % faster).
+// Bit for bit the same results.  (The FP16 block kernels at 56 registers,
+// 9 CTAs, ran 5 % slower than at 64.)
 template <typename T, int SEL, int EPI, bool PRK>
 __global__ void __launch_bounds__(256, 2) k_hop_r128(const HopArgs<T> a) {
   hop_site<T, OneRhs<T>, SEL, EPI, PRK>(a);
@@ -303,7 +305,8 @@ static void launch_v(const HopArgs<T>& a, cudaStream_t st) {
     k_hop_r128<T, SEL, EPI, PRK><<<blocks, threads, 0, st>>>(a);
     return;
   }
-  if constexpr (SEL == HOP_ALL && !PRK && std::is_same<T, float>::value) {
+  if constexpr (!PRK && ((SEL == HOP_ALL && std::is_same<T, float>::value) ||
+                         (SEL == HOP_OUTER && std::is_same<T, H16>::value))) {
     if (threads == 128) {  // (the bound assumes CTAs of at most 128 threads)
       k_hop_r73<T, SEL, EPI, PRK><<<blocks, threads, 0, st>>>(a);
       return;
