@@ -7,9 +7,21 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "kernels.h"
 
 namespace qwsg {
+
+// A named range for profilers (NVTX: ncu --nvtx, Nsight Systems), named
+// after the reference's routine and timing region it stands for; it costs
+// nothing measurable when no tool is attached.
+struct Region {
+  explicit Region(const char* name) { nvtxRangePushA(name); }
+  ~Region() { nvtxRangePop(); }
+  Region(const Region&) = delete;
+  Region& operator=(const Region&) = delete;
+};
 
 struct Error : std::runtime_error {
   int code;

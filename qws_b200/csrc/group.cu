@@ -158,6 +158,7 @@ static double now_s() {
 
 long run_round(std::vector<GroupMember>& mem, std::map<GroupSig, GroupSig>& next, Staging& stg,
                cudaStream_t st, long* member_launches, double* t) {
+  Region region_("group_round");
   const double t0 = now_s();
   std::map<GroupSig, std::vector<int>> sigs;
   std::vector<GroupSig> cur(mem.size());
@@ -253,6 +254,7 @@ long run_round(std::vector<GroupMember>& mem, std::map<GroupSig, GroupSig>& next
 }  // namespace
 
 void group_bicgstab_dd_mix2_hf(std::vector<GroupItem>& items, cudaStream_t st, GroupStats* gs) {
+  Region region_("group_bicgstab_dd_mix2_hf");
   const int n = (int)items.size();
   if (n == 0) return;
   for (int i = 0; i < n; i++) {

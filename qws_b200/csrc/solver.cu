@@ -467,6 +467,7 @@ void Ctx::check_launch(const char* what) {
 // operators
 // ---------------------------------------------------------------------------
 void dslash_full_d(Ctx& c, double* out, const double* in) {
+  Region region_("ddd_d");
   auto a = hop_args_c<double>(c);
   a.src = in;
   a.out = out;
@@ -479,6 +480,7 @@ void dslash_full_d(Ctx& c, double* out, const double* in) {
 }
 
 void dslash_full_s(Ctx& c, float* out, const float* in) {
+  Region region_("ddd_s");
   auto a = hop_args_c<float>(c);
   a.src = in;
   a.out = out;
@@ -570,6 +572,7 @@ void Ctx::ensure_face_lists() {
 template <typename T>
 static void jinv_t(Ctx& c, typename Store<T>::type* x, const typename Store<T>::type* b, int col,
                    int nm, typename Store<T>::type* tmp) {
+  Region region_("jinv_ddd_in_s");
   const int steps = nm < 1 ? 1 : nm;
   auto a = hop_args_c<T>(c);
   a.aux = b;
@@ -725,6 +728,7 @@ static void graphed(Ctx& c, const Ctx::GraphKey& k, F&& body) {
 // final-stage branches compute a_E = J_E(s_E), a_O = J_O(s_O - D_face,O (a_E, 0)),
 // out = D (a_E, a_O); here the last product is one full-lattice D.
 void prec_ddd_s(Ctx& c, float* out, const float* in, int nsap, int nm) {
+  Region region_("prec_ddd_s");
   if (nsap > 10 || nm > 10) throw Error(2, "prec_ddd_s_: nsap and nm must be <= 10 (qws.cc:798-799)");
   c.ensure_sap();
   c.ensure_face_lists();
@@ -740,6 +744,7 @@ void prec_ddd_s(Ctx& c, float* out, const float* in, int nsap, int nm) {
 
 // prec_s_ (qws.cc:929-975): out = M_SAP in.
 void prec_s(Ctx& c, float* out, const float* in, int nsap, int nm) {
+  Region region_("prec_s");
   c.ensure_sap();
   c.ensure_face_lists();
   float *s = c.sap_s, *a = c.sap_a;
@@ -758,6 +763,7 @@ void prec_s(Ctx& c, float* out, const float* in, int nsap, int nm) {
 // the launches alone (buffers, face lists and fields already in place), for
 // callers that capture them inside a larger step
 static void prec_s_h_seq(Ctx& c, float* out, const float* in, int nsap, int nm) {
+  Region region_("assign_mult_mSAP_s_h");
   graphed(c, {2, out, in, nsap, nm, c.kappa}, [&] {
     spinor_s2h(c.G, c.h_b, in, c.st);
     spinor_h2h(c.G, c.h_s, c.h_b, c.st);
@@ -829,6 +835,7 @@ void sap_kernel(Ctx& c, float* out, const float* in, const float* aux, int op, i
 // iterations run (a half iteration that converged counts as one).
 int bicgstab_precdd_s(Ctx& c, float* x, const float* b, double tol, int maxiter, int nsap, int nm,
                       double* final_rel) {
+  Region region_("bicgstab_precdd_s");
   c.ensure_inner();
   const Geom& G = c.G;
   float *q = c.in_q, *r = c.in_r, *p = c.in_p, *t = c.in_t, *r0 = c.in_r0;
@@ -894,6 +901,7 @@ int bicgstab_precdd_s(Ctx& c, float* x, const float* b, double tol, int maxiter,
 // every reduction.  The arithmetic and its order are the host loop's.
 int bicgstab_precdd_s_h(Ctx& c, float* x, const float* b, double tol, int maxiter, int nsap,
                         int nm, double* final_rel) {
+  Region region_("bicgstab_precdd_s_h");
   if (nsap > 10 || nm > 10)
     throw Error(2, "assign_mult_mSAP_s_h_: nsap and nm must be <= 10 (prec_ddd_s_h.h:100-101)");
   c.ensure_hp();
@@ -948,6 +956,7 @@ int bicgstab_precdd_s_h(Ctx& c, float* x, const float* b, double tol, int maxite
 // prec_s_ because its inner solve is flexible.
 static int approx_inv(Ctx& c, double* x, const double* b, double tol_s, int maxiter_s, int nsap,
                       int nm, bool hf) {
+  Region region_("approx_inv_dirac_op");
   blas_norm2<double>(c.G, b, c.d_res, c.rb, c.st);
   const double bn = std::sqrt(c.fetch(1)[0]);
   blas_d2s(c.G, c.ai_b, b, 1.0 / bn, c.st);
@@ -1031,6 +1040,7 @@ static int outer_loop(Ctx& c, double* x, const double* b, double tol, int iter_b
 void bicgstab_dd_mix(Ctx& c, double* x, const double* b, double tol, int maxiter, double tol_s,
                      int maxiter_s, int nsap, int nm, SolveStats* stats, double* hist,
                      int hist_len) {
+  Region region_("bicgstab_dd_mix");
   c.ensure_outer();
   long inner = 0;
   double rel = 0;
@@ -1062,6 +1072,7 @@ double true_residual(Ctx& c, const double* x, const double* b) {
 void bicgstab_dd_mix2_hf(Ctx& c, double* x, const double* b, double tol, int maxiter,
                          double tol_s, int maxiter_s, int nsap, int nm, int reliable,
                          SolveStats* stats) {
+  Region region_("bicgstab_dd_mix2_hf");
   c.ensure_outer();
   c.ensure_hp();
   long inner = 0;

@@ -275,12 +275,14 @@ void true_residual_mrhs(Ctx& c, const double* x, const double* b, double* rel) {
 
 int bicgstab_precdd_s_mrhs(Ctx& c, float* x, const float* b, double tol, int maxiter, int nsap,
                            int nm, int* iters) {
+  Region region_("bicgstab_precdd_s");
   c.ensure_inner();
   return inner_solve(c, x, b, tol, maxiter, nsap, nm, false, nullptr, iters);
 }
 
 int bicgstab_precdd_s_h_mrhs(Ctx& c, float* x, const float* b, double tol, int maxiter, int nsap,
                              int nm, int* iters) {
+  Region region_("bicgstab_precdd_s_h");
   c.ensure_hp();
   return inner_solve(c, x, b, tol, maxiter, nsap, nm, true, nullptr, iters);
 }
@@ -288,6 +290,7 @@ int bicgstab_precdd_s_h_mrhs(Ctx& c, float* x, const float* b, double tol, int m
 // bicgstab_dd_mix_ on all RHS (iter = 1 .. maxiter-1); per-RHS statistics
 void bicgstab_dd_mix_mrhs(Ctx& c, double* x, const double* b, double tol, int maxiter,
                           double tol_s, int maxiter_s, int nsap, int nm, SolveStats* st) {
+  Region region_("bicgstab_dd_mix");
   c.ensure_outer();
   const int nr = c.G.nr;
   bool act[kMax];
@@ -311,6 +314,7 @@ void bicgstab_dd_mix_mrhs(Ctx& c, double* x, const double* b, double tol, int ma
 void bicgstab_dd_mix2_hf_mrhs(Ctx& c, double* x, const double* b, double tol, int maxiter,
                               double tol_s, int maxiter_s, int nsap, int nm, int reliable,
                               SolveStats* st) {
+  Region region_("bicgstab_dd_mix2_hf");
   c.ensure_outer();
   c.ensure_hp();
   const int nr = c.G.nr;
