@@ -50,6 +50,13 @@ int qwsg_destroy(qwsg_lattice* lat);
 /* run all work on this cudaStream_t (NULL = the legacy default stream);
  * until called, the handle uses a private non-blocking stream */
 int qwsg_set_stream(qwsg_lattice* lat, void* cuda_stream);
+/* No counterpart in the reference: give the handle a new private
+ * non-blocking stream of this CUDA priority (lower = higher priority; the
+ * library destroys it with the handle) and return it.  Handles driven from
+ * several host threads need streams of their own: a CUDA graph captured on
+ * a stream takes in every launch made into that stream meanwhile, from any
+ * thread. */
+int qwsg_own_stream(qwsg_lattice* lat, int priority, void** cuda_stream);
 int qwsg_set_kappa(qwsg_lattice* lat, double kappa);
 int qwsg_geometry(const qwsg_lattice* lat, int* volume, int* pad);
 int qwsg_sync(qwsg_lattice* lat);
@@ -82,9 +89,10 @@ int qwsg_batch_set_tols(qwsg_lattice* batch, const double* tols);
  * grid and time boundary (no counterpart in the reference): its work buffers
  * then serve that lattice's fields and kappa, so a pool of handles per volume
  * serves many gauge fields without allocating.  Per-RHS kappas and
- * tolerances are dropped (set them again) and the handle's CUDA graphs
- * released; the handle's pending work is finished first.  The old parent
- * is not touched and may already be destroyed. */
+ * tolerances are dropped (set them again) and the handle's CUDA graphs are
+ * updated to the new fields before their next use; the handle's pending
+ * work (on its own stream) is finished first.  The old parent is not
+ * touched and may already be destroyed. */
 int qwsg_batch_set_parent(qwsg_lattice* batch, qwsg_lattice* parent);
 int qwsg_nrhs(const qwsg_lattice* lat, int* nrhs);
 /* per-RHS results of the last multi-RHS solve: stats of the DD solvers,

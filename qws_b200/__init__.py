@@ -70,6 +70,7 @@ def load_library(path: str | os.PathLike | None = None):
         "qwsg_create": [ctypes.POINTER(vp), ip, ip, c_int],
         "qwsg_destroy": [vp],
         "qwsg_set_stream": [vp, vp],
+        "qwsg_own_stream": [vp, c_int, ctypes.POINTER(vp)],
         "qwsg_set_kappa": [vp, c_double],
         "qwsg_geometry": [vp, ip, ip],
         "qwsg_sync": [vp],
@@ -306,8 +307,22 @@ class Lattice:
 
     # ---- configuration -----------------------------------------------------
     def set_stream(self, stream):
+        """Run this handle's work on `stream` (a torch stream, kept here, or a
+        raw cudaStream_t)."""
         handle = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
         _check(self.lib.qwsg_set_stream(self.h, ctypes.c_void_p(handle)))
+        self.stream = stream
+
+    def use_own_stream(self, priority=0):
+        """A private CUDA stream of this priority, made and owned by the
+        library (qwsg_own_stream), as a torch ExternalStream.  torch's own
+        streams come from a small pool that hands the same stream to several
+        owners; handles used from several threads must not share one (a graph
+        captured on a stream takes in every launch made into it meanwhile)."""
+        p = ctypes.c_void_p()
+        _check(self.lib.qwsg_own_stream(self.h, int(priority), ctypes.byref(p)))
+        self.stream = self.torch.cuda.ExternalStream(p.value)
+        return self.stream
 
     def set_kappa(self, kappa):
         self.kappa = float(kappa)

@@ -245,7 +245,7 @@ int qwsg_batch_set_parent(qwsg_lattice* l, qwsg_lattice* parent) {
         throw Error(1, "qwsg_batch_set_parent: the lattice must have the same extents and block grid");
     if (p.G.tbc != c.G.tbc) throw Error(1, "qwsg_batch_set_parent: the time boundary differs");
     QWSG_CUDA(cudaStreamSynchronize(c.st));  // the handle's running work
-    c.clear_graphs();                        // they hold the old fields' addresses
+    c.graph_gen++;  // the graphs hold the old fields' addresses: update before use
     c.rhs_kappas.clear();                    // per-RHS clover terms of the old gauge field
     c.rhs_tols.clear();
     c.parent = &p;
@@ -383,6 +383,20 @@ int qwsg_set_stream(qwsg_lattice* l, void* stream) {
     if (c.own_stream) cudaStreamDestroy(c.st);
     c.own_stream = false;
     c.st = (cudaStream_t)stream;  // NULL = the legacy default stream
+  });
+}
+
+int qwsg_own_stream(qwsg_lattice* l, int priority, void** stream) {
+  return guarded([&] {
+    check_ctx(l);
+    Ctx& c = *l->c;
+    cudaStream_t s = nullptr;
+    QWSG_CUDA(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, priority));
+    QWSG_CUDA(cudaStreamSynchronize(c.st));
+    if (c.own_stream) cudaStreamDestroy(c.st);
+    c.st = s;
+    c.own_stream = true;
+    if (stream) *stream = (void*)s;
   });
 }
 

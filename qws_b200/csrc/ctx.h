@@ -209,9 +209,10 @@ struct Ctx {
     int nsap, nm;
     double kappa;
     double tol = 0;  // the stopping tolerance a captured solver step compares with
+    long gen = 0;    // graph_gen at capture (set by graphed)
     bool operator==(const GraphKey& o) const {
       return op == o.op && a == o.a && b == o.b && nsap == o.nsap && nm == o.nm &&
-             kappa == o.kappa && tol == o.tol;
+             kappa == o.kappa && tol == o.tol && gen == o.gen;
     }
   };
   struct GraphEntry {
@@ -223,6 +224,10 @@ struct Ctx {
   bool use_graphs = true;
   long n_graph_launches = 0;
   void clear_graphs();
+  // bumped when the fields the graphs read change (a multi-RHS handle moved
+  // to another parent): the graphs are then captured again and, where the
+  // launch sequence is the same, updated in place instead of instantiated
+  long graph_gen = 0;
 
   // set while this lattice takes part in a group solve (group.cu): its
   // read-backs wait for the group's merged launches

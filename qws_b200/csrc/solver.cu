@@ -641,7 +641,8 @@ void Ctx::clear_graphs() {
 // Run `body` (launches only) through a cached CUDA graph.  Everything the
 // body allocates or builds must exist before the first capture.
 template <typename F>
-static void graphed(Ctx& c, const Ctx::GraphKey& k, F&& body) {
+static void graphed(Ctx& c, Ctx::GraphKey k, F&& body) {
+  k.gen = c.graph_gen;
   // the link form is settled before a capture (its check reads back a result)
   // and a change of form drops the graphs captured with the other one
   c.ensure_links12();
@@ -683,10 +684,11 @@ static void graphed(Ctx& c, const Ctx::GraphKey& k, F&& body) {
   }
   cudaGraph_t g = nullptr;
   QWSG_CUDA(cudaStreamEndCapture(c.st, &g));
-  // the same step with other scalar arguments (kappa, tolerance): the launch
-  // sequence is the same, so update the instantiated graph in place -- far
-  // cheaper than instantiating one (a service sees a new kappa in nearly
-  // every request); launches already enqueued keep their arguments
+  // the same step with other scalar arguments (kappa, tolerance) or other
+  // fields (graph_gen): the launch sequence is the same, so update the
+  // instantiated graph in place -- far cheaper than instantiating one (a
+  // service sees a new kappa in nearly every request); launches already
+  // enqueued keep their arguments
   for (size_t i = 0; i < c.graphs.size(); i++) {
     auto& en = c.graphs[i];
     if (en.key.op == k.op && en.key.a == k.a && en.key.b == k.b && en.key.nsap == k.nsap &&

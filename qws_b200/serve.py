@@ -145,9 +145,10 @@ class _Resident:
         import qws_b200
 
         self.L, self.gid = L, gauge_id
-        self.stream = torch.cuda.Stream(priority=stream_priority(L))
         # (kappa is set per job; a merged job's kernels take only its sign)
-        self.lat = qws_b200.Lattice(L, NB, tbc=-1, kappa=0.125, stream=self.stream)
+        self.lat = qws_b200.Lattice(L, NB, tbc=-1, kappa=0.125)
+        # a stream of its own (torch's streams are pooled and shared)
+        self.stream = self.lat.use_own_stream(stream_priority(L))
         self.lat.set_hop_threads(hop_threads)
         self.lat.set_graphs(graphs)
         self.graphs = graphs
@@ -253,6 +254,7 @@ class Service:
         self.evicted = 0                  # resident fields freed for others
         self.handles_moved = 0            # work handles taken over by another field
         self.stall_s = 5.0                # see _stalled
+        self.failed = None                # set when the scheduler had to stop
         self._stall_since = None
         self.stop = False
         self.workers = [threading.Thread(target=self._worker, daemon=True) for _ in range(workers)]
@@ -283,6 +285,8 @@ class Service:
         req.t_arrival = time.monotonic()
         with self.cv:
             self.pending.append(req)
+            if self.failed:
+                self._reject(req, self.failed)
             self.cv.notify_all()
         return req
 
@@ -294,6 +298,8 @@ class Service:
                 req.rid = next(self.ids)
                 req.t_arrival = time.monotonic()
                 self.pending.append(req)
+                if self.failed:
+                    self._reject(req, self.failed)
             self.cv.notify_all()
         return list(reqs)
 
@@ -491,15 +497,27 @@ class Service:
             while True:
                 if self.stop and not self.pending:
                     return
-                if self.idle_workers == 0:
-                    self._expire()
-                job = self._next_job() if self.idle_workers > 0 and self.pending else None
-                self._stalled(job, time.monotonic())
+                try:
+                    if self.idle_workers == 0:
+                        self._expire()
+                    job = self._next_job() if self.idle_workers > 0 and self.pending else None
+                    self._stalled(job, time.monotonic())
+                except Exception as e:  # the scheduler cannot go on (a CUDA error, say)
+                    self._fail_pending(f"ServiceFailed: {type(e).__name__}: {e}")
+                    return
                 if job is None:
                     self.cv.wait(0.02)
                     continue
                 self.idle_workers -= 1
                 self.jobs.put(job)
+
+    def _fail_pending(self, why):
+        """The scheduler stops: every pending request and every later one
+        fails with `why` instead of leaving its caller waiting.  Called with
+        cv held."""
+        self.failed = why
+        for q in list(self.pending):
+            self._reject(q, why)
 
     # ---- execution -------------------------------------------------------------
     def _worker(self):
@@ -534,7 +552,7 @@ class Service:
     def _run(self, res, group):
         p = self._stage(res, group)
         s = self.solver
-        with self._torch.cuda.stream(p["res"].stream):
+        with self._torch.cuda.stream(p["B"].stream):
             p["stats"] = p["B"].bicgstab_dd_mix2_hf(
                 p["xd"], p["bd"], max(q.tol for q in group), s["maxiter"], s["tol_s"],
                 s["maxiter_s"], p["cfg"]["nsap"], p["cfg"]["nm"], reliable=s["reliable"])
@@ -623,12 +641,15 @@ class Service:
         B = res.work.get(nr)
         if B is not None and B.parent is not res.lat:  # taken over from another field
             B.set_parent(res.lat)
-            B.set_stream(res.stream)
-        if B is None:  # work buffers of an nr-RHS solve on this field, kept for reuse
-            B = res.lat.batch(nr, stream=res.stream)
+        if B is None:  # work buffers of an nr-RHS solve, kept for reuse
+            # on a stream of its own: a handle that moves to another field
+            # has nothing but its own work to wait for, and no other thread
+            # launches into a stream whose graphs it captures
+            B = res.lat.batch(nr)
             try:
+                B.use_own_stream(stream_priority(res.L))
                 B.set_graphs(self.graphs)
-                with torch.cuda.stream(res.stream):
+                with torch.cuda.stream(B.stream):
                     B.job_b, B.job_x = B.empty("f64"), B.empty("f64")
             except Exception:
                 B.job_b = B.job_x = None
@@ -639,8 +660,9 @@ class Service:
             B.set_kappas([q.kappa for q in group], r0.csw)
             B.set_tols([q.tol for q in group])
         res.stream.synchronize()
+        B.stream.synchronize()  # (per-RHS clover terms are built on the handle's stream)
         t2 = time.monotonic()
-        with torch.cuda.stream(res.stream):
+        with torch.cuda.stream(B.stream):
             S = np.ascontiguousarray(group[0].source, np.float64) if nr == 1 else None
             if S is None or not torch.from_numpy(S).is_pinned():
                 # pageable (or several) sources: a multi-threaded copy into the
@@ -669,7 +691,7 @@ class Service:
         nr = len(group)
         r0 = group[0]
         torch = self._torch
-        with torch.cuda.stream(res.stream):
+        with torch.cuda.stream(B.stream):
             per = B.batch_stats()[0] if nr > 1 else [p["stats"]]
             # the solver's own final true residual (reliable restarts
             # compute it), else one more D application

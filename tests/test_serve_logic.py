@@ -41,6 +41,7 @@ def make_service(budget, max_batch=16):
     svc.lifo_after_s = None
     svc.group = 1
     svc.handles_moved = 0
+    svc.failed = None
     svc.group_max_sites = float("inf")
     svc.group_rounds = 0
     svc.group_launches = [0, 0]
@@ -405,3 +406,28 @@ def test_stalled_admission_fails_the_requests():
     svc.idle_workers = 2
     svc._stalled(None, 300.5)
     assert svc.pending == [q2]
+
+
+def test_scheduler_failure_fails_requests_instead_of_hanging(monkeypatch):
+    """An exception in the scheduler (a CUDA error while freeing memory, say)
+    fails every pending and every later request with ServiceFailed; nobody
+    waits for ever."""
+    svc = make_service(1e12)
+    svc.stop = False
+    svc.idle_workers = 1
+    svc.workers = [None]
+    svc._stall_since = None
+    svc.stall_s = 5.0
+    svc.jobs = None
+    svc.ids = iter(range(100))
+    q = req(L1, 0, 0.13)
+    svc.pending = [q]
+
+    def boom():
+        raise RuntimeError("CUDA error: an illegal memory access was encountered")
+
+    monkeypatch.setattr(svc, "_next_job", boom)
+    svc._scheduler()  # returns instead of looping
+    assert q.done.is_set() and q.error.startswith("ServiceFailed: RuntimeError")
+    q2 = svc.submit(req(L1, 1, 0.13))
+    assert q2.wait(0.1).error.startswith("ServiceFailed")
