@@ -425,13 +425,20 @@ class Service:
             while fit is None and nr >= 1:
                 have = res is not None and nr in res.work
                 base = field_bytes(r.L) if res is None else 0
-                # the work buffers of an idle field of the same volume serve
-                # as well as new ones (they move to this field); if making
-                # room needs that field evicted, new buffers instead
-                d = None if have else self._donor(r.L, nr, exclude=res)
-                options = [(base, d)] if have or d is not None else []
-                if not have:
-                    options.append((base + work_bytes(r.L, nr), None))
+                fresh = base + work_bytes(r.L, nr)
+                # new work buffers when they fit the free budget (a field
+                # keeps its buffers, and their CUDA graphs, for its next
+                # job); else the buffers of an idle field of the same volume
+                # (they move to this field, their graphs updated to its
+                # fields); if making room needs that field evicted, new
+                # buffers after all
+                if have:
+                    options = [(base, None)]
+                elif self.used + fresh <= self.budget:
+                    options = [(fresh, None)]
+                else:
+                    d = self._donor(r.L, nr, exclude=res)
+                    options = ([(base, d)] if d is not None else []) + [(fresh, None)]
                 for need, d in options:
                     if need == 0 or self.used + need <= self.budget or \
                             (not blocked and self._evict(need, keep=(res, d))):
