@@ -50,7 +50,7 @@ def _dd_operator_norms(o, b):
 
 
 @pytest.mark.parametrize("case", ["CASE0", "CASE_4111_1111", "CASE1", "CASE2", "CASE3",
-                                  "CASE4", "CASE7", "CASE8", "CASE9"])
+                                  "CASE4", "CASE5", "CASE6", "CASE7", "CASE8", "CASE9"])
 def test_dd_operator_norms(case):
     g, o, b, _ = _setup(case)
     assert check_sh_ok("input", float(np.sum(b * b)), _golden(g, "input"))
