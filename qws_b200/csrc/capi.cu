@@ -390,9 +390,9 @@ int qwsg_own_stream(qwsg_lattice* l, int priority, void** stream) {
   return guarded([&] {
     check_ctx(l);
     Ctx& c = *l->c;
+    QWSG_CUDA(cudaStreamSynchronize(c.st));
     cudaStream_t s = nullptr;
     QWSG_CUDA(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, priority));
-    QWSG_CUDA(cudaStreamSynchronize(c.st));
     if (c.own_stream) cudaStreamDestroy(c.st);
     c.st = s;
     c.own_stream = true;

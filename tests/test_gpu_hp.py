@@ -21,9 +21,15 @@ pytestmark = pytest.mark.gpu
 
 GOLD = json.loads((Path(__file__).parent / "golden" / "case_norms.json").read_text())
 KAPPA = 0.05
+# main.cc's fields on the lattices of the DD goldens: SAP blocks 16x6x4x3
+# (one rank, and rank grids (1,2,2,2) and (1,1,4,4)), 16x3x4x4 (an odd
+# extent) and 16x6x6x2 (two sites across)
 CASES = {
     "CASE0": ((32, 6, 4, 3), (1, 1, 1, 1)),
+    "CASE2": ((32, 3, 4, 4), (1, 1, 1, 2)),
+    "CASE4": ((32, 6, 6, 2), (1, 1, 1, 2)),
     "CASE7": ((32, 6, 4, 3), (1, 2, 2, 2)),
+    "CASE9": ((32, 6, 4, 3), (1, 1, 4, 4)),
 }
 
 
