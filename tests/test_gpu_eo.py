@@ -1,4 +1,5 @@
-"""GPU even-odd (site parity) family against the oracle and the CASE0 golden.
+"""GPU even-odd (site parity) family against the oracle (on the CASE0, 4 and 7
+lattices) and the CASE0 golden.
 
 main.cc fills its arrays with the DD generator and reads them with the
 even-odd operators too; oracle/qwsref.py's eo_perm gives the field an
@@ -30,12 +31,20 @@ def rel(a, b, m):
     return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
 
 
-@pytest.fixture(scope="module", params=["CASE0", "CASE7"])
+# golden lattices whose global extents are all even (site parity is then
+# consistent across the periodic boundaries)
+EO_CASES = {
+    "CASE0": ((32, 6, 4, 3), (1, 1, 1, 1)),
+    "CASE4": ((32, 6, 6, 2), (1, 1, 1, 2)),
+    "CASE7": ((32, 6, 4, 3), (1, 2, 2, 2)),
+}
+
+
+@pytest.fixture(scope="module", params=list(EO_CASES))
 def setup(request):
     import qws_b200
 
-    lloc, npe = ((32, 6, 4, 3), (1, 1, 1, 1)) if request.param == "CASE0" else \
-        ((32, 6, 4, 3), (1, 2, 2, 2))
+    lloc, npe = EO_CASES[request.param]
     L = tuple(a * b for a, b in zip(lloc, npe))
     NB = (2 * npe[0], npe[1], npe[2], npe[3])
     U, C, S = gen_main_fields(lloc, npe, 2)
