@@ -199,6 +199,13 @@ int qwsg_ddd_out_h(qwsg_lattice* lat, float* out, const float* in, int colour, d
  * prec_ddd_s_h.h:143-150 (no separate entry point there). */
 int qwsg_sap_update_s(qwsg_lattice* lat, float* s, const float* a, const float* in, int colour);
 int qwsg_sap_update_h(qwsg_lattice* lat, float* s, const float* a, const float* in, int colour);
+/* The FP32 spinor field `in` as the FP16 kernels store it and read it back,
+ * into `out` (FP32, device): per site (and RHS) n = max_i |v_i|, each
+ * component stored as the FP16 round-to-nearest-even of the FP32 product
+ * v_i * (1/n), read back as FP16 value * n in FP32; a site with n < 1e-30 is
+ * stored as zero.  The storage format of assign_q_s2h_ / assign_q_h2s_
+ * (qws_h.cc:175-269), which store one global scale for the whole field. */
+int qwsg_store_h(qwsg_lattice* lat, float* out, const float* in);
 /* bicgstab_precdd_s_h_ (bicgstab_precdd_s_h.cc:83): flexible FP32 BiCGStab
  * with the FP16 SAP preconditioner; x solves D x = b */
 int qwsg_bicgstab_precdd_s_h(qwsg_lattice* lat, float* x, const float* b, double tol, int maxiter,

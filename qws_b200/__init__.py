@@ -133,6 +133,7 @@ def load_library(path: str | os.PathLike | None = None):
         "qwsg_ddd_out_h": [vp, vp, vp, c_int, c_double],
         "qwsg_sap_update_s": [vp, vp, vp, vp, c_int],
         "qwsg_sap_update_h": [vp, vp, vp, vp, c_int],
+        "qwsg_store_h": [vp, vp, vp],
         "qwsg_bicgstab_precdd_s_h": [vp, vp, vp, c_double, c_int, c_int, c_int, ip,
                                      ctypes.POINTER(c_double)],
         "qwsg_bicgstab_dd_mix2_hf": [vp, vp, vp, c_double, c_int, c_double, c_int, c_int, c_int,
@@ -562,6 +563,13 @@ class Lattice:
         """nm Richardson steps on one colour with the FP16-storage kernel."""
         out = self._out(b, out)
         _check(self.lib.qwsg_jinv_h(self.h, _ptr(out), _ptr(b), int(colour), int(nm)))
+        return out
+
+    def store_h(self, x, out=None):
+        """x (FP32) as the FP16 kernels store it (per-site scale, FP16
+        round-to-nearest-even) and read it back (qwsg_store_h)."""
+        out = self._out(x, out)
+        _check(self.lib.qwsg_store_h(self.h, _ptr(out), _ptr(x)))
         return out
 
     def ddd_out_h(self, x, colour, factor, out=None):

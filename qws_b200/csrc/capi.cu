@@ -704,6 +704,16 @@ int qwsg_sap_update_h(qwsg_lattice* l, float* s, const float* a, const float* in
     sap_kernel(*l->c, s, a, in, 3, colour, 0, 0.0, true);
   });
 }
+int qwsg_store_h(qwsg_lattice* l, float* out, const float* in) {
+  return guarded([&] {
+    check_ctx(l);
+    Ctx& c = *l->c;
+    if (!c.h_b) c.h_b = c.alloc_spinor_h();
+    spinor_s2h(c.G, c.h_b, in, c.st);
+    spinor_h2s(c.G, out, c.h_b, c.st);
+    c.check_launch("qwsg_store_h");
+  });
+}
 int qwsg_bicgstab_precdd_s_h(qwsg_lattice* l, float* x, const float* b, double tol, int maxiter,
                              int nsap, int nm, int* iters, double* final_rel) {
   return guarded([&] {

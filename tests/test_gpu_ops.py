@@ -310,3 +310,34 @@ def test_fp16_pair_kernels_equal_single_rhs(setup, lattice):
                 np.testing.assert_array_equal(pairs[k][0], single[k], err_msg=k)
     finally:
         B.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nr", [1, 2])
+def test_fp16_storage_bit_exact(setup, lattice, nr):
+    """The FP16 storage format itself, bit for bit (the counterpart of the
+    reference's fp16 conversion dump, testhf.cc): a field stored and read
+    back by the device (qwsg_store_h, one and two RHS per handle) equals the
+    numpy emulation store16 exactly -- FP32 site maximum, FP32 reciprocal and
+    products, round-to-nearest-even FP16.  Site magnitudes span 70 decades;
+    one component per site is a million times below the site's maximum
+    (FP16 subnormals), one site is zero and one is FP32-denormal (both
+    stored as zero)."""
+    V = int(np.prod(L))
+    rng = np.random.default_rng(9 + nr)
+    v = rng.standard_normal((nr, V, 24)) * 10.0 ** rng.uniform(-35, 35, (nr, V, 1))
+    v[..., 5] *= 1e-6
+    v[:, 0] = 0.0
+    v[:, 1] = 1e-40
+    v = v.astype(np.float32)
+    want = store16(v.reshape(-1, 24)).astype(np.float32).reshape(v.shape)
+    assert np.isfinite(want).all()
+    h = lattice if nr == 1 else lattice.batch(nr)
+    try:
+        x = h.to_device(v[0] if nr == 1 else v)
+        got = h.to_host(h.store_h(x)).reshape(v.shape)
+        np.testing.assert_array_equal(got.view(np.uint32), want.view(np.uint32))
+        assert not got[:, :2].any()
+    finally:
+        if h is not lattice:
+            h.close()
