@@ -9,8 +9,9 @@ launch time and the algorithmic HBM bandwidth (bytes each launch must move:
 spinors read and written once, links and clover once per site).
 
 Kernels: jinv (one Richardson step on one colour), dslash_s / dslash_d (full
-D in FP32 / FP64), block_s (block-interior D on one colour), face_s (face hops
-of one colour), jinv_h / face_h (the FP16-storage Richardson step and face
+D in FP32 / FP64), block_s (block-interior D on one colour), update_s (the SAP
+half-sweep update s += in - D_blk a on one colour), face_s (face hops of one
+colour), jinv_h / face_h (the FP16-storage Richardson step and face
 hops through the single-operator entry points, conversions included), prec
 (the whole SAP preconditioner prec_ddd_s_), prec_h (the FP16-storage SAP),
 solve_hf (a whole precision-form solve to 1e-10; --new-kappa rebuilds the
@@ -94,6 +95,10 @@ def main():
             fn, nbytes = (lambda: lat.ddd(bd, out=out_d)), V * (2 * sp64 + lc64)
         elif k == "block_s":
             fn, nbytes = (lambda: lat.ddd_in(bs, 0, out=out_s)), (V // 2) * (2 * sp32 + lc32)
+        elif k == "update_s":  # one SAP half-sweep update on one colour: s += in - D_blk a
+            rhs = lat.to_device(np.roll(b, 1, axis=-2).astype(np.float32))  # its own stream
+            fn = lambda: lat.sap_update(out_s, bs, rhs, 0)
+            nbytes = (V // 2) * (4 * sp32 + lc32)  # a, in, s read + written; links, clover
         elif k == "face_s":
             fn, nbytes = (lambda: lat.ddd_out(bs, 0, 0.1, out=out_s)), None
         elif k == "jinv_h":  # FP16 storage: with the conversions of the single-op entry point
