@@ -11,8 +11,9 @@ spinors read and written once, links and clover once per site).
 Kernels: jinv (one Richardson step on one colour), dslash_s / dslash_d (full
 D in FP32 / FP64), block_s (block-interior D on one colour), update_s (the SAP
 half-sweep update s += in - D_blk a on one colour), face_s (face hops of one
-colour), jinv_h / face_h (the FP16-storage Richardson step and face
-hops through the single-operator entry points, conversions included), prec
+colour), block_d (block-interior D in FP64), jinv_h / face_h / update_h (the
+FP16-storage Richardson step, face hops and SAP update through the
+single-operator entry points, conversions included), prec
 (the whole SAP preconditioner prec_ddd_s_), prec_h (the FP16-storage SAP),
 solve_hf (a whole precision-form solve to 1e-10; --new-kappa rebuilds the
 clover term for another kappa before each, as a serving loop sees them).  --nrhs N runs the launch on a multi-RHS handle (N
@@ -99,6 +100,11 @@ def main():
             rhs = lat.to_device(np.roll(b, 1, axis=-2).astype(np.float32))  # its own stream
             fn = lambda: lat.sap_update(out_s, bs, rhs, 0)
             nbytes = (V // 2) * (4 * sp32 + lc32)  # a, in, s read + written; links, clover
+        elif k == "update_h":  # the same update with the FP16-storage kernel (conversions included)
+            rhs = lat.to_device(np.roll(b, 1, axis=-2).astype(np.float32))
+            fn, nbytes = (lambda: lat.sap_update(out_s, bs, rhs, 0, half=True)), None
+        elif k == "block_d":
+            fn, nbytes = (lambda: lat.ddd_in(bd, 0, out=out_d)), (V // 2) * (2 * sp64 + lc64)
         elif k == "face_s":
             fn, nbytes = (lambda: lat.ddd_out(bs, 0, 0.1, out=out_s)), None
         elif k == "jinv_h":  # FP16 storage: with the conversions of the single-op entry point
