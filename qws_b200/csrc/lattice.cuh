@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <type_traits>
 
 namespace qwsg {
@@ -79,6 +80,52 @@ struct Geom {
   FastDiv fB[4], fVb, fnbh0, fNB1, fNB2, fstr[4];
 };
 
+// The members of G that follow from its extents L, block extents B and block
+// grid NB (set and checked by the caller): site counts, plane stride, the
+// in-block order (block_local) and the multipliers of the site decoding.
+//
+// In-block order: the faces of the fastest direction are the only strided
+// ones, so it should have the largest extent; the slowest direction's stride
+// Vb/B_slowest is how far apart in a launch a site and its farthest neighbour
+// are read, which must stay within a few MB for the neighbour to be in L2
+// (16384 sites, ~13 MB of FP32 operator traffic).  Take the largest-extent
+// direction as fastest whose remaining largest extent, made slowest,
+// satisfies that; else the largest slowest and the second largest fastest.
+// Ties: t, z, y, x.
+inline void geom_layout(Geom& G) {
+  G.V = G.L[0] * G.L[1] * G.L[2] * G.L[3];
+  G.Vh = G.V / 2;
+  G.Vb = G.B[0] * G.B[1] * G.B[2] * G.B[3];
+  G.nbh0 = G.NB[0] / 2;
+  G.pad = (G.V + 127) / 128 * 128;
+  int d[4] = {3, 2, 1, 0};
+  std::stable_sort(d, d + 4, [&](int a, int b) { return G.B[a] > G.B[b]; });
+  int order[4] = {d[1], d[2], d[3], d[0]};  // fastest .. slowest
+  for (int f = 0; f < 4; f++) {
+    const int slow = d[f == 0 ? 1 : 0];
+    if (G.Vb / G.B[slow] <= 16384) {
+      int k = 0;
+      order[k++] = d[f];
+      for (int j = 0; j < 4; j++)
+        if (j != f && d[j] != slow) order[k++] = d[j];
+      order[3] = slow;
+      break;
+    }
+  }
+  int stride = 1;
+  for (int k = 0; k < 4; k++) {
+    G.str[order[k]] = stride;
+    stride *= G.B[order[k]];
+  }
+  G.rot = order[0];
+  for (int mu = 0; mu < 4; mu++) G.fstr[mu] = make_fastdiv(G.str[mu]);
+  for (int mu = 0; mu < 4; mu++) G.fB[mu] = make_fastdiv(G.B[mu]);
+  G.fVb = make_fastdiv(G.Vb);
+  G.fnbh0 = make_fastdiv(G.nbh0);
+  G.fNB1 = make_fastdiv(G.NB[1]);
+  G.fNB2 = make_fastdiv(G.NB[2]);
+}
+
 // plane stride of spinor fields and the entry of (site, rhs)
 __host__ __device__ __forceinline__ int spad(const Geom& G) { return G.pad << G.lgnr; }
 __host__ __device__ __forceinline__ int sentry(const Geom& G, int g, int r) {
@@ -92,7 +139,7 @@ struct Site {
 };
 
 // Inside a block, sites are lexicographic in an order of the four
-// directions chosen per block shape (G.str, set in the Ctx constructor):
+// directions chosen per block shape (G.str, set by geom_layout):
 // the largest extent is slowest, so the far neighbours of a site are the
 // nearest they can be and stay in L2 between the launches' reads; the
 // second largest is fastest, so every block face but that direction's is a
@@ -166,8 +213,8 @@ __device__ __forceinline__ void site_coords(const Geom& G, int g, int x[4]) {
 }
 
 // index of the neighbour across the block face in direction mu (dir = +1/-1)
-__device__ __forceinline__ int nbr_across(const Geom& G, const Site& s, int mu, int dir,
-                                          int* ncol) {
+__host__ __device__ __forceinline__ int nbr_across(const Geom& G, const Site& s, int mu, int dir,
+                                                   int* ncol) {
   int bc0 = s.bc[0], bc1 = s.bc[1], bc2 = s.bc[2], bc3 = s.bc[3];
   int l0 = s.lc[0], l1 = s.lc[1], l2 = s.lc[2], l3 = s.lc[3];
   int* bcp = mu == 0 ? &bc0 : mu == 1 ? &bc1 : mu == 2 ? &bc2 : &bc3;

@@ -17,8 +17,6 @@ namespace qwsg {
 
 namespace {
 
-int round_up(int v, int m) { return (v + m - 1) / m * m; }
-
 template <typename T>
 HopArgs<T> hop_args(const Geom& G, const typename Store<T>::type* U,
                     const typename Store<T>::type* C) {
@@ -183,48 +181,8 @@ Ctx::Ctx(const int L[4], const int NB[4], int tbc, int nrhs) {
   if (V >= (1L << 30)) throw Error(1, "lattice too large for 32-bit site indices");
   if (((long)(V + 127) / 128 * 128) * nrhs * 12 >= (1L << 31))
     throw Error(1, "lattice x right-hand sides too large for 32-bit plane offsets");
-  G.V = (int)V;
-  G.Vh = G.V / 2;
-  G.Vb = G.B[0] * G.B[1] * G.B[2] * G.B[3];
-  G.nbh0 = NB[0] / 2;
   G.tbc = tbc;
-  G.pad = round_up(G.V, 128);
-  // in-block order (block_local).  The faces of the fastest direction are
-  // the only strided ones, so it should have the largest extent; the
-  // slowest direction's stride Vb/B_slowest is how far apart in a launch
-  // a site and its farthest neighbour are read, which must stay within a
-  // few MB for the neighbour to be in L2 (16384 sites, ~13 MB of FP32
-  // operator traffic).  Take the largest-extent direction as fastest whose
-  // remaining largest extent, made slowest, satisfies that; else the
-  // largest slowest and the second largest fastest.  Ties: t, z, y, x.
-  {
-    int d[4] = {3, 2, 1, 0};
-    std::stable_sort(d, d + 4, [&](int a, int b) { return G.B[a] > G.B[b]; });
-    int order[4] = {d[1], d[2], d[3], d[0]};  // fastest .. slowest
-    for (int f = 0; f < 4; f++) {
-      const int slow = d[f == 0 ? 1 : 0];
-      if (G.Vb / G.B[slow] <= 16384) {
-        int k = 0;
-        order[k++] = d[f];
-        for (int j = 0; j < 4; j++)
-          if (j != f && d[j] != slow) order[k++] = d[j];
-        order[3] = slow;
-        break;
-      }
-    }
-    int stride = 1;
-    for (int k = 0; k < 4; k++) {
-      G.str[order[k]] = stride;
-      stride *= G.B[order[k]];
-    }
-    G.rot = order[0];
-  }
-  for (int mu = 0; mu < 4; mu++) G.fstr[mu] = make_fastdiv(G.str[mu]);
-  for (int mu = 0; mu < 4; mu++) G.fB[mu] = make_fastdiv(G.B[mu]);
-  G.fVb = make_fastdiv(G.Vb);
-  G.fnbh0 = make_fastdiv(G.nbh0);
-  G.fNB1 = make_fastdiv(G.NB[1]);
-  G.fNB2 = make_fastdiv(G.NB[2]);
+  geom_layout(G);  // V, Vh, Vb, pad, the in-block order, the divisions
   QWSG_CUDA(cudaGetDevice(&device));
   QWSG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   own_stream = true;
