@@ -161,6 +161,18 @@ __host__ __device__ __forceinline__ int block_local(const Geom& G, const int lc[
   return rot_pos(G, 0, lc[0]) * G.str[0] + rot_pos(G, 1, lc[1]) * G.str[1] +
          rot_pos(G, 2, lc[2]) * G.str[2] + rot_pos(G, 3, lc[3]) * G.str[3];
 }
+// whether DD-order site g lies on a face of its block (an in-block
+// coordinate 0 or B-1): the sites the face kernels visit
+__host__ __device__ __forceinline__ bool on_block_face(const Geom& G, int g) {
+  const int col = g >= G.Vh;
+  const int t = (g - col * G.Vh) % G.Vb;
+  bool face = false;
+  for (int mu = 0; mu < 4; mu++) {
+    const int l = rot_coord(G, mu, (t / G.str[mu]) % G.B[mu]);
+    face |= (l == 0) || (l == G.B[mu] - 1);
+  }
+  return face;
+}
 // offset of the interior hop from in-block coordinate l to l + dir along mu
 __host__ __device__ __forceinline__ int rot_step(const Geom& G, int mu, int l, int dir) {
   int d = dir * G.str[mu];

@@ -498,16 +498,8 @@ template void dslash_outer<double>(Ctx&, double*, const double*, int, int, doubl
 void Ctx::ensure_face_lists() {
   if (face_list[0] && face_list[1]) return;
   std::vector<int> lst[2];
-  for (int g = 0; g < G.V; g++) {
-    int col = g >= G.Vh;
-    const int t = (g - col * G.Vh) % G.Vb;
-    bool face = false;
-    for (int mu = 0; mu < 4; mu++) {  // block_local
-      const int l = rot_coord(G, mu, (t / G.str[mu]) % G.B[mu]);
-      face |= (l == 0) || (l == G.B[mu] - 1);
-    }
-    if (face) lst[col].push_back(g);
-  }
+  for (int g = 0; g < G.V; g++)
+    if (on_block_face(G, g)) lst[g >= G.Vh].push_back(g);
   for (int c2 = 0; c2 < 2; c2++) {
     if (face_list[c2]) continue;  // made by an earlier call that failed on the other
     int* d = nullptr;

@@ -10,7 +10,9 @@
 //     when it lies in the same block, nbr_across(...) when it crosses a block
 //     face (periodic wrap included) -- equals dd_index of the neighbour's
 //     coordinates and lies in [0, V), and the colour nbr_across reports is
-//     the neighbour's block colour.
+//     the neighbour's block colour;
+//   * on_block_face(g), which makes the face kernels' site lists, holds
+//     exactly when some hop of g leaves its block.
 // It prints one line per lattice and exits non-zero on the first failure.
 // Built and run by tests/test_geometry_host.py (nvcc, no GPU needed).
 #include <cstdio>
@@ -56,6 +58,9 @@ static int check(const int L[4], const int NB[4], bool planted) {
     if ((s.bc[0] + s.bc[1] + s.bc[2] + s.bc[3]) % 2 != s.col)
       return fail("block colour", L, NB, g, -1, 0);
     if (dd_index(G, x) != g) return fail("dd_index(decode_site(g)) != g", L, NB, g, -1, 0);
+    bool face = false;  // some hop leaves the block
+    for (int mu = 0; mu < 4; mu++) face |= s.lc[mu] == 0 || s.lc[mu] == G.B[mu] - 1;
+    if (on_block_face(G, (int)g) != face) return fail("face-site test", L, NB, g, -1, 0);
     for (int mu = 0; mu < 4; mu++)
       for (int dir = -1; dir <= 1; dir += 2) {
         int y[4] = {x[0], x[1], x[2], x[3]};
